@@ -1,0 +1,198 @@
+"""CPU oracle for the DSPLIB filtering path.  TEST INFRASTRUCTURE ONLY.
+
+Two checkers live here, both loaded through ctypes:
+
+* ``port``: this project's C restatement (``dsplib_oracle.c``), built into
+  ``oracle/_build/liboracle_port.so`` by ``oracle/Makefile``.
+* ``ref``: the reference's own natural-C kernels (``DSPLIB_fir_cn.cpp`` and
+  ``DSPLIB_cascadeBiquad_cn.cpp``) compiled unmodified, with the stand-in TI
+  headers of ``oracle/shim``, into ``oracle/_ref/libdsplib_ref.so``.  Present
+  whenever the library was built here (it travels with the repository
+  snapshot) — it is optional; tests that need it skip when it is absent.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package.  The product library never does.
+
+Parity status: the port is pinned against the reference ``_cn`` library and
+against golden vectors generated by the reference's Python models
+(``tests/golden/make_golden.py``).  Q-mode FIR has no reference counterpart in
+the natural-C path; its restatement follows the MMA output-stage configuration
+(``src/common/c7504/DSPLIB_configurations.cpp:94-160``) and is "parity
+unpinned" by reference tests.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "_build", "liboracle_port.so")
+REF_SO = os.path.join(HERE, "_ref", "libdsplib_ref.so")
+
+DT = {np.dtype(np.int8): 0, np.dtype(np.int16): 1, np.dtype(np.int32): 2, np.dtype(np.float32): 12}
+
+_port = None
+_ref = None
+
+
+def build(ref_root: str | None = None) -> None:
+    """Compile the checker libraries (port always; reference when its sources exist)."""
+    args = ["make", "-s", "-C", HERE]
+    if ref_root:
+        args.append(f"REF={ref_root}")
+    subprocess.run(args, check=True)
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
+
+
+def port():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_SO):
+            build()
+        _port = ctypes.CDLL(PORT_SO)
+        for name in ("oracle_fir_cn", "oracle_fir_q", "oracle_fir_f64", "oracle_biquad_df",
+                     "oracle_biquad_df_f64", "oracle_biquad_tif", "oracle_tif_coefficients"):
+            getattr(_port, name).restype = None
+    return _port
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError(REF_SO)
+        _ref = ctypes.CDLL(REF_SO)
+    return _ref
+
+
+# ------------------------------------------------------------------ FIR
+
+
+def fir(x, h, T, *, nch, impl="port", threads=1):
+    """Natural-C FIR with explicit tap count ``T``; ``h`` rows hold the stored
+    taps (pitch = row length)."""
+    x = np.ascontiguousarray(x)
+    h = np.ascontiguousarray(h)
+    batch, in_pitch = x.shape
+    out_size = in_pitch - T + 1
+    y = np.zeros((batch, out_size), dtype=x.dtype)
+    fp = h.shape[1]
+    if impl == "port":
+        port().oracle_fir_cn(DT[x.dtype], _ptr(x), _ptr(h), _ptr(y), batch, T, out_size, in_pitch, out_size,
+                             fp if nch else 0)
+    else:
+        assert fp == T or not nch, "reference _cn derives the Nch tap pitch from T"
+        lib = ref()
+        if threads > 1:
+            rc = lib.ref_fir_cn_mt(DT[x.dtype], _ptr(x), _ptr(h), _ptr(y), batch, T, out_size, in_pitch,
+                                   out_size, int(nch), 0, 0, int(threads))
+        else:
+            rc = lib.ref_fir_cn(DT[x.dtype], _ptr(x), _ptr(h), _ptr(y), batch, T, out_size, in_pitch, out_size,
+                                int(nch), 0, 0)
+        assert rc == 0, rc
+    return y
+
+
+def fir_q(x, h, T, shift, *, nch):
+    x = np.ascontiguousarray(x)
+    h = np.ascontiguousarray(h)
+    batch, in_pitch = x.shape
+    out_size = in_pitch - T + 1
+    y = np.zeros((batch, out_size), dtype=x.dtype)
+    port().oracle_fir_q(DT[x.dtype], _ptr(x), _ptr(h), _ptr(y), batch, T, out_size, in_pitch, out_size,
+                        h.shape[1] if nch else 0, int(shift))
+    return y
+
+
+def fir_f64(x, h, T, *, nch):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    h = np.ascontiguousarray(h, dtype=np.float32)
+    batch, in_pitch = x.shape
+    out_size = in_pitch - T + 1
+    y = np.zeros((batch, out_size), dtype=np.float64)
+    port().oracle_fir_f64(_ptr(x), _ptr(h), _ptr(y), batch, T, out_size, in_pitch, out_size,
+                          h.shape[1] if nch else 0)
+    return y
+
+
+# --------------------------------------------------------------- biquad
+
+FORM = {"TIF": 0, "DF1": 1, "DF2": 2, "TDF2": 3}
+
+
+def nvars(form):
+    return 4 if form == FORM["DF1"] else 2
+
+
+def biquad(form, x, coef, state, *, nch, impl="port", threads=1):
+    """Direct-form cascade over time-major ``x`` [N, C] (dense pitch C).
+    ``coef`` natural [rows, S*5]; ``state`` [S*nv, C] is updated in place.
+    ``impl='ref'`` runs the reference _cn kernel (TIF -> DF2, as NATC does)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    coef = np.ascontiguousarray(coef, dtype=np.float32)
+    assert state.flags.c_contiguous and state.dtype == np.float32
+    N, C = x.shape
+    S = coef.shape[1] // 5
+    y = np.zeros((N, C), dtype=np.float32)
+    if impl == "port":
+        port().oracle_biquad_df(int(form), _ptr(x), _ptr(coef), _ptr(state), _ptr(y), N, S, C, int(nch), C, C,
+                                state.shape[1])
+    else:
+        lib = ref()
+        if threads > 1:
+            rc = lib.ref_biquad_cn_mt(int(form), _ptr(x), _ptr(coef), _ptr(state), _ptr(y), N, S, C, int(nch),
+                                      C, C, state.shape[1], int(threads))
+        else:
+            rc = lib.ref_biquad_cn(int(form), _ptr(x), _ptr(coef), _ptr(state), _ptr(y), N, S, C, int(nch), C,
+                                   C, state.shape[1])
+        assert rc == 0, rc
+    return y
+
+
+def biquad_f64(form, x, coef, state64, *, nch):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    coef = np.ascontiguousarray(coef, dtype=np.float32)
+    assert state64.flags.c_contiguous and state64.dtype == np.float64
+    N, C = x.shape
+    S = coef.shape[1] // 5
+    y = np.zeros((N, C), dtype=np.float64)
+    port().oracle_biquad_df_f64(int(form), _ptr(x), _ptr(coef), _ptr(state64), _ptr(y), N, S, C, int(nch), C,
+                                C, state64.shape[1])
+    return y
+
+
+def tif_groups(S):
+    return 1 if S <= 7 else (S + 6) // 7
+
+
+def tif_coefficients(natural_row):
+    """natural [S*5] -> (tifCoef [S*4], gains [G]) for one channel."""
+    nat = np.ascontiguousarray(natural_row, dtype=np.float32)
+    S = nat.size // 5
+    tc = np.zeros(S * 4, dtype=np.float32)
+    g = np.zeros(tif_groups(S), dtype=np.float32)
+    port().oracle_tif_coefficients(_ptr(nat), S, _ptr(tc), _ptr(g))
+    return tc, g
+
+
+def biquad_tif(x, tif_coef, gains, state, *, nch):
+    """TIF cascade; tif_coef [rows, S*4] storage order {c0,c1,-a2,-a1}, gains [rows, G]."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    tif_coef = np.ascontiguousarray(tif_coef, dtype=np.float32)
+    gains = np.ascontiguousarray(gains, dtype=np.float32)
+    N, C = x.shape
+    S = tif_coef.shape[1] // 4
+    y = np.zeros((N, C), dtype=np.float32)
+    port().oracle_biquad_tif(_ptr(x), _ptr(tif_coef), _ptr(gains), _ptr(state), _ptr(y), N, S, C, int(nch), C, C,
+                             state.shape[1])
+    return y
