@@ -1,0 +1,521 @@
+#!/usr/bin/env python
+"""Benchmark of the DSPLIB filtering hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+Default workload (N = 1): the plain DSPLIB_cascadeBiquad fp32 configuration,
+32 channels x 8192 samples x 4 stages (DF2, OPTIMIZED path: chunked
+parallel-in-time scan), seeded synthetic coefficients: each stage a conjugate
+pole pair r ~ U[0.5, 0.95], theta ~ U[0, pi], a zero pair on the unit circle
+at phi ~ U[0, pi], gain normalised so |H(e^{j theta})| = 1; input N(0, 1);
+zero initial state.  Other workloads: the FIR configurations (see WORKLOADS).
+
+One step = one exec call over the whole batch, inputs resident in HBM.  The
+batch is far smaller than L2, so L2 is flushed (256 MiB write) between steps,
+outside the CUDA events that time each step.  ``value`` = samples processed by
+all ranks / max-over-ranks device time.  ``e2e`` = the same metric through the
+C ABI with pinned host buffers (host->device and device->host copies inside
+the library call).  Multi-GPU: one process per GPU (torchrun), each rank runs
+its own channel block (no data-path collective), weak scaling.
+
+``--impl reference`` times the reference's natural-C kernels (compiled from
+the reference sources into oracle/_ref) on the host cores with all threads,
+on the same workload, and prints the same JSON line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_FLUSH_BYTES = 256 << 20
+FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, FALLBACK_BF16_TFLOPS, "fallback"
+
+
+def profile_traffic(name):
+    """dram bytes per launch recorded from an ncu capture in profiles/<name>.md."""
+    p = os.path.join(ROOT, "profiles", name + ".md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_launch"):
+            try:
+                return int(float(line.split("=")[1].split()[0]))
+            except Exception:
+                return None
+    return None
+
+
+# ----------------------------------------------------------- workloads
+
+
+def biquad_coefficients(rng, rows, S):
+    """Natural [rows, S*5] per the default-workload rule (module docstring)."""
+    out = np.zeros((rows, S, 5), np.float64)
+    for r_ in range(rows):
+        for s in range(S):
+            r = rng.uniform(0.5, 0.95)
+            th = rng.uniform(0, math.pi)
+            ph = rng.uniform(0, math.pi)
+            b = np.array([1.0, -2 * math.cos(ph), 1.0])
+            a = np.array([1.0, -2 * r * math.cos(th), r * r])
+            z = np.exp(-1j * th * np.arange(3))
+            g = 1.0 / max(abs(np.dot(b, z) / np.dot(a, z)), 1e-12)
+            out[r_, s] = [g * b[0], g * b[1], g * b[2], a[1], a[2]]
+    return out.reshape(rows, S * 5).astype(np.float32)
+
+
+def lowpass_taps(rng, rows, T):
+    """Hamming-windowed sinc low-pass, cutoff ~ U[0.05, 0.45] of Nyquist, unit DC gain; stored order."""
+    n = np.arange(T) - (T - 1) / 2.0
+    out = np.zeros((rows, T), np.float32)
+    for r_ in range(rows):
+        fc = rng.uniform(0.05, 0.45)
+        h = fc * np.sinc(fc * n) * np.hamming(T)
+        out[r_] = (h / h.sum())[::-1]
+    return out
+
+
+class Workload:
+    name = ""
+    metric = "Gsamples/s"
+    dtype = "f32"
+
+
+class BiquadWorkload(Workload):
+    def __init__(self, C=32, N=8192, S=4, form=2, seed=2):
+        import c7x_dsplib_b200 as D
+
+        self.D = D
+        self.C, self.N, self.S, self.form = C, N, S, form
+        self.name = f"cascadeBiquad_DF2_{C}ch_x_{N}_x_{S}stages"
+        rng = np.random.default_rng(seed)
+        self.x = rng.standard_normal((N, C)).astype(np.float32)
+        self.nat = biquad_coefficients(rng, 1, S)
+        self.opt, _ = D.opt_coefficients(self.nat, form, 0, C)
+        self.samples = N * C
+        nv = 4 if form == 1 else 2
+        self.alg_bytes = 4 * (2 * N * C) + 4 * 5 * S + 2 * 4 * (S * nv * C)
+        self.bound = "hbm"
+        self.kernel = "biquad_scan_kernel"
+
+    def config(self):
+        return {"workload": self.name, "channels": self.C, "samples_per_channel": self.N, "stages": self.S,
+                "form": "DF2", "funcStyle": "OPTIMIZED", "coefficients": "shared"}
+
+    def setup_device(self, torch, func_style=None):
+        D = self.D
+        fs = D.OPTIMIZED if func_style is None else func_style
+        self.xd = torch.from_numpy(self.x).cuda()
+        self.yd = torch.zeros_like(self.xd)
+        self.sd = torch.zeros((self.S * 2, self.C), device="cuda")
+        self.cd = torch.from_numpy(self.opt if fs == D.OPTIMIZED else self.nat).cuda()
+        args, pin, pout, pvar, pcn, popt = D.biquad_descs(self.C, self.N, self.S, self.form, 0, func_style=fs)
+        self.h = D.BiquadHandle()
+        st = self.h.init(args, pin, popt if fs == D.OPTIMIZED else pcn, pvar, pout)
+        assert st == D.SUCCESS, self.h.last_error()
+        self.h.set_async(True)
+
+    def step(self):
+        st = self.h.exec(self.xd, self.cd, self.sd, self.yd)
+        if st != self.D.SUCCESS:
+            raise RuntimeError(self.h.last_error())
+
+    def e2e_setup(self, torch):
+        D = self.D
+        self.hx = torch.from_numpy(self.x).pin_memory()
+        self.hy = torch.zeros_like(self.hx).pin_memory()
+        self.hs = torch.zeros((self.S * 2, self.C)).pin_memory()
+        self.hc = torch.from_numpy(self.opt).pin_memory()
+        args, pin, pout, pvar, pcn, popt = D.biquad_descs(self.C, self.N, self.S, self.form, 0)
+        self.he = D.BiquadHandle()
+        assert self.he.init(args, pin, popt, pvar, pout) == D.SUCCESS
+        self.h2d = self.hx.numel() * 4 + self.hc.numel() * 4 + self.hs.numel() * 4
+        self.d2h = self.hy.numel() * 4 + self.hs.numel() * 4
+
+    def e2e_step(self):
+        st = self.he.exec(self.hx, self.hc, self.hs, self.hy)
+        if st != self.D.SUCCESS:
+            raise RuntimeError(self.he.last_error())
+
+    def cpu_reference(self, threads, budget_s):
+        import oracle
+
+        reps, t_total = 0, 0.0
+        while t_total < budget_s or reps < 2:
+            st = np.zeros((self.S * 2, self.C), np.float32)
+            t0 = time.perf_counter()
+            oracle.biquad(self.form, self.x, self.nat, st, nch=0, impl="ref", threads=threads)
+            t_total += time.perf_counter() - t0
+            reps += 1
+        return self.samples * reps / t_total / 1e9, f"{reps} full passes of the workload ({self.C} ch x {self.N})"
+
+
+class FirWorkload(Workload):
+    def __init__(self, name, dtype, B, N, T, *, nch, precision=0, qmode=False, shift=0, seed=3):
+        import c7x_dsplib_b200 as D
+
+        self.D = D
+        self.name = name
+        self.B, self.N, self.T, self.nch, self.precision, self.qmode, self.shift = B, N, T, nch, precision, qmode, shift
+        rng = np.random.default_rng(seed)
+        self.npdt = dtype
+        if dtype == np.float32:
+            self.x = rng.standard_normal((B, N)).astype(np.float32)
+            self.hh = lowpass_taps(rng, B if nch else 1, T)
+            self.dtype = "f32"
+        else:
+            info = np.iinfo(dtype)
+            lo, hi = (-4096, 4095) if (dtype == np.int16 and name.startswith("fir_int16_16ch")) else (info.min,
+                                                                                                      info.max)
+            self.x = rng.integers(lo, hi, size=(B, N), endpoint=True).astype(dtype)
+            self.hh = rng.integers(lo, hi, size=(B if nch else 1, T), endpoint=True).astype(dtype)
+            self.dtype = {np.int8: "i8", np.int16: "i16", np.int32: "i32"}[dtype]
+        elt = np.dtype(dtype).itemsize
+        self.out_size = N - T + 1
+        self.samples = B * self.out_size
+        self.alg_bytes = elt * (B * N + B * self.out_size + self.hh.size)
+        self.alg_flops = 2.0 * T * self.samples
+        self.bound = "tensor" if precision == 1 else "hbm"
+        self.kernel = "fir_f32_simt_kernel" if dtype == np.float32 else "fir_direct_kernel"
+
+    def config(self):
+        return {"workload": self.name, "channels": self.B, "samples_per_channel": self.N, "taps": self.T,
+                "coefficients": "per-channel" if self.nch else "shared",
+                "precision": ["simt_fp32", "bf16x3"][self.precision] if self.dtype == "f32" else
+                ("q_mode shift=%d" % self.shift if self.qmode else "wrap (natural-C)")}
+
+    def setup_device(self, torch, func_style=None):
+        D = self.D
+        fs = D.OPTIMIZED if func_style is None else func_style
+        self.xd = torch.from_numpy(self.x).cuda()
+        self.hd = torch.from_numpy(self.hh).cuda()
+        self.yd = torch.zeros((self.B, self.out_size), dtype=self.xd.dtype, device="cuda")
+        code = {"f32": D.FLOAT32, "i8": D.INT8, "i16": D.INT16, "i32": D.INT32}[self.dtype]
+        args, pin, pf, po = D.fir_setup(code, self.B, self.N, self.T, nch=self.nch, func_style=fs, shift=self.shift)
+        self.h = D.FirHandle()
+        assert self.h.init(args, pin, pf, po) == D.SUCCESS
+        self.h.set_precision(self.precision)
+        self.h.set_qmode(self.qmode)
+        self.h.set_async(True)
+        self.args = (args, pin, pf, po)
+
+    def step(self):
+        st = self.h.exec(self.xd, self.hd, self.yd)
+        if st != self.D.SUCCESS:
+            raise RuntimeError(self.h.last_error())
+
+    def e2e_setup(self, torch):
+        self.hx = torch.from_numpy(self.x).pin_memory()
+        self.hhp = torch.from_numpy(self.hh).pin_memory()
+        self.hy = torch.zeros((self.B, self.out_size), dtype=self.hx.dtype).pin_memory()
+        self.he = self.D.FirHandle()
+        args, pin, pf, po = self.args
+        assert self.he.init(args, pin, pf, po) == self.D.SUCCESS
+        self.he.set_precision(self.precision)
+        self.he.set_qmode(self.qmode)
+        elt = np.dtype(self.npdt).itemsize
+        self.h2d = (self.x.size + self.hh.size) * elt
+        self.d2h = self.samples * elt
+
+    def e2e_step(self):
+        st = self.he.exec(self.hx, self.hhp, self.hy)
+        if st != self.D.SUCCESS:
+            raise RuntimeError(self.he.last_error())
+
+    def cpu_reference(self, threads, budget_s):
+        import oracle
+
+        # bounded sample: a channel subset sized to the budget, scaled by samples
+        rows = self.B
+        per_row_s = None
+        reps, t_total, done = 0, 0.0, 0
+        sub = min(self.B, max(threads, 1))
+        while t_total < budget_s or reps < 1:
+            xs = np.ascontiguousarray(self.x[:sub])
+            hs = np.ascontiguousarray(self.hh[:sub] if self.nch else self.hh)
+            t0 = time.perf_counter()
+            oracle.fir(xs, hs, self.T, nch=self.nch, impl="ref", threads=threads)
+            dt = time.perf_counter() - t0
+            t_total += dt
+            done += sub * self.out_size
+            reps += 1
+            if per_row_s is None:
+                per_row_s = dt / sub
+                if dt < budget_s / 20 and sub < rows:
+                    sub = min(rows, max(sub, int(sub * (budget_s / 10) / max(dt, 1e-6))))
+        return done / t_total / 1e9, f"{done // self.out_size} channel passes of {self.N} samples (subset of the " \
+                                     f"{self.B}-channel workload)"
+
+
+WORKLOADS = {
+    "biquad_32x8192x4": lambda: BiquadWorkload(),
+    "biquad_4096x8192x4": lambda: BiquadWorkload(C=4096),
+    "fir_int16_16ch_4096_64taps": lambda: FirWorkload("fir_int16_16ch_4096_64taps", np.int16, 16, 4096, 64, nch=0,
+                                                      qmode=True, shift=15, seed=1),
+    "fir_f32_1024ch_65536_256taps_simt": lambda: FirWorkload("fir_f32_1024ch_65536_256taps_simt", np.float32, 1024,
+                                                             65536, 256, nch=1, precision=0),
+    "fir_f32_1024ch_65536_256taps_bf16x3": lambda: FirWorkload("fir_f32_1024ch_65536_256taps_bf16x3", np.float32,
+                                                               1024, 65536, 256, nch=1, precision=1),
+    "fir_int8_4096ch_16384_128taps": lambda: FirWorkload("fir_int8_4096ch_16384_128taps", np.int8, 4096, 16384, 128,
+                                                         nch=0, qmode=True, shift=7, seed=4),
+    "fir_int16_4096ch_16384_128taps": lambda: FirWorkload("fir_int16_4096ch_16384_128taps", np.int16, 4096, 16384,
+                                                          128, nch=0, qmode=True, shift=15, seed=4),
+}
+DEFAULT = "biquad_32x8192x4"
+
+
+# ----------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for l in self.lines:
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ----------------------------------------------------------- main
+
+
+def best_threads(wl):
+    """All host threads, unless thread start-up outweighs the work (tiny workloads): then one."""
+    n = os.cpu_count() or 1
+    if n == 1:
+        return 1
+    v1, _ = wl.cpu_reference(1, budget_s=0.2)
+    vn, _ = wl.cpu_reference(n, budget_s=0.2)
+    return n if vn >= v1 else 1
+
+
+def run_reference(a, wl):
+    threads = best_threads(wl)
+    try:
+        import oracle
+
+        if not oracle.ref_available():
+            print(json.dumps({"impl": "reference", "unavailable": "reference natural-C library oracle/_ref not built"}))
+            return
+        value, sample = wl.cpu_reference(threads, budget_s=2.0)
+        # K timed steps of the same bounded sample, after W warm-up steps
+        for _ in range(a.warmup):
+            wl.cpu_reference(threads, budget_s=0.0)
+        vals = []
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            v, _ = wl.cpu_reference(threads, budget_s=0.05)
+            vals.append(v)
+        elapsed = time.perf_counter() - t0
+        value = statistics.median(vals)
+    except Exception as e:  # the reference arm must always print its line
+        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {e}"}))
+        return
+    line = {"metric": f"{wl.name} {wl.metric}", "value": value, "unit": wl.metric, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": elapsed * 1e3 / max(a.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype,
+            "data": "synthetic (seeded)", "config": wl.config(), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": wl.metric, "cores": threads, "kind": "reference",
+                             "sample": sample + "; reference _cn compiled from the reference sources, channels split "
+                                                "over std::threads"},
+            "e2e": {"value": value, "unit": wl.metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if a.impl == "reference":
+        if rank == 0:
+            run_reference(a, WORKLOADS[a.workload]())
+        return
+
+    import torch
+
+    import c7x_dsplib_b200 as D
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    wl = WORKLOADS[a.workload]()
+    wl.setup_device(torch)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    wl.h.set_stream(stream)
+
+    for _ in range(a.warmup):
+        wl.step()
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = D.kernel_launch_count()
+    for i in range(a.steps):
+        flush.zero_()
+        starts[i].record(stream)
+        wl.step()
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    launches = D.kernel_launch_count() - n0
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / a.steps
+    value = wl.samples * world / (ms_per_step * 1e-3) / 1e9
+
+    hbm, bf16, peak_kind = peaks()
+    kernel_ms = statistics.median(step_ms)
+    if wl.bound == "hbm":
+        achieved = wl.alg_bytes / (kernel_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+                "fallback 6650 GB/s", "algorithmic_bytes_per_launch": wl.alg_bytes}
+    else:
+        achieved = wl.alg_flops / (kernel_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
+                "peak_source": f"{peak_kind} bf16_tflops", "algorithmic_flops_per_launch": wl.alg_flops}
+    traffic = profile_traffic(f"{wl.kernel}_{wl.name}")
+    roof["traffic"] = traffic
+    roof["kernel"] = wl.kernel
+    roof["median_launch_ms"] = kernel_ms
+
+    # end to end through the C ABI with pinned host buffers
+    wl.e2e_setup(torch)
+    for _ in range(3):
+        wl.e2e_step()
+    e2e_steps = max(10, min(a.steps, 200))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        wl.e2e_step()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": wl.samples * world / e2e_s / 1e9, "unit": wl.metric, "h2d_bytes_per_step": wl.h2d,
+           "d2h_bytes_per_step": wl.d2h, "ms_per_step": e2e_s * 1e3}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            import oracle
+
+            if oracle.ref_available():
+                threads = best_threads(wl)
+                v, sample = wl.cpu_reference(threads, budget_s=3.0)
+                cpu = {"value": v, "unit": wl.metric, "cores": threads, "kind": "reference",
+                       "sample": sample + "; reference _cn compiled from the reference sources"}
+        except Exception as e:
+            cpu = {"value": None, "unit": wl.metric, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": f"{wl.name} {wl.metric}", "value": value, "unit": wl.metric, "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic (seeded)",
+                "config": dict(wl.config(), l2="flushed between steps (256 MiB write outside the timed events)",
+                               parallelism=f"channel blocks x{world}, no collective"),
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

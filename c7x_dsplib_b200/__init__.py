@@ -1,0 +1,314 @@
+"""B200-native DSPLIB filtering path: DSPLIB_fir and DSPLIB_cascadeBiquad.
+
+The product is the C-ABI shared library ``libdsplib_b200.so`` built from
+``csrc/`` (``python -m c7x_dsplib_b200.build``); its entry points are declared
+in ``include/DSPLIB_fir.h``, ``include/DSPLIB_cascadeBiquad.h`` and
+``include/dsplib_gpu.h``.  This module is the Python binding of that C ABI:
+
+* ``lib()`` returns the loaded ``ctypes.CDLL`` with argument types set;
+* ``FirHandle`` / ``BiquadHandle`` mirror the reference call sequence
+  (getHandleSize -> init_checkParams -> init -> exec_checkParams -> exec);
+* ``fir()`` / ``cascade_biquad()`` run one call on numpy arrays (host
+  buffers, staged by the library) or torch CUDA tensors (device buffers).
+
+There is no CPU implementation here: if the library is missing or no CUDA
+device is present, calls fail with an error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libdsplib_b200.so")
+
+# DSPLIB_STATUS (include/DSPLIB_types.h)
+SUCCESS = 0
+ERR_FAILURE = 1
+ERR_INVALID_VALUE = 2
+ERR_INVALID_TYPE = 3
+ERR_INVALID_DIMENSION = 4
+ERR_NULL_POINTER = 5
+ERR_NOT_IMPLEMENTED = 6
+ERR_NOT_ALIGNED_WIDTHS = 9
+
+# DSPLIB_data_type_e (include/DSPLIB_bufParams.h)
+INT8, INT16, INT32, INT64, UINT8, UINT16, UINT32, UINT64, FLOAT32, FLOAT64 = 0, 1, 2, 3, 5, 6, 8, 9, 12, 13
+NATC, OPTIMIZED = 0, 1
+TIF, DF1, DF2, TDF2 = 0, 1, 2, 3
+FIR_SIMT, FIR_BF16X3 = 0, 1
+MMA_SIZE = {1: 32, 2: 16, 4: 8}  # DSPLIB_MMA_SIZE_{8,16,32}_BIT
+
+_NP2DT = {np.dtype(np.int8): INT8, np.dtype(np.int16): INT16, np.dtype(np.int32): INT32,
+          np.dtype(np.float32): FLOAT32}
+
+
+class BufParams2D(ctypes.Structure):
+    _fields_ = [("data_type", ctypes.c_uint32), ("dim_x", ctypes.c_uint32), ("dim_y", ctypes.c_uint32),
+                ("stride_y", ctypes.c_int32)]
+
+
+class FirInitArgs(ctypes.Structure):
+    _fields_ = [("funcStyle", ctypes.c_int8), ("dataSize", ctypes.c_int32), ("batchSize", ctypes.c_int32),
+                ("filterSize", ctypes.c_int32), ("shift", ctypes.c_uint32), ("enableNchCoefs", ctypes.c_uint32),
+                ("enableMMA", ctypes.c_uint32), ("MMA_SIZE", ctypes.c_int32), ("enableQ", ctypes.c_uint32),
+                ("Q", ctypes.c_uint32)]
+
+
+class BiquadInitArgs(ctypes.Structure):
+    _fields_ = [("funcStyle", ctypes.c_int8), ("dataSize", ctypes.c_uint32), ("numStages", ctypes.c_uint32),
+                ("numChannels", ctypes.c_uint32), ("enableNChCoeffs", ctypes.c_uint32),
+                ("biquadForm", ctypes.c_uint32)]
+
+
+_lib = None
+_P = ctypes.POINTER
+_VP = ctypes.c_void_p
+_BP = _P(BufParams2D)
+
+# name -> (restype, argtypes); every symbol declared in include/*.h
+SIGNATURES = {
+    "DSPLIB_fir_getHandleSize": (ctypes.c_int32, [_P(FirInitArgs)]),
+    "DSPLIB_fir_getSizes": (ctypes.c_int, [_P(FirInitArgs), _BP, _BP, _BP]),
+    "DSPLIB_fir_init": (ctypes.c_int, [_VP, _BP, _BP, _BP, _P(FirInitArgs)]),
+    "DSPLIB_fir_init_checkParams": (ctypes.c_int, [_VP, _BP, _BP, _BP, _P(FirInitArgs)]),
+    "DSPLIB_fir_exec": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "DSPLIB_fir_exec_checkParams": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "DSPLIB_fir_perfEst": (None, [_VP, _BP, _BP, _BP, _P(ctypes.c_uint64), _P(ctypes.c_uint64)]),
+    "DSPLIB_cascadeBiquad_getHandleSize": (ctypes.c_int32, [_P(BiquadInitArgs)]),
+    "DSPLIB_cascadeBiquad_get_coefficientsBufferDesc": (
+        ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _BP]),
+    "DSPLIB_cascadeBiquad_get_coefficients": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, _BP, _BP, _VP, _VP]),
+    "DSPLIB_cascadeBiquad_init": (ctypes.c_int, [_VP, _BP, _BP, _BP, _BP, _P(BiquadInitArgs)]),
+    "DSPLIB_cascadeBiquad_init_checkParams": (ctypes.c_int, [_VP, _BP, _BP, _BP, _BP, _P(BiquadInitArgs)]),
+    "DSPLIB_cascadeBiquad_exec": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "DSPLIB_cascadeBiquad_exec_checkParams": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "DSPLIB_cascadeBiquad_perfEst": (None, [_VP, _BP, _BP, _BP, _BP, _P(ctypes.c_uint64), _P(ctypes.c_uint64)]),
+    "DSPLIB_gpu_setStream": (ctypes.c_int, [_VP, _VP]),
+    "DSPLIB_gpu_setAsync": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "DSPLIB_gpu_lastError": (ctypes.c_char_p, [_VP]),
+    "DSPLIB_gpu_firSetPrecision": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "DSPLIB_gpu_firSetQMode": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "DSPLIB_gpu_kernelLaunchCount": (ctypes.c_int64, []),
+}
+
+
+def lib() -> ctypes.CDLL:
+    """Load libdsplib_b200.so (build it first: python -m c7x_dsplib_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing; build it with `python -m c7x_dsplib_b200.build`")
+        l = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+class DsplibError(RuntimeError):
+    def __init__(self, what, status, detail=""):
+        super().__init__(f"{what} returned {status}{': ' + detail if detail else ''}")
+        self.status = status
+
+
+def bp(data_type, dim_x, dim_y, stride_y) -> BufParams2D:
+    return BufParams2D(int(data_type), int(dim_x), int(dim_y), int(stride_y))
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return int(a)
+
+
+def _dtype_code(a):
+    if isinstance(a, np.ndarray):
+        return _NP2DT[a.dtype]
+    import torch
+
+    return {torch.int8: INT8, torch.int16: INT16, torch.int32: INT32, torch.float32: FLOAT32}[a.dtype]
+
+
+def _elt(code):
+    return {INT8: 1, INT16: 2, INT32: 4, FLOAT32: 4}[code]
+
+
+class _Handle:
+    size_fn = ""
+
+    def __init__(self):
+        L = lib()
+        self.buf = ctypes.create_string_buffer(int(getattr(L, self.size_fn)(None)))
+        self.h = ctypes.cast(self.buf, ctypes.c_void_p)
+
+    def last_error(self) -> str:
+        s = lib().DSPLIB_gpu_lastError(self.h)
+        return s.decode() if s else ""
+
+    def set_stream(self, stream):
+        """stream: torch.cuda.Stream, raw cudaStream_t int, or None (default stream)."""
+        raw = getattr(stream, "cuda_stream", stream)
+        return lib().DSPLIB_gpu_setStream(self.h, raw or None)
+
+    def set_async(self, on: bool):
+        return lib().DSPLIB_gpu_setAsync(self.h, int(bool(on)))
+
+    def _check(self, what, st):
+        if st != SUCCESS:
+            raise DsplibError(what, st, self.last_error())
+        return st
+
+
+class FirHandle(_Handle):
+    """Reference call sequence of test/DSPLIB_fir/DSPLIB_fir_d.c:101-305."""
+
+    size_fn = "DSPLIB_fir_getHandleSize"
+
+    def init(self, args: FirInitArgs, pin: BufParams2D, pfilt: BufParams2D, pout: BufParams2D) -> int:
+        self.args, self.pin, self.pfilt, self.pout = args, pin, pfilt, pout
+        return lib().DSPLIB_fir_init(self.h, ctypes.byref(pin), ctypes.byref(pfilt), ctypes.byref(pout),
+                                     ctypes.byref(args))
+
+    def init_check(self, args, pin, pfilt, pout) -> int:
+        return lib().DSPLIB_fir_init_checkParams(self.h, ctypes.byref(pin), ctypes.byref(pfilt), ctypes.byref(pout),
+                                                 ctypes.byref(args))
+
+    def exec(self, x, h, y) -> int:
+        return lib().DSPLIB_fir_exec(self.h, _ptr(x), _ptr(h), _ptr(y))
+
+    def set_precision(self, p: int):
+        return lib().DSPLIB_gpu_firSetPrecision(self.h, int(p))
+
+    def set_qmode(self, on: bool):
+        return lib().DSPLIB_gpu_firSetQMode(self.h, int(bool(on)))
+
+
+class BiquadHandle(_Handle):
+    """Reference call sequence of test/DSPLIB_cascadeBiquad/DSPLIB_cascadeBiquad_d.c:97-363."""
+
+    size_fn = "DSPLIB_cascadeBiquad_getHandleSize"
+
+    def init(self, args: BiquadInitArgs, pin, pcoef, pvar, pout) -> int:
+        self.args = args
+        return lib().DSPLIB_cascadeBiquad_init(self.h, ctypes.byref(pin), ctypes.byref(pcoef), ctypes.byref(pvar),
+                                               ctypes.byref(pout), ctypes.byref(args))
+
+    def init_check(self, args, pin, pcoef, pvar, pout) -> int:
+        return lib().DSPLIB_cascadeBiquad_init_checkParams(self.h, ctypes.byref(pin), ctypes.byref(pcoef),
+                                                           ctypes.byref(pvar), ctypes.byref(pout), ctypes.byref(args))
+
+    def exec(self, x, coef, state, y) -> int:
+        return lib().DSPLIB_cascadeBiquad_exec(self.h, _ptr(x), _ptr(coef), _ptr(state), _ptr(y))
+
+
+# ------------------------------------------------------------------ helpers
+
+
+def fir_setup(dtype_code, batch, N, T, *, nch, func_style=OPTIMIZED, mma=False, shift=0, in_pitch=None,
+              out_pitch=None, filter_pitch=None):
+    """Descriptors + InitArgs for a FIR call, as the reference driver builds them."""
+    elt = _elt(dtype_code)
+    args = FirInitArgs(funcStyle=func_style, dataSize=N, batchSize=batch, filterSize=T, shift=shift,
+                       enableNchCoefs=int(nch), enableMMA=int(mma), MMA_SIZE=MMA_SIZE[elt], enableQ=0, Q=0)
+    out_size = N - T + 1
+    pin = bp(dtype_code, N, batch, (in_pitch or N) * elt)
+    pout = bp(dtype_code, (out_pitch or out_size), batch, (out_pitch or out_size) * elt)
+    pfilt = bp(dtype_code, T, batch if nch else 1, (filter_pitch or T) * elt)
+    st = lib().DSPLIB_fir_getSizes(ctypes.byref(args), ctypes.byref(pin), ctypes.byref(pfilt), ctypes.byref(pout))
+    if st != SUCCESS:
+        raise DsplibError("DSPLIB_fir_getSizes", st)
+    return args, pin, pfilt, pout
+
+
+def fir(x, h, T=None, *, nch=None, func_style=OPTIMIZED, precision=FIR_SIMT, qmode=False, shift=0, out=None,
+        handle=None):
+    """y = FIR(x, h) over channel-major rows of ``x`` [batch, N] with stored
+    taps ``h`` [1 or batch, T] (reference tap order).  numpy in -> numpy out
+    (host staging inside the library); torch CUDA in -> torch CUDA out."""
+    batch, N = x.shape
+    T = T or h.shape[1]
+    if nch is None:
+        nch = h.shape[0] > 1
+    code = _dtype_code(x)
+    args, pin, pfilt, pout = fir_setup(code, batch, N, T, nch=nch, func_style=func_style, shift=shift)
+    out_size = N - T + 1
+    if out is None:
+        if isinstance(x, np.ndarray):
+            out = np.zeros((batch, out_size), dtype=x.dtype)
+        else:
+            import torch
+
+            out = torch.zeros((batch, out_size), dtype=x.dtype, device=x.device)
+    hd = handle or FirHandle()
+    hd._check("DSPLIB_fir_init", hd.init(args, pin, pfilt, pout))
+    hd.set_precision(precision)
+    hd.set_qmode(qmode)
+    hd._check("DSPLIB_fir_exec", hd.exec(x, h, out))
+    return out
+
+
+def biquad_descs(C, N, S, form, nch, *, pitch=None, var_pitch=None, func_style=OPTIMIZED):
+    nv = 4 if form == DF1 else 2
+    pin = bp(FLOAT32, C, N, (pitch or C) * 4)
+    pout = bp(FLOAT32, C, N, (pitch or C) * 4)
+    pvar = bp(FLOAT32, C, S * nv, (var_pitch or C) * 4)
+    pcn = bp(FLOAT32, S * 5, C if nch else 1, S * 5 * 4)
+    popt = BufParams2D()
+    st = lib().DSPLIB_cascadeBiquad_get_coefficientsBufferDesc(FLOAT32, S, C, form, int(nch), ctypes.byref(popt))
+    if st != SUCCESS:
+        raise DsplibError("get_coefficientsBufferDesc", st)
+    args = BiquadInitArgs(funcStyle=func_style, dataSize=N, numStages=S, numChannels=C, enableNChCoeffs=int(nch),
+                          biquadForm=form)
+    return args, pin, pout, pvar, pcn, popt
+
+
+def opt_coefficients(natural, form, nch, C):
+    """Natural [rows, S*5] float32 -> the optimized buffer get_coefficients makes (numpy)."""
+    natural = np.ascontiguousarray(natural, dtype=np.float32)
+    S = natural.shape[1] // 5
+    pcn = bp(FLOAT32, S * 5, C if nch else 1, S * 5 * 4)
+    popt = BufParams2D()
+    lib().DSPLIB_cascadeBiquad_get_coefficientsBufferDesc(FLOAT32, S, C, form, int(nch), ctypes.byref(popt))
+    if form != TIF and not nch:
+        return natural.copy(), popt
+    opt = np.zeros(popt.dim_y * popt.stride_y // 4, dtype=np.float32)
+    st = lib().DSPLIB_cascadeBiquad_get_coefficients(form, int(nch), ctypes.byref(pcn), ctypes.byref(popt),
+                                                     natural.ctypes.data, opt.ctypes.data)
+    if st != SUCCESS:
+        raise DsplibError("get_coefficients", st)
+    return opt, popt
+
+
+def cascade_biquad(x, coef, state, *, form, nch, func_style=OPTIMIZED, out=None, handle=None):
+    """One exec over time-major ``x`` [N, C].  ``coef`` is the natural buffer
+    for NATC and the optimized buffer (``opt_coefficients``) for OPTIMIZED;
+    ``state`` [S*nv, C] is updated in place."""
+    N, C = x.shape
+    nv = 4 if form == DF1 else 2
+    S = state.shape[0] // nv
+    args, pin, pout, pvar, pcn, popt = biquad_descs(C, N, S, form, nch, pitch=x.shape[1],
+                                                    var_pitch=state.shape[1], func_style=func_style)
+    if out is None:
+        if isinstance(x, np.ndarray):
+            out = np.zeros_like(x)
+        else:
+            import torch
+
+            out = torch.zeros_like(x)
+    hd = handle or BiquadHandle()
+    hd._check("DSPLIB_cascadeBiquad_init", hd.init(args, pin, pcn if func_style == NATC else popt, pvar, pout))
+    hd._check("DSPLIB_cascadeBiquad_exec", hd.exec(x, coef, state, out))
+    return out
+
+
+def kernel_launch_count() -> int:
+    return int(lib().DSPLIB_gpu_kernelLaunchCount())

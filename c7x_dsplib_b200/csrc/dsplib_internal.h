@@ -1,0 +1,127 @@
+// Internal declarations of the B200 DSPLIB library: handle layouts, the
+// device-buffer staging helpers and the kernel launchers that the C-ABI entry
+// points (fir_api.cpp, biquad_api.cpp) call.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+
+#include "dsplib.h"
+
+namespace dsplib {
+
+constexpr uint32_t kMagicFir = 0xF1A0B200u;
+constexpr uint32_t kMagicBiquad = 0xB1A0B200u;
+
+// First member of every handle: GPU settings that survive re-init
+// (the reference test drivers re-run init on the same handle to switch
+// NATC <-> OPTIMIZED, test/DSPLIB_fir/DSPLIB_fir_d.c:291-297).
+struct HandleCommon {
+   uint32_t magic;
+   int32_t async;
+   cudaStream_t stream;
+   int32_t firPrecision;
+   int32_t firQMode;
+   char err[200];
+};
+
+struct FirPriv {
+   HandleCommon common;
+   DSPLIB_fir_InitArgs initArgs;
+   int32_t dtype;
+   int32_t elt;
+   int32_t inPitch;     // elements, bufParamsIn->stride_y / elt (DSPLIB_fir.cpp:153)
+   int32_t outPitch;    // elements (DSPLIB_fir.cpp:154)
+   int32_t filterPitch; // elements (DSPLIB_fir.cpp:156)
+   int32_t outputSize;  // bufParamsOut->dim_x (DSPLIB_fir.cpp:155)
+   int32_t initialized;
+};
+
+struct BiquadPriv {
+   HandleCommon common;
+   DSPLIB_cascadeBiquad_InitArgs initArgs;
+   int32_t inPitch;   // elements (DSPLIB_cascadeBiquad.cpp:450)
+   int32_t outPitch;  // elements (:451)
+   int32_t varPitch;  // elements (:452)
+   int32_t coefPitch; // elements between channel-interleaved coefficient rows (OPT, per-channel)
+   int32_t coefRows;  // rows of the coefficient buffer passed to init
+   int32_t coefCols;  // elements per coefficient row
+   int32_t initialized;
+};
+
+// ---------------------------------------------------------------- runtime
+
+void setError(HandleCommon *h, const char *fmt, ...);
+DSPLIB_STATUS cudaFail(HandleCommon *h, cudaError_t e, const char *what);
+void countLaunch(int n = 1);
+
+// True when p is device-accessible global memory (device or managed allocation).
+bool isDevicePtr(const void *p);
+
+// Per-device, per-thread growable scratch used to stage host buffers.
+// Returns nullptr on allocation failure.
+void *stagingBuffer(int slot, size_t bytes);
+
+// A strided 2-D region of a caller buffer: rows of width bytes, pitch bytes apart.
+struct Region {
+   void *host;        // caller pointer
+   void *dev;         // device pointer the kernel uses
+   size_t width;      // bytes per row that the kernel touches
+   size_t height;     // rows
+   size_t pitch;      // bytes between rows
+   bool staged;       // host buffer copied through a staging buffer
+   size_t bytes() const { return height ? (height - 1) * pitch + width : 0; }
+};
+
+// Prepare a region: device pointers are used in place, host pointers are
+// staged (copied in when copyIn).  Returns cudaSuccess or the failure.
+cudaError_t regionIn(Region &r, int slot, bool copyIn, cudaStream_t s);
+// Copy a staged region back to the caller's host buffer (row by row, leaving
+// the bytes between rows untouched).
+cudaError_t regionOut(const Region &r, cudaStream_t s);
+
+// ---------------------------------------------------------------- kernels
+
+struct FirLaunch {
+   const void *x;
+   const void *h; // first tap row (already offset past any MMA padding)
+   void *y;
+   int dtype;
+   int batch;
+   int T;
+   int outSize;
+   long long inPitch;   // elements
+   long long outPitch;  // elements
+   long long filtPitch; // elements between tap rows, 0 = shared
+   int shift;
+};
+
+enum FirKernelKind {
+   FIR_NATC = 0,      // bit-exact natural-C semantics (wrap / sequential float)
+   FIR_QMODE = 1,     // exact accumulator, round/shift/saturate
+   FIR_F32_SIMT = 2,  // FP32 FMA register-tiled CUDA-core kernel
+   FIR_F32_BF16X3 = 3 // tcgen05 split-BF16x3 tensor-core kernel
+};
+
+cudaError_t launchFir(const FirLaunch &a, FirKernelKind kind, cudaStream_t s);
+
+struct BiquadLaunch {
+   const float *x;
+   float *y;
+   float *state;
+   const float *coef;
+   int form;     // DSPLIB_biquadForm (TIF only with optLayout)
+   int nch;      // per-channel coefficients
+   int optLayout; // 1: coefficients in the get_coefficients layout
+   int N, C, S;
+   long long inPitch, outPitch, varPitch, coefPitch; // elements
+};
+
+// NATC: sequential recursion per channel, bit-exact to the reference _cn kernels.
+cudaError_t launchBiquadSequential(const BiquadLaunch &a, cudaStream_t s);
+// OPTIMIZED: chunked parallel-in-time scan.
+cudaError_t launchBiquadScan(const BiquadLaunch &a, cudaStream_t s);
+
+} // namespace dsplib

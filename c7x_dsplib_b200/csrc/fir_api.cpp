@@ -1,0 +1,233 @@
+// DSPLIB_fir C-ABI entry points (drop-in for src/DSPLIB_fir/DSPLIB_fir.cpp and
+// the getSizes part of DSPLIB_fir_ci.cpp).  Parameter handling mirrors the
+// reference line by line where callers can observe it (status codes, computed
+// sizes and pitches); exec launches CUDA kernels instead of C7x code.
+#include <cstring>
+
+#include "dsplib_internal.h"
+
+using namespace dsplib;
+
+namespace {
+
+bool firTypeKnown(uint32_t t)
+{
+   return t == DSPLIB_INT16 || t == DSPLIB_INT32 || t == DSPLIB_INT8 || t == DSPLIB_FLOAT32;
+}
+
+// DSPLIB_fir_ci.cpp:63-103.  Computed in uint32 like the reference, so an
+// oversize filter wraps the output length the same way.
+void firSizes(const DSPLIB_fir_InitArgs *a, int32_t elt, DSPLIB_bufParams2D_t *filt, DSPLIB_bufParams2D_t *out)
+{
+   uint32_t dataSize = (uint32_t) a->dataSize;
+   uint32_t filterSize = (uint32_t) a->filterSize;
+   uint32_t mma = (uint32_t) a->MMA_SIZE;
+   out->dim_x = dataSize - filterSize + 1;
+   filt->dim_y = (a->enableNchCoefs == 0) ? 1 : (uint32_t) a->batchSize;
+   if (a->enableMMA) {
+      filt->dim_x = 2 * mma + filterSize + mma - 1;
+      filt->stride_y = (int32_t) (filt->dim_x * (uint32_t) elt);
+   }
+}
+
+FirPriv *firHandle(DSPLIB_kernelHandle h)
+{
+   FirPriv *p = (FirPriv *) h;
+   if (!p || p->common.magic != kMagicFir || !p->initialized) return nullptr;
+   return p;
+}
+
+} // namespace
+
+extern "C" {
+
+int32_t DSPLIB_fir_getHandleSize(DSPLIB_fir_InitArgs *pKerInitArgs)
+{
+   (void) pKerInitArgs;
+   return (int32_t) sizeof(FirPriv);
+}
+
+DSPLIB_STATUS DSPLIB_fir_getSizes(const DSPLIB_fir_InitArgs *pKerInitArgs,
+                                  DSPLIB_bufParams2D_t *bufParamsIn,
+                                  DSPLIB_bufParams2D_t *bufParamsFilter,
+                                  DSPLIB_bufParams2D_t *bufParamsOut)
+{
+   if (!firTypeKnown(bufParamsIn->data_type)) return DSPLIB_ERR_NOT_IMPLEMENTED; // DSPLIB_fir.cpp:93-95
+   firSizes(pKerInitArgs, DSPLIB_sizeof(bufParamsIn->data_type), bufParamsFilter, bufParamsOut);
+   return DSPLIB_SUCCESS;
+}
+
+DSPLIB_STATUS DSPLIB_fir_init_checkParams(DSPLIB_kernelHandle handle,
+                                          const DSPLIB_bufParams2D_t *bufParamsIn,
+                                          const DSPLIB_bufParams2D_t *bufParamsFilter,
+                                          const DSPLIB_bufParams2D_t *bufParamsOut,
+                                          const DSPLIB_fir_InitArgs *pKerInitArgs)
+{
+   (void) pKerInitArgs;
+   // DSPLIB_fir.cpp:27-66
+   if (handle == NULL) return DSPLIB_ERR_NULL_POINTER;
+   if (!firTypeKnown(bufParamsIn->data_type)) return DSPLIB_ERR_INVALID_TYPE;
+   if (bufParamsIn->data_type != bufParamsOut->data_type) return DSPLIB_ERR_INVALID_TYPE;
+   if (bufParamsIn->data_type != bufParamsFilter->data_type) return DSPLIB_ERR_INVALID_TYPE;
+   if (bufParamsIn->data_type != DSPLIB_FLOAT32) return DSPLIB_ERR_INVALID_TYPE;
+   return DSPLIB_SUCCESS;
+}
+
+DSPLIB_STATUS DSPLIB_fir_exec_checkParams(DSPLIB_kernelHandle handle,
+                                          const void *pIn,
+                                          const void *pFilter,
+                                          const void *pOut)
+{
+   (void) handle;
+   if (pIn == NULL || pFilter == NULL || pOut == NULL) return DSPLIB_ERR_NULL_POINTER; // DSPLIB_fir.cpp:110-115
+   return DSPLIB_SUCCESS;
+}
+
+DSPLIB_STATUS DSPLIB_fir_init(DSPLIB_kernelHandle handle,
+                              DSPLIB_bufParams2D_t *bufParamsIn,
+                              DSPLIB_bufParams2D_t *bufParamsFilter,
+                              DSPLIB_bufParams2D_t *bufParamsOut,
+                              DSPLIB_fir_InitArgs *pKerInitArgs)
+{
+   if (handle == NULL || pKerInitArgs == NULL || bufParamsIn == NULL) return DSPLIB_ERR_NULL_POINTER;
+   FirPriv *p = (FirPriv *) handle;
+   if (p->common.magic != kMagicFir) {
+      std::memset(&p->common, 0, sizeof(p->common));
+      p->common.magic = kMagicFir;
+   }
+   p->common.err[0] = 0;
+   p->initArgs = *pKerInitArgs;
+   p->initialized = 0;
+   p->dtype = (int32_t) bufParamsIn->data_type;
+
+   // DSPLIB_fir.cpp:134-157
+   int32_t elt = 0;
+   DSPLIB_STATUS status = DSPLIB_SUCCESS;
+   switch (bufParamsIn->data_type) {
+   case DSPLIB_FLOAT32:
+   case DSPLIB_INT32:
+   case DSPLIB_UINT32: elt = 4; break;
+   case DSPLIB_INT16:
+   case DSPLIB_UINT16: elt = 2; break;
+   case DSPLIB_INT8:
+   case DSPLIB_UINT8: elt = 1; break;
+   default: status = DSPLIB_ERR_INVALID_TYPE; break;
+   }
+   p->elt = elt;
+   if (elt != 0) {
+      p->inPitch = bufParamsIn->stride_y / elt;
+      p->outPitch = bufParamsOut->stride_y / elt;
+      p->outputSize = (int32_t) bufParamsOut->dim_x;
+      p->filterPitch = bufParamsFilter->stride_y / elt;
+   }
+   // DSPLIB_fir.cpp:159-196: both styles accept exactly INT8/INT16/INT32/FLOAT32.
+   if (elt == 0 || !firTypeKnown(bufParamsIn->data_type)) return DSPLIB_ERR_INVALID_TYPE;
+   if (pKerInitArgs->funcStyle != DSPLIB_FUNCTION_NATC && pKerInitArgs->funcStyle != DSPLIB_FUNCTION_OPTIMIZED) {
+      // The reference treats every non-NATC style as OPTIMIZED (DSPLIB_fir.cpp:177).
+      p->initArgs.funcStyle = DSPLIB_FUNCTION_OPTIMIZED;
+   }
+   p->initialized = 1;
+   return status;
+}
+
+DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilter, void *pOut)
+{
+   FirPriv *p = firHandle(handle);
+   if (!p) return DSPLIB_ERR_FAILURE;
+   HandleCommon *hc = &p->common;
+   if (pIn == NULL || pFilter == NULL || pOut == NULL) {
+      setError(hc, "exec: null buffer");
+      return DSPLIB_ERR_NULL_POINTER;
+   }
+   const DSPLIB_fir_InitArgs &ia = p->initArgs;
+   const int elt = p->elt;
+   const int T = ia.filterSize;
+   const int batch = ia.batchSize;
+   const int outSize = p->outputSize;
+   if (batch <= 0 || outSize <= 0) return DSPLIB_SUCCESS; // nothing to compute (reference loops run zero times)
+   const bool natc = ia.funcStyle == DSPLIB_FUNCTION_NATC;
+   const bool nch = ia.enableNchCoefs != 0;
+   const long long M = ia.MMA_SIZE;
+
+   // Tap rows.  NATC follows DSPLIB_fir_cn.cpp:50-52 (the caller passes the
+   // first tap; MMA rows are 3*M + T - 1 apart).  OPTIMIZED follows the _ci
+   // path: the caller passes the padded buffer, taps start 2*M elements in,
+   // rows are stride_y apart (DSPLIB_fir_d.c:195-208, DSPLIB_fir_ci.cpp:283).
+   long long tapOffset = 0, filtPitch = 0;
+   if (natc) {
+      filtPitch = nch ? (ia.enableMMA ? (3 * M + T - 1) : T) : 0;
+   }
+   else {
+      tapOffset = ia.enableMMA ? 2 * M : 0;
+      filtPitch = nch ? p->filterPitch : 0;
+   }
+   if (T < 0 || p->inPitch <= 0 || p->outPitch <= 0 || (nch && filtPitch < T) || tapOffset < 0) {
+      setError(hc, "exec: inconsistent sizes (T=%d inPitch=%d outPitch=%d filterPitch=%lld)", T, p->inPitch,
+               p->outPitch, filtPitch);
+      return DSPLIB_ERR_INVALID_DIMENSION;
+   }
+
+   FirKernelKind kind;
+   if (natc) kind = FIR_NATC;
+   else if (p->dtype == DSPLIB_FLOAT32)
+      kind = hc->firPrecision == DSPLIB_GPU_FIR_BF16X3 ? FIR_F32_BF16X3 : FIR_F32_SIMT;
+   else kind = hc->firQMode ? FIR_QMODE : FIR_NATC;
+
+   cudaStream_t s = hc->stream;
+   Region rin{pIn, nullptr, (size_t) (outSize + (T > 0 ? T : 1) - 1) * elt, (size_t) batch,
+              (size_t) p->inPitch * elt, false};
+   Region rf{(char *) pFilter + tapOffset * elt, nullptr, (size_t) (T > 0 ? T : 1) * elt, (size_t) (nch ? batch : 1),
+             (size_t) (nch ? filtPitch : (T > 0 ? T : 1)) * elt, false};
+   Region rout{pOut, nullptr, (size_t) outSize * elt, (size_t) batch, (size_t) p->outPitch * elt, false};
+   cudaError_t e;
+   if ((e = regionIn(rin, 0, true, s)) != cudaSuccess) return cudaFail(hc, e, "stage input");
+   if ((e = regionIn(rf, 1, true, s)) != cudaSuccess) return cudaFail(hc, e, "stage filter");
+   if ((e = regionIn(rout, 2, false, s)) != cudaSuccess) return cudaFail(hc, e, "stage output");
+
+   FirLaunch a;
+   a.x = rin.dev;
+   a.h = rf.dev;
+   a.y = rout.dev;
+   a.dtype = p->dtype;
+   a.batch = batch;
+   a.T = T;
+   a.outSize = outSize;
+   a.inPitch = p->inPitch;
+   a.outPitch = p->outPitch;
+   a.filtPitch = nch ? filtPitch : 0; // staging keeps the caller's row pitch
+   a.shift = (int) ia.shift;
+   if ((e = launchFir(a, kind, s)) != cudaSuccess) return cudaFail(hc, e, "FIR kernel launch");
+   if ((e = regionOut(rout, s)) != cudaSuccess) return cudaFail(hc, e, "copy output");
+   if (!hc->async || rin.staged || rf.staged || rout.staged) {
+      if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, "FIR execution");
+   }
+   return DSPLIB_SUCCESS;
+}
+
+void DSPLIB_fir_perfEst(DSPLIB_kernelHandle handle,
+                        const DSPLIB_bufParams2D_t *bufParamsIn,
+                        const DSPLIB_bufParams2D_t *bufParamsFilter,
+                        const DSPLIB_bufParams2D_t *bufParamsOut,
+                        uint64_t *archCycles,
+                        uint64_t *estCycles)
+{
+   (void) bufParamsIn;
+   (void) bufParamsFilter;
+   (void) bufParamsOut;
+   FirPriv *p = firHandle(handle);
+   if (!p) return;
+   // Roofline estimate in nanoseconds on a B200: HBM 6.5 TB/s; FP32 FMA
+   // 70 TFLOP/s (SIMT), split-BF16x3 1.6 PFLOP/s / 3 products.
+   double outs = (double) p->outputSize * p->initArgs.batchSize;
+   double bytes = (double) p->elt * (outs + (double) p->initArgs.batchSize * p->initArgs.dataSize);
+   double flops = 2.0 * p->initArgs.filterSize * outs;
+   double peak = 70e12;
+   if (p->dtype == DSPLIB_FLOAT32 && p->common.firPrecision == DSPLIB_GPU_FIR_BF16X3) peak = 1.6e15 / 3.0;
+   if (p->initArgs.funcStyle == DSPLIB_FUNCTION_NATC) peak = 35e12;
+   double t = bytes / 6.5e12;
+   if (flops / peak > t) t = flops / peak;
+   if (archCycles) *archCycles = (uint64_t) (t * 1e9);
+   if (estCycles) *estCycles = (uint64_t) (t * 1e9) + 4000; // + launch and sync
+}
+
+} // extern "C"

@@ -1,0 +1,154 @@
+// Runtime plumbing shared by the FIR and biquad entry points: error text on the
+// handle, device/host pointer classification, staging of host buffers through
+// per-thread device scratch, and the DSPLIB_gpu_* extension functions.
+#include <atomic>
+#include <cstdarg>
+#include <cstring>
+
+#include "dsplib_internal.h"
+
+namespace dsplib {
+
+static std::atomic<int64_t> g_launches{0};
+
+void countLaunch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void setError(HandleCommon *h, const char *fmt, ...)
+{
+   if (!h) return;
+   va_list ap;
+   va_start(ap, fmt);
+   vsnprintf(h->err, sizeof(h->err), fmt, ap);
+   va_end(ap);
+}
+
+DSPLIB_STATUS cudaFail(HandleCommon *h, cudaError_t e, const char *what)
+{
+   setError(h, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+   return DSPLIB_ERR_FAILURE;
+}
+
+bool isDevicePtr(const void *p)
+{
+   cudaPointerAttributes attr;
+   cudaError_t e = cudaPointerGetAttributes(&attr, p);
+   if (e != cudaSuccess) {
+      (void) cudaGetLastError();
+      return false;
+   }
+   return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+namespace {
+constexpr int kMaxDevices = 16;
+constexpr int kSlots = 6;
+struct Scratch {
+   void *ptr[kMaxDevices][kSlots] = {};
+   size_t cap[kMaxDevices][kSlots] = {};
+};
+thread_local Scratch t_scratch;
+} // namespace
+
+void *stagingBuffer(int slot, size_t bytes)
+{
+   int dev = 0;
+   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices || slot < 0 || slot >= kSlots)
+      return nullptr;
+   if (bytes == 0) bytes = 16;
+   if (t_scratch.cap[dev][slot] < bytes) {
+      if (t_scratch.ptr[dev][slot]) cudaFree(t_scratch.ptr[dev][slot]);
+      t_scratch.ptr[dev][slot] = nullptr;
+      t_scratch.cap[dev][slot] = 0;
+      size_t want = bytes + bytes / 4; // grow with headroom
+      void *p = nullptr;
+      if (cudaMalloc(&p, want) != cudaSuccess) {
+         (void) cudaGetLastError();
+         return nullptr;
+      }
+      t_scratch.ptr[dev][slot] = p;
+      t_scratch.cap[dev][slot] = want;
+   }
+   return t_scratch.ptr[dev][slot];
+}
+
+cudaError_t regionIn(Region &r, int slot, bool copyIn, cudaStream_t s)
+{
+   r.staged = false;
+   r.dev = r.host;
+   if (r.height == 0 || r.width == 0) return cudaSuccess;
+   if (isDevicePtr(r.host)) return cudaSuccess;
+   void *buf = stagingBuffer(slot, r.bytes());
+   if (!buf) return cudaErrorMemoryAllocation;
+   r.dev = buf;
+   r.staged = true;
+   if (!copyIn) return cudaSuccess;
+   if (r.pitch <= r.width || r.height == 1)
+      return cudaMemcpyAsync(buf, r.host, r.bytes(), cudaMemcpyHostToDevice, s);
+   return cudaMemcpy2DAsync(buf, r.pitch, r.host, r.pitch, r.width, r.height, cudaMemcpyHostToDevice, s);
+}
+
+cudaError_t regionOut(const Region &r, cudaStream_t s)
+{
+   if (!r.staged || r.height == 0 || r.width == 0) return cudaSuccess;
+   if (r.pitch <= r.width || r.height == 1)
+      return cudaMemcpyAsync(r.host, r.dev, r.bytes(), cudaMemcpyDeviceToHost, s);
+   return cudaMemcpy2DAsync(r.host, r.pitch, r.dev, r.pitch, r.width, r.height, cudaMemcpyDeviceToHost, s);
+}
+
+static HandleCommon *common(DSPLIB_kernelHandle h)
+{
+   if (!h) return nullptr;
+   HandleCommon *c = (HandleCommon *) h;
+   if (c->magic != kMagicFir && c->magic != kMagicBiquad) return nullptr;
+   return c;
+}
+
+} // namespace dsplib
+
+using namespace dsplib;
+
+extern "C" {
+
+DSPLIB_STATUS DSPLIB_gpu_setStream(DSPLIB_kernelHandle handle, void *stream)
+{
+   HandleCommon *c = common(handle);
+   if (!c) return DSPLIB_ERR_NULL_POINTER;
+   c->stream = (cudaStream_t) stream;
+   return DSPLIB_SUCCESS;
+}
+
+DSPLIB_STATUS DSPLIB_gpu_setAsync(DSPLIB_kernelHandle handle, int32_t async)
+{
+   HandleCommon *c = common(handle);
+   if (!c) return DSPLIB_ERR_NULL_POINTER;
+   c->async = async ? 1 : 0;
+   return DSPLIB_SUCCESS;
+}
+
+const char *DSPLIB_gpu_lastError(DSPLIB_kernelHandle handle)
+{
+   HandleCommon *c = common(handle);
+   if (!c) return "invalid or uninitialised handle";
+   return c->err;
+}
+
+DSPLIB_STATUS DSPLIB_gpu_firSetPrecision(DSPLIB_kernelHandle handle, int32_t precision)
+{
+   HandleCommon *c = common(handle);
+   if (!c || c->magic != kMagicFir) return DSPLIB_ERR_NULL_POINTER;
+   if (precision != DSPLIB_GPU_FIR_SIMT && precision != DSPLIB_GPU_FIR_BF16X3) return DSPLIB_ERR_INVALID_VALUE;
+   c->firPrecision = precision;
+   return DSPLIB_SUCCESS;
+}
+
+DSPLIB_STATUS DSPLIB_gpu_firSetQMode(DSPLIB_kernelHandle handle, int32_t enable)
+{
+   HandleCommon *c = common(handle);
+   if (!c || c->magic != kMagicFir) return DSPLIB_ERR_NULL_POINTER;
+   c->firQMode = enable ? 1 : 0;
+   return DSPLIB_SUCCESS;
+}
+
+int64_t DSPLIB_gpu_kernelLaunchCount(void) { return g_launches.load(); }
+
+} // extern "C"

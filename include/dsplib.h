@@ -1,0 +1,11 @@
+/* Umbrella header, as src/dsplib.h of the reference (:19 biquad, :28 FIR). */
+#ifndef DSPLIB_H_
+#define DSPLIB_H_
+
+#include "DSPLIB_types.h"
+#include "DSPLIB_bufParams.h"
+#include "DSPLIB_cascadeBiquad.h"
+#include "DSPLIB_fir.h"
+#include "dsplib_gpu.h"
+
+#endif

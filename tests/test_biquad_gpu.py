@@ -1,0 +1,240 @@
+"""Cascade-biquad parity on the GPU, through the C ABI, against the CPU oracle.
+
+NATC is bit-exact to the reference natural-C kernels (outputs and final
+states).  OPTIMIZED (chunked parallel-in-time scan) is checked against the
+FP64 oracle: max |y - y64| / max |y64| <= 1e-4 per channel, and against the
+reference test criterion abs 2^-10 (test/DSPLIB_cascadeBiquad/
+DSPLIB_cascadeBiquad_d.c:391-405); final states to the same bounds.
+"""
+import numpy as np
+import pytest
+
+import c7x_dsplib_b200 as D
+import oracle
+from conftest import case_keys
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+TOL_REF = 2.0 ** -10
+REL = 1e-4
+FORMS = [D.DF1, D.DF2, D.TDF2, D.TIF]
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+def stable_sections(rng, rows, S, rmax=0.95):
+    """Natural [rows, S*5]: conjugate poles r in [0.5, rmax], zeros on the unit circle."""
+    r = rng.uniform(0.5, rmax, size=(rows, S))
+    th = rng.uniform(0, np.pi, size=(rows, S))
+    ph = rng.uniform(0, np.pi, size=(rows, S))
+    a1, a2 = -2 * r * np.cos(th), r * r
+    b0 = rng.uniform(0.3, 1.2, size=(rows, S))
+    c = np.stack([b0, -2 * np.cos(ph) * b0, b0, a1, a2], axis=-1)
+    return c.reshape(rows, S * 5).astype(np.float32)
+
+
+def nv(form):
+    return 4 if form == D.DF1 else 2
+
+
+def oracle_run(form, x, nat, state, nch):
+    """fp32 form-exact port (TIF through its own transform) and the FP64 ground truth."""
+    st32 = state.copy()
+    if form == D.TIF:
+        rows = nat.shape[0]
+        tcs, gns = zip(*[oracle.tif_coefficients(nat[r]) for r in range(rows)])
+        y32 = oracle.biquad_tif(x, np.stack(tcs), np.stack(gns), st32, nch=nch)
+    else:
+        y32 = oracle.biquad(form, x, nat, st32, nch=nch)
+    # FP64 truth on the direct form with the same natural coefficients (TIF: DF2 equivalent, zero state)
+    s64 = np.zeros((state.shape[0] * (2 if form == D.DF1 else 1), state.shape[1]), np.float64)
+    if form == D.TIF:
+        s64 = np.zeros((nat.shape[1] // 5 * 2, x.shape[1]), np.float64)
+        y64 = oracle.biquad_f64(D.DF2, x, nat, s64, nch=nch)
+    else:
+        s64 = state.astype(np.float64).copy()
+        y64 = oracle.biquad_f64(form, x, nat, s64, nch=nch)
+    return y32, st32, y64, s64
+
+
+def rel_per_channel(y, y64):
+    return np.max(np.abs(y.astype(np.float64) - y64), axis=0) / np.maximum(np.max(np.abs(y64), axis=0), 1e-6)
+
+
+@pytest.mark.parametrize("form", [D.DF1, D.DF2, D.TDF2])
+@pytest.mark.parametrize("nch", [0, 1])
+@pytest.mark.parametrize("on_device", [False, True])
+def test_natc_bitexact(form, nch, on_device):
+    rng = np.random.default_rng(form * 7 + nch)
+    for (N, C, S) in [(1, 1, 1), (64, 2, 3), (513, 17, 5), (2000, 40, 12)]:
+        x = rng.uniform(-1, 1, size=(N, C)).astype(np.float32)
+        nat = stable_sections(rng, C if nch else 1, S)
+        st = rng.standard_normal((S * nv(form), C)).astype(np.float32) * 0.1
+        s_ref = st.copy()
+        want = oracle.biquad(form, x, nat, s_ref, nch=nch)
+        if on_device:
+            sd = dev(st)
+            got = host(D.cascade_biquad(dev(x), dev(nat), sd, form=form, nch=nch, func_style=D.NATC))
+            st_got = host(sd)
+        else:
+            st_got = st.copy()
+            got = D.cascade_biquad(x, nat, st_got, form=form, nch=nch, func_style=D.NATC)
+        assert np.array_equal(got, want), (N, C, S)
+        assert np.array_equal(st_got, s_ref), (N, C, S)
+
+
+def test_natc_tif_runs_df2():
+    """NATC with biquadForm = TIF runs DF2 on natural coefficients (DSPLIB_cascadeBiquad.cpp:468-471)."""
+    rng = np.random.default_rng(1)
+    x = rng.uniform(-1, 1, size=(300, 8)).astype(np.float32)
+    nat = stable_sections(rng, 1, 3)
+    st = np.zeros((6, 8), np.float32)
+    s_ref = st.copy()
+    got = D.cascade_biquad(x, nat, st, form=D.TIF, nch=0, func_style=D.NATC)
+    assert np.array_equal(got, oracle.biquad(D.DF2, x, nat, s_ref, nch=0))
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference _cn library not built")
+def test_natc_bitexact_vs_reference_cn():
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal((8192, 32)).astype(np.float32)
+    nat = stable_sections(rng, 1, 4)
+    for form in (D.DF1, D.DF2, D.TDF2):
+        st = np.zeros((4 * nv(form), 32), np.float32)
+        s2 = st.copy()
+        got = D.cascade_biquad(dev(x), dev(nat), dev(st), form=form, nch=0, func_style=D.NATC)
+        assert np.array_equal(host(got), oracle.biquad(form, x, nat, s2, nch=0, impl="ref"))
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("nch", [0, 1])
+def test_opt_scan_accuracy(form, nch):
+    rng = np.random.default_rng(100 + form * 3 + nch)
+    for (N, C, S) in [(1, 1, 1), (31, 3, 2), (8192, 32, 4), (40000, 40, 3), (3001, 65, 8), (700, 5, 13)]:
+        x = rng.standard_normal((N, C)).astype(np.float32)
+        nat = stable_sections(rng, C if nch else 1, S)
+        st = np.zeros((S * nv(form), C), np.float32)
+        opt, _ = D.opt_coefficients(nat, form, nch, C)
+        sd = dev(st)
+        y = host(D.cascade_biquad(dev(x), dev(opt), sd, form=form, nch=nch))
+        y32, st32, y64, _ = oracle_run(form, x, nat, st, nch)
+        assert np.max(rel_per_channel(y, y64)) <= REL, (N, C, S)
+        assert np.max(np.abs(y - y32)) <= TOL_REF, (N, C, S)
+        sc = np.max(np.abs(st32)) + 1e-3
+        assert np.max(np.abs(host(sd) - st32)) <= REL * max(1.0, sc) * 10, (N, C, S)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_opt_streaming_state_carry(form):
+    """numExecReps-style streaming (DSPLIB_cascadeBiquad_d.c:260-273): four exec calls
+    on consecutive blocks equal one call on the whole signal."""
+    rng = np.random.default_rng(form)
+    N, C, S = 5000, 12, 4
+    x = rng.standard_normal((4 * N, C)).astype(np.float32)
+    nat = stable_sections(rng, 1, S)
+    opt, _ = D.opt_coefficients(nat, form, 0, C)
+    st = dev(np.zeros((S * nv(form), C), np.float32))
+    h = D.BiquadHandle()
+    parts = []
+    for k in range(4):
+        parts.append(host(D.cascade_biquad(dev(x[k * N:(k + 1) * N]), dev(opt), st, form=form, nch=0, handle=h)))
+    y = np.concatenate(parts)
+    _, st32, y64, _ = oracle_run(form, x, nat, np.zeros((S * nv(form), C), np.float32), 0)
+    assert np.max(rel_per_channel(y, y64)) <= REL
+    assert np.max(np.abs(host(st) - st32)) <= 1e-3
+
+
+def test_opt_nonzero_initial_state():
+    rng = np.random.default_rng(77)
+    for form in (D.DF1, D.DF2, D.TDF2):
+        N, C, S = 3000, 33, 3
+        x = rng.standard_normal((N, C)).astype(np.float32)
+        nat = stable_sections(rng, C, S)
+        st = (rng.standard_normal((S * nv(form), C)) * 0.5).astype(np.float32)
+        opt, _ = D.opt_coefficients(nat, form, 1, C)
+        sd = dev(st)
+        y = host(D.cascade_biquad(dev(x), dev(opt), sd, form=form, nch=1))
+        s_ref = st.copy()
+        want = oracle.biquad(form, x, nat, s_ref, nch=1)
+        s64 = st.astype(np.float64)
+        y64 = oracle.biquad_f64(form, x, nat, s64, nch=1)
+        assert np.max(rel_per_channel(y, y64)) <= REL
+        assert np.max(np.abs(y - want)) <= TOL_REF
+        assert np.max(np.abs(host(sd) - s64)) <= 1e-3
+
+
+def test_opt_in_place():
+    rng = np.random.default_rng(3)
+    N, C, S = 10000, 32, 4
+    x = rng.standard_normal((N, C)).astype(np.float32)
+    nat = stable_sections(rng, 1, S)
+    opt, _ = D.opt_coefficients(nat, D.DF2, 0, C)
+    xd = dev(x)
+    D.cascade_biquad(xd, dev(opt), dev(np.zeros((2 * S, C), np.float32)), form=D.DF2, nch=0, out=xd)
+    _, _, y64, _ = oracle_run(D.DF2, x, nat, np.zeros((2 * S, C), np.float32), 0)
+    assert np.max(rel_per_channel(host(xd), y64)) <= REL
+
+
+def test_opt_deep_cascade_uses_sequential_kernel():
+    rng = np.random.default_rng(6)
+    N, C, S = 500, 9, 20  # DF1 beyond the scan kernel's stage limit
+    x = rng.standard_normal((N, C)).astype(np.float32)
+    nat = stable_sections(rng, 1, S, rmax=0.7)
+    st = np.zeros((4 * S, C), np.float32)
+    y = host(D.cascade_biquad(dev(x), dev(nat), dev(st), form=D.DF1, nch=0))
+    s_ref = st.copy()
+    assert np.array_equal(y, oracle.biquad(D.DF1, x, nat, s_ref, nch=0))
+
+
+def _golden_cases():
+    import os
+
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "biquad_golden.npz"))
+    return case_keys(d, "b")
+
+
+@pytest.mark.parametrize("key", _golden_cases())
+@pytest.mark.parametrize("style", [D.NATC, D.OPTIMIZED])
+def test_reference_flow_golden(golden_biquad, key, style):
+    """Reference driver flow (DSPLIB_cascadeBiquad_d.c:97-405): pitched buffers,
+    get_coefficients for OPTIMIZED, numExecReps consecutive exec calls carrying
+    the state; outputs against the reference golden at abs 2^-10."""
+    meta = golden_biquad[key + "_meta"]
+    cid, form, nch, N, C, S, reps, pitch_b, var_b = (int(v) for v in meta)
+    pitch, var_pitch = pitch_b // 4, var_b // 4
+    x = golden_biquad[key + "_x"]
+    nat = golden_biquad[key + "_coef"]
+    args, pin, pout, pvar, pcn, popt = D.biquad_descs(C, N, S, form, nch, pitch=pitch, var_pitch=var_pitch,
+                                                      func_style=style)
+    coef = nat if style == D.NATC else D.opt_coefficients(nat, form, nch, C)[0]
+    xin = np.zeros((reps * N, pitch), np.float32)
+    xin[:, :C] = x
+    out = np.zeros_like(xin)
+    state = np.zeros((S * nv(form if style == D.OPTIMIZED else (D.DF2 if form == D.TIF else form)), var_pitch),
+                     np.float32)
+    h = D.BiquadHandle()
+    assert h.init_check(args, pin, pcn if style == D.NATC else popt, pvar, pout) == D.SUCCESS
+    assert h.init(args, pin, pcn if style == D.NATC else popt, pvar, pout) == D.SUCCESS
+    xd, od, sd, cd = dev(xin), dev(out), dev(state), dev(coef)
+    for r in range(reps):
+        st = D.lib().DSPLIB_cascadeBiquad_exec(h.h, xd.data_ptr() + r * N * pitch * 4, cd.data_ptr(),
+                                                sd.data_ptr(), od.data_ptr() + r * N * pitch * 4)
+        assert st == D.SUCCESS, h.last_error()
+    y = host(od)[:, :C]
+    assert np.max(np.abs(y - golden_biquad[key + "_y64"])) <= TOL_REF
+    if style == D.NATC:
+        f = D.DF2 if form == D.TIF else form
+        s_ref = np.zeros((S * nv(f), C), np.float32)
+        assert np.array_equal(y, oracle.biquad(f, x, nat, s_ref, nch=nch))
+        assert np.array_equal(host(sd)[:, :C], s_ref)
+    elif form == D.TDF2:  # TDF2 states coincide with scipy's sosfilt zf
+        zf = golden_biquad[key + "_zf64"].reshape(S * 2, C)
+        assert np.max(np.abs(host(sd)[:, :C] - zf)) <= TOL_REF
