@@ -156,116 +156,63 @@ template <int FORM> __global__ void __launch_bounds__(128) biquad_seq_kernel(Biq
 
 // ------------------------------------------------------------ scan
 
-template <int FORM> struct Form {
-   static constexpr int D = FORM == DSPLIB_BIQUAD_DF1 ? 4 : 2;
+// 2x2 matrix [[a, b], [c, d]] in FP64.
+struct M2 {
+   double a, b, c, d;
 };
 
-// One-sample state transition (zero input) of each form, as a D x D matrix
-// (row-major): state' = A * state.
-template <int FORM> __device__ void transition(const Coef &c, double *A)
+__device__ __forceinline__ M2 mmul(const M2 &x, const M2 &y)
 {
-   if (FORM == DSPLIB_BIQUAD_DF2) { // (w1, w2): w1' = -a1 w1 - a2 w2, w2' = w1
-      A[0] = -(double) c.k[3];
-      A[1] = -(double) c.k[4];
-      A[2] = 1.0;
-      A[3] = 0.0;
-   }
-   else if (FORM == DSPLIB_BIQUAD_TDF2) { // (w1, w2): y = w1; w1' = w2 - a1 y; w2' = -a2 y
-      A[0] = -(double) c.k[3];
-      A[1] = 1.0;
-      A[2] = -(double) c.k[4];
-      A[3] = 0.0;
-   }
-   else if (FORM == DSPLIB_BIQUAD_TIF) { // (d0, d1): d0' = a11 d0 + d1; d1' = a12 d0
-      A[0] = (double) c.k[3];
-      A[1] = 1.0;
-      A[2] = (double) c.k[2];
-      A[3] = 0.0;
-   }
-   else { // DF1 (xd1, xd2, yd1, yd2): xd1' = 0, xd2' = xd1, yd1' = b1 xd1 + b2 xd2 - a1 yd1 - a2 yd2, yd2' = yd1
-      for (int i = 0; i < 16; i++) A[i] = 0.0;
-      A[1 * 4 + 0] = 1.0;
-      A[2 * 4 + 0] = (double) c.k[1];
-      A[2 * 4 + 1] = (double) c.k[2];
-      A[2 * 4 + 2] = -(double) c.k[3];
-      A[2 * 4 + 3] = -(double) c.k[4];
-      A[3 * 4 + 2] = 1.0;
-   }
+   return {fma(x.a, y.a, x.b * y.c), fma(x.a, y.b, x.b * y.d), fma(x.c, y.a, x.d * y.c), fma(x.c, y.b, x.d * y.d)};
 }
 
-template <int D> __device__ void matSquare(double *M)
+// m * v + e
+__device__ __forceinline__ double2 affine(const M2 &m, double2 v, double2 e)
 {
-   double R[D * D];
-#pragma unroll
-   for (int i = 0; i < D; i++)
-#pragma unroll
-      for (int j = 0; j < D; j++) {
-         double acc = 0.0;
-#pragma unroll
-         for (int k = 0; k < D; k++) acc = fma(M[i * D + k], M[k * D + j], acc);
-         R[i * D + j] = acc;
-      }
-#pragma unroll
-   for (int i = 0; i < D * D; i++) M[i] = R[i];
+   return make_double2(fma(m.a, v.x, fma(m.b, v.y, e.x)), fma(m.c, v.x, fma(m.d, v.y, e.y)));
 }
 
-// p = M p + e
-template <int D> __device__ __forceinline__ void affine(const double *M, double *p, const double *e)
+// One-sample state transition (zero input) in the scan's state coordinates.
+//   DF2  (w1, w2):  w1' = -a1 w1 - a2 w2,  w2' = w1
+//   TDF2 (w1, w2):  y = w1,  w1' = w2 - a1 y,  w2' = -a2 y.  DF1 is run in
+//        this transposed realization of the same section: its minimal state.
+//   TIF  (d0, d1):  d0' = a11 d0 + d1,  d1' = a12 d0
+template <int FORM> __device__ __forceinline__ M2 transition(const Coef &c)
 {
-   double r[D];
-#pragma unroll
-   for (int i = 0; i < D; i++) {
-      double acc = e[i];
-#pragma unroll
-      for (int k = 0; k < D; k++) acc = fma(M[i * D + k], p[k], acc);
-      r[i] = acc;
-   }
-#pragma unroll
-   for (int i = 0; i < D; i++) p[i] = r[i];
+   if (FORM == DSPLIB_BIQUAD_DF2) return {-(double) c.k[3], -(double) c.k[4], 1.0, 0.0};
+   if (FORM == DSPLIB_BIQUAD_TIF) return {(double) c.k[3], 1.0, (double) c.k[2], 0.0};
+   return {-(double) c.k[3], 1.0, -(double) c.k[4], 0.0};
 }
 
-// Run the stage recursion over v[0..len) from state st (FP32, fused
-// multiply-add).  WRITE = false computes only the end state.
-template <int FORM, int L, bool WRITE>
-__device__ __forceinline__ void runChunk(float (&v)[L], int len, const Coef &c, float *st)
+// The stage recursion over v[0..len) from state st (FP32, fused multiply-add).
+// WRITE = false computes only the end state.  DF1 uses the TDF2 recursion.
+// For DF1 the last two stage inputs and outputs are kept for the final state.
+// Each recursion is arranged so that one fused multiply-add per sample lies
+// on the loop-carried dependency chain (the older state enters the inner term).
+// FULL = true: len == L, no per-sample predicate.
+template <int FORM, int L, bool WRITE, bool FULL>
+__device__ __forceinline__ void runChunk(float (&v)[L], int len, const Coef &c, float2 &st, float4 *tail)
 {
    if (FORM == DSPLIB_BIQUAD_DF2) {
       const float b0 = c.k[0], b1 = c.k[1], b2 = c.k[2], a1 = c.k[3], a2 = c.k[4];
-      float w1 = st[0], w2 = st[1];
+      float w1 = st.x, w2 = st.y;
 #pragma unroll
       for (int i = 0; i < L; i++) {
-         if (i < len) {
-            const float w0 = fmaf(-a2, w2, fmaf(-a1, w1, v[i]));
-            if (WRITE) v[i] = fmaf(b2, w2, fmaf(b1, w1, b0 * w0));
+         if (FULL || i < len) {
+            const float w0 = fmaf(-a1, w1, fmaf(-a2, w2, v[i]));
+            if (WRITE) v[i] = fmaf(b0, w0, fmaf(b1, w1, b2 * w2));
             w2 = w1;
             w1 = w0;
          }
       }
-      st[0] = w1;
-      st[1] = w2;
-   }
-   else if (FORM == DSPLIB_BIQUAD_TDF2) {
-      const float b0 = c.k[0], b1 = c.k[1], b2 = c.k[2], a1 = c.k[3], a2 = c.k[4];
-      float w1 = st[0], w2 = st[1];
-#pragma unroll
-      for (int i = 0; i < L; i++) {
-         if (i < len) {
-            const float x = v[i];
-            const float y = fmaf(x, b0, w1);
-            w1 = fmaf(-a1, y, fmaf(x, b1, w2));
-            w2 = fmaf(-a2, y, x * b2);
-            if (WRITE) v[i] = y;
-         }
-      }
-      st[0] = w1;
-      st[1] = w2;
+      st = make_float2(w1, w2);
    }
    else if (FORM == DSPLIB_BIQUAD_TIF) {
       const float c0 = c.k[0], c1 = c.k[1], a12 = c.k[2], a11 = c.k[3];
-      float d0 = st[0], d1 = st[1];
+      float d0 = st.x, d1 = st.y;
 #pragma unroll
       for (int i = 0; i < L; i++) {
-         if (i < len) {
+         if (FULL || i < len) {
             const float x = v[i];
             const float o = x + d0;
             const float nd0 = fmaf(a11, d0, fmaf(x, c0, d1));
@@ -274,224 +221,405 @@ __device__ __forceinline__ void runChunk(float (&v)[L], int len, const Coef &c, 
             if (WRITE) v[i] = o;
          }
       }
-      st[0] = d0;
-      st[1] = d1;
+      st = make_float2(d0, d1);
    }
    else {
-      const float b0 = c.k[0], b1 = c.k[1], b2 = c.k[2], a1 = c.k[3], a2 = c.k[4];
-      float xd1 = st[0], xd2 = st[1], yd1 = st[2], yd2 = st[3];
+      // TDF2: y = b0 x + w1; w1' = w2 + b1 x - a1 y; w2' = b2 x - a2 y, with y
+      // substituted so that w1' = -a1 w1 + (w2 + (b1 - a1 b0) x).
+      const float b0 = c.k[0], a1 = c.k[3], a2 = c.k[4];
+      const float c1 = (float) ((double) c.k[1] - (double) a1 * b0);
+      const float c2 = (float) ((double) c.k[2] - (double) a2 * b0);
+      float w1 = st.x, w2 = st.y;
+      float u1 = 0.f, u2 = 0.f, y1 = 0.f, y2 = 0.f;
 #pragma unroll
       for (int i = 0; i < L; i++) {
-         if (i < len) {
+         if (FULL || i < len) {
             const float x = v[i];
-            const float y = fmaf(-a2, yd2, fmaf(-a1, yd1, fmaf(b2, xd2, fmaf(b1, xd1, b0 * x))));
-            xd2 = xd1;
-            xd1 = x;
-            yd2 = yd1;
-            yd1 = y;
-            if (WRITE) v[i] = y;
+            if (WRITE) {
+               const float y = fmaf(x, b0, w1);
+               v[i] = y;
+               if (FORM == DSPLIB_BIQUAD_DF1) {
+                  u2 = u1;
+                  u1 = x;
+                  y2 = y1;
+                  y1 = y;
+               }
+            }
+            const float w1n = fmaf(-a1, w1, fmaf(x, c1, w2));
+            w2 = fmaf(-a2, w1, x * c2);
+            w1 = w1n;
          }
       }
-      st[0] = xd1;
-      st[1] = xd2;
-      st[2] = yd1;
-      st[3] = yd2;
+      st = make_float2(w1, w2);
+      if (FORM == DSPLIB_BIQUAD_DF1 && WRITE) *tail = make_float4(u1, u2, y1, y2);
    }
 }
 
-constexpr int kScanW = 16; // warps (chunks) per CTA
-constexpr int kScanL = 32; // samples per chunk
+template <int FORM, int L, bool WRITE>
+__device__ __forceinline__ void runChunkAny(float (&v)[L], int len, const Coef &c, float2 &st, float4 *tail)
+{
+   if (len == L) runChunk<FORM, L, WRITE, true>(v, len, c, st, tail);
+   else runChunk<FORM, L, WRITE, false>(v, len, c, st, tail);
+}
 
-struct ScanSmem {
-   // byte offsets inside dynamic shared memory
-   size_t M, Mc, E, Agg, In, Win, Cf, total;
+constexpr int kScanL = 32;      // samples per chunk
+constexpr int kPad = 33;        // row pitch (double2) of the chunk x channel tables
+constexpr int kMaxCluster = 16; // CTAs per cluster
+constexpr int kPowTableBytes = 64 * 1024;
+
+__host__ __device__ constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x / 2); }
+
+// Matrix powers kept per stage and channel: M^(2^k), M = A^L, for
+// k = 0 .. log2(W) + 4 (the last five cover the CTA span A^(W*L) and its
+// powers up to 16 CTAs).
+template <int W> struct ScanShape {
+   static constexpr int LOGW = ilog2c(W);
+   static constexpr int NP = LOGW + 5;
+   static constexpr int CPW = 32 / W; // channels scanned by one warp
 };
 
-__host__ __device__ inline ScanSmem scanLayout(int S, int D)
+struct ScanSmem {
+   size_t E, P, Agg, Win, Pow, Cf, total;
+   bool powTable;
+};
+
+template <int W> __host__ __device__ inline ScanSmem scanLayout(int S)
 {
    ScanSmem o;
    size_t off = 0;
-   o.M = off;
-   off += (size_t) S * 32 * D * D * sizeof(double);
-   o.Mc = off;
-   off += (size_t) S * 32 * D * D * sizeof(double);
    o.E = off;
-   off += (size_t) kScanW * 32 * D * sizeof(double);
+   off += (size_t) W * kPad * sizeof(double2);
+   o.P = off;
+   off += (size_t) W * kPad * sizeof(double2);
    o.Agg = off;
-   off += (size_t) 2 * 32 * D * sizeof(double);
-   o.In = off;
-   off += (size_t) 32 * D * sizeof(double);
+   off += (size_t) 2 * 32 * sizeof(double2);
    o.Win = off;
-   off += (size_t) S * 32 * D * sizeof(double);
+   off += (size_t) S * 32 * sizeof(double2);
+   const size_t pow = (size_t) S * 32 * ScanShape<W>::NP * sizeof(M2);
+   o.powTable = pow <= (size_t) kPowTableBytes;
+   o.Pow = off; // all stages' powers, or one stage's (recomputed per stage) when that is too large
+   off += o.powTable ? pow : (size_t) 32 * ScanShape<W>::NP * sizeof(M2);
    o.Cf = off;
    off += (size_t) S * 32 * 5 * sizeof(float);
    o.total = off;
    return o;
 }
 
-template <int FORM, bool CLUSTER>
-__global__ void __launch_bounds__(kScanW * 32, 1) biquad_scan_kernel(BiquadLaunch a)
+// Writes M^(2^k), k = 0 .. NP-1, of M = A^L to out[] (two matrices live at a time).
+template <int FORM, int W> __device__ __forceinline__ void stagePowers(const Coef &c, M2 *out)
 {
-   constexpr int D = Form<FORM>::D;
-   constexpr int W = kScanW;
+   M2 P = transition<FORM>(c);
+#pragma unroll
+   for (int r = 1; r < kScanL; r <<= 1) P = mmul(P, P);
+   out[0] = P;
+#pragma unroll
+   for (int k = 1; k < ScanShape<W>::NP; k++) {
+      P = mmul(P, P);
+      out[k] = P;
+   }
+}
+
+// Inclusive Kogge-Stone scan of x_j over the W lanes of a segment:
+// x_j <- sum_{i <= j} M^(j - i) x_i, with P[k] = M^(2^k) (shared memory).
+template <int W>
+__device__ __forceinline__ double2 segmentScan(double2 val, int j, const M2 *P, int count)
+{
+#pragma unroll
+   for (int k = 0; (1 << k) < W; k++) {
+      double2 o;
+      o.x = __shfl_up_sync(0xffffffffu, val.x, 1 << k, W);
+      o.y = __shfl_up_sync(0xffffffffu, val.y, 1 << k, W);
+      if ((1 << k) < count && j >= (1 << k)) val = affine(P[k], o, val);
+   }
+   return val;
+}
+
+// M^n v for 0 <= n < 2^nb, with P[k] = M^(2^k).
+__device__ __forceinline__ double2 powApply(const M2 *P, int n, int nb, double2 v)
+{
+   const double2 z = make_double2(0.0, 0.0);
+#pragma unroll
+   for (int k = 0; k < 5; k++)
+      if (k < nb && ((n >> k) & 1)) v = affine(P[k], v, z);
+   return v;
+}
+
+template <int FORM, int W, bool CLUSTER>
+__global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunch a)
+{
    constexpr int L = kScanL;
    constexpr int nv = FORM == DSPLIB_BIQUAD_DF1 ? 4 : 2;
+   constexpr int LOGW = ScanShape<W>::LOGW;
+   constexpr int NP = ScanShape<W>::NP;
+   constexpr int CPW = ScanShape<W>::CPW;
    extern __shared__ __align__(16) unsigned char smem[];
-   const ScanSmem lay = scanLayout(a.S, D);
-   double *sM = (double *) (smem + lay.M);
-   double *sMc = (double *) (smem + lay.Mc);
-   double *sE = (double *) (smem + lay.E);
-   double *sAgg = (double *) (smem + lay.Agg);
-   double *sIn = (double *) (smem + lay.In);
-   double *sWin = (double *) (smem + lay.Win);
+   const ScanSmem lay = scanLayout<W>(a.S);
+   double2 *sE = (double2 *) (smem + lay.E);
+   double2 *sP = (double2 *) (smem + lay.P);
+   double2 *sAgg = (double2 *) (smem + lay.Agg);
+   double2 *sWin = (double2 *) (smem + lay.Win);
+   M2 *sPow = (M2 *) (smem + lay.Pow);
    float *sCf = (float *) (smem + lay.Cf);
 
    const int lane = threadIdx.x & 31;
    const int w = threadIdx.x >> 5;
    const int ch = blockIdx.y * 32 + lane;
    const bool active = ch < a.C;
+   // scan role: warp w scans the W chunks of channels CPW*w .. CPW*w+CPW-1
+   const int j = lane % W;
+   const int cc = w * CPW + lane / W;
    int K = 1, rank = 0;
    if (CLUSTER) {
       cg::cluster_group cl = cg::this_cluster();
       K = (int) cl.num_blocks();
       rank = (int) cl.block_rank();
    }
+   const int logK = ilog2c(K);
+   const long long windowLen = (long long) K * W * L;
 
-   // Per stage and lane: coefficients, M = A^L, Mc = A^(W*L), initial state.
+   // First window's input, issued before the table set-up so the loads overlap it.
+   long long t0 = ((long long) rank * W + w) * L;
+   int len = (active && t0 < a.N) ? (int) ((a.N - t0) < L ? (a.N - t0) : L) : 0;
+   float v[L];
+   {
+      const float *xp = a.x + t0 * a.inPitch + ch;
+      if (len == L) {
+#pragma unroll
+         for (int i = 0; i < L; i++) v[i] = xp[i * a.inPitch];
+      }
+      else {
+#pragma unroll
+         for (int i = 0; i < L; i++) v[i] = i < len ? xp[i * a.inPitch] : 0.0f;
+      }
+   }
+
+   // Coefficients, matrix powers and the initial state (scan coordinates) per stage and channel.
    for (int s = w; s < a.S; s += W) {
       Coef c;
       if (active) c = loadCoef(a, s, ch);
       else
          for (int k = 0; k < 5; k++) c.k[k] = 0.0f;
       for (int k = 0; k < 5; k++) sCf[(s * 32 + lane) * 5 + k] = c.k[k];
-      double A[D * D];
-      transition<FORM>(c, A);
-      for (int r = 1; r < L; r <<= 1) matSquare<D>(A);
-      for (int i = 0; i < D * D; i++) sM[(s * 32 + lane) * D * D + i] = A[i];
-      for (int r = 1; r < W; r <<= 1) matSquare<D>(A);
-      for (int i = 0; i < D * D; i++) sMc[(s * 32 + lane) * D * D + i] = A[i];
-      for (int i = 0; i < D; i++)
-         sWin[(s * 32 + lane) * D + i] = active ? (double) a.state[(long long) (s * nv + i) * a.varPitch + ch] : 0.0;
+      if (lay.powTable) stagePowers<FORM, W>(c, sPow + (s * 32 + lane) * NP);
+      double2 st0 = make_double2(0.0, 0.0);
+      if (active) {
+         const float *sp = a.state + (long long) (s * nv) * a.varPitch + ch;
+         if (FORM == DSPLIB_BIQUAD_DF1) { // DF1 (xd1, xd2, yd1, yd2) -> transposed-form state
+            const double xd1 = sp[0], xd2 = sp[a.varPitch], yd1 = sp[2 * a.varPitch], yd2 = sp[3 * a.varPitch];
+            st0.x = c.k[1] * xd1 + c.k[2] * xd2 - c.k[3] * yd1 - c.k[4] * yd2;
+            st0.y = c.k[2] * xd1 - c.k[4] * yd1;
+         }
+         else {
+            st0 = make_double2(sp[0], sp[a.varPitch]);
+         }
+      }
+      sWin[s * 32 + lane] = st0;
+   }
+   float xd1_0 = 0.f, yd1_0 = 0.f; // DF1 with a single sample: the old xd1/yd1 shift into xd2/yd2
+   if (FORM == DSPLIB_BIQUAD_DF1 && active && a.N == 1) {
+      xd1_0 = a.state[ch];
+      yd1_0 = a.state[2 * a.varPitch + ch];
    }
    if (CLUSTER) cg::this_cluster().sync();
    else __syncthreads();
 
-   const long long windowLen = (long long) K * W * L;
    int phase = 0;
    for (long long win0 = 0; win0 < a.N; win0 += windowLen) {
-      const long long t0 = win0 + ((long long) rank * W + w) * L;
-      int len = 0;
-      if (active && t0 < a.N) len = (int) ((a.N - t0) < L ? (a.N - t0) : L);
-      float v[L];
+      if (win0 > 0) {
+         t0 = win0 + ((long long) rank * W + w) * L;
+         len = (active && t0 < a.N) ? (int) ((a.N - t0) < L ? (a.N - t0) : L) : 0;
+         const float *xp = a.x + t0 * a.inPitch + ch;
+         if (len == L) {
 #pragma unroll
-      for (int i = 0; i < L; i++) v[i] = i < len ? a.x[(t0 + i) * a.inPitch + ch] : 0.0f;
-
+            for (int i = 0; i < L; i++) v[i] = xp[i * a.inPitch];
+         }
+         else {
+#pragma unroll
+            for (int i = 0; i < L; i++) v[i] = i < len ? xp[i * a.inPitch] : 0.0f;
+         }
+      }
       for (int s = 0; s < a.S; s++) {
          Coef c;
 #pragma unroll
          for (int k = 0; k < 5; k++) c.k[k] = sCf[(s * 32 + lane) * 5 + k];
-         const double *M = sM + (s * 32 + lane) * D * D;
          // 1. zero-state end state of this chunk
-         float e[D];
-#pragma unroll
-         for (int i = 0; i < D; i++) e[i] = 0.0f;
-         runChunk<FORM, L, false>(v, len, c, e);
-#pragma unroll
-         for (int i = 0; i < D; i++) sE[(w * 32 + lane) * D + i] = (double) e[i];
+         float2 e = make_float2(0.f, 0.f);
+         runChunkAny<FORM, L, false>(v, len, c, e, nullptr);
+         sE[w * kPad + lane] = make_double2(e.x, e.y);
          __syncthreads();
-         // 2a. CTA aggregate: state at the end of this CTA's span starting from zero
-         double *agg = sAgg + (phase & 1) * 32 * D;
-         if (w == W - 1) {
-            double p[D];
-#pragma unroll
-            for (int i = 0; i < D; i++) p[i] = 0.0;
-            for (int j = 0; j < W; j++) affine<D>(M, p, sE + (j * 32 + lane) * D);
-#pragma unroll
-            for (int i = 0; i < D; i++) agg[lane * D + i] = p[i];
+
+         // 2. scan over the CTA's W chunks (FP64)
+         const M2 *P;
+         if (lay.powTable) {
+            P = sPow + (s * 32 + cc) * NP;
          }
-         if (CLUSTER) cg::this_cluster().sync();
-         else __syncthreads();
-         // 2b. combine the cluster's aggregates in order: state entering this
-         // CTA, and the state at the end of the window (next window's carry).
-         if (w == 0) {
-            const double *Mc = sMc + (s * 32 + lane) * D * D;
-            double cur[D], mine[D];
+         else {
+            P = sPow + cc * NP;
+            if (j == 0) {
+               Coef cs;
 #pragma unroll
-            for (int i = 0; i < D; i++) cur[i] = sWin[(s * 32 + lane) * D + i];
-            for (int q = 0; q < K; q++) {
-               if (q == rank)
-#pragma unroll
-                  for (int i = 0; i < D; i++) mine[i] = cur[i];
-               double eq[D];
-               if (CLUSTER && q != rank) {
-                  const double *remote = cg::this_cluster().map_shared_rank(agg, q);
-#pragma unroll
-                  for (int i = 0; i < D; i++) eq[i] = remote[lane * D + i];
-               }
-               else {
-#pragma unroll
-                  for (int i = 0; i < D; i++) eq[i] = agg[lane * D + i];
-               }
-               affine<D>(Mc, cur, eq);
+               for (int k = 0; k < 5; k++) cs.k[k] = sCf[(s * 32 + cc) * 5 + k];
+               stagePowers<FORM, W>(cs, sPow + cc * NP);
             }
-#pragma unroll
-            for (int i = 0; i < D; i++) {
-               sIn[lane * D + i] = mine[i];
-               sWin[(s * 32 + lane) * D + i] = cur[i];
-            }
+            __syncwarp();
          }
+         double2 val = segmentScan<W>(sE[j * kPad + cc], j, P, W);
+         double2 ex;
+         ex.x = __shfl_up_sync(0xffffffffu, val.x, 1, W);
+         ex.y = __shfl_up_sync(0xffffffffu, val.y, 1, W);
+         if (j == 0) ex = make_double2(0.0, 0.0);
+
+         // 3. entry state of this CTA, and the state at the end of the window
+         const double2 win = sWin[s * 32 + cc];
+         double2 mine = win, wend;
+         if (CLUSTER && K > 1) {
+            double2 *agg = sAgg + (phase & 1) * 32;
+            if (j == W - 1) agg[cc] = val; // end of this CTA's span from a zero entry state
+            cg::this_cluster().sync();
+            // lane j holds CTA j's aggregate; scan them with Mc = A^(W*L) powers
+            double2 ej = make_double2(0.0, 0.0);
+            if (j < K) ej = (j == rank) ? agg[cc] : cg::this_cluster().map_shared_rank(agg, j)[cc];
+            const double2 incl = segmentScan<W>(ej, j, P + LOGW, K);
+            const int seg = lane - j;
+            double2 before;
+            before.x = __shfl_sync(0xffffffffu, incl.x, seg + (rank > 0 ? rank - 1 : 0));
+            before.y = __shfl_sync(0xffffffffu, incl.y, seg + (rank > 0 ? rank - 1 : 0));
+            double2 last;
+            last.x = __shfl_sync(0xffffffffu, incl.x, seg + K - 1);
+            last.y = __shfl_sync(0xffffffffu, incl.y, seg + K - 1);
+            mine = powApply(P + LOGW, rank, logK, win);
+            if (rank > 0) mine = make_double2(mine.x + before.x, mine.y + before.y);
+            wend = affine(P[LOGW + logK], win, last);
+         }
+         else {
+            wend = affine(P[LOGW], win, make_double2(0.0, 0.0));
+            double2 lastv;
+            lastv.x = __shfl_sync(0xffffffffu, val.x, lane - j + W - 1);
+            lastv.y = __shfl_sync(0xffffffffu, val.y, lane - j + W - 1);
+            wend = make_double2(wend.x + lastv.x, wend.y + lastv.y);
+         }
+         // true initial state of chunk j: M^j * entry + exclusive prefix
+         const double2 tv = powApply(P, j, LOGW, mine);
+         sP[j * kPad + cc] = make_double2(tv.x + ex.x, tv.y + ex.y);
+         __syncwarp();
+         if (j == 0) sWin[s * 32 + cc] = wend;
          __syncthreads();
-         // 2c. this chunk's initial state
-         double p[D];
-#pragma unroll
-         for (int i = 0; i < D; i++) p[i] = sIn[lane * D + i];
-         for (int j = 0; j < w; j++) affine<D>(M, p, sE + (j * 32 + lane) * D);
-         // 3. rerun from the true state, producing the stage output in place
-         float st[D];
-#pragma unroll
-         for (int i = 0; i < D; i++) st[i] = (float) p[i];
-         runChunk<FORM, L, true>(v, len, c, st);
-         if (FORM == DSPLIB_BIQUAD_TIF) {
+
+         // 4. rerun from the true state, producing the stage output in place
+         const double2 p = sP[w * kPad + lane];
+         float2 st = make_float2((float) p.x, (float) p.y);
+         float4 tail = make_float4(0.f, 0.f, 0.f, 0.f);
+         runChunkAny<FORM, L, true>(v, len, c, st, &tail);
+         if (FORM == DSPLIB_BIQUAD_TIF && c.k[4] != 1.0f) {
             const float g = c.k[4];
 #pragma unroll
             for (int i = 0; i < L; i++) v[i] *= g;
          }
+         float *sp = a.state + (long long) (s * nv) * a.varPitch + ch;
          if (len > 0 && t0 + len == a.N) { // chunk holding the last sample: final state
-#pragma unroll
-            for (int i = 0; i < D; i++) a.state[(long long) (s * nv + i) * a.varPitch + ch] = st[i];
+            if (FORM == DSPLIB_BIQUAD_DF1) {
+               sp[0] = tail.x;
+               sp[2 * a.varPitch] = tail.z;
+               if (len >= 2) {
+                  sp[a.varPitch] = tail.y;
+                  sp[3 * a.varPitch] = tail.w;
+               }
+               else if (a.N == 1) {
+                  sp[a.varPitch] = xd1_0;
+                  sp[3 * a.varPitch] = yd1_0;
+               }
+            }
+            else {
+               sp[0] = st.x;
+               sp[a.varPitch] = st.y;
+            }
+         }
+         if (FORM == DSPLIB_BIQUAD_DF1 && len == L && t0 + L == a.N - 1) { // next chunk holds one sample
+            sp[a.varPitch] = tail.x;
+            sp[3 * a.varPitch] = tail.z;
          }
          phase++;
-         __syncthreads();
       }
+      {
+         float *yp = a.y + t0 * a.outPitch + ch;
+         if (len == L) {
 #pragma unroll
-      for (int i = 0; i < L; i++)
-         if (i < len) a.y[(t0 + i) * a.outPitch + ch] = v[i];
+            for (int i = 0; i < L; i++) yp[i * a.outPitch] = v[i];
+         }
+         else {
+#pragma unroll
+            for (int i = 0; i < L; i++)
+               if (i < len) yp[i * a.outPitch] = v[i];
+         }
+      }
    }
    // Keep every CTA's shared memory alive until the cluster's last remote read.
    if (CLUSTER) cg::this_cluster().sync();
 }
 
-template <int FORM> cudaError_t launchScanForm(const BiquadLaunch &a, cudaStream_t s)
+// Largest power-of-two cluster <= want that can be resident (<= 8 portable, 16 opt-in).
+template <int FORM, int W> int pickCluster(int want, size_t smemBytes)
 {
-   constexpr int D = Form<FORM>::D;
-   const ScanSmem lay = scanLayout(a.S, D);
-   const long long cta = (long long) kScanW * kScanL;
-   int K = (int) ((a.N + cta - 1) / cta);
-   if (K > 8) K = 8;
-   if (K < 1) K = 1;
-   dim3 grid(K, (a.C + 31) / 32);
-   dim3 block(kScanW * 32);
+   static int cached[17] = {0};
+   if (want > W) want = W;
+   if (want > kMaxCluster) want = kMaxCluster;
+   int K = 1;
+   while (K * 2 <= want) K *= 2;
+   if (K <= 1) return 1;
+   if (cached[K]) return cached[K];
+   auto fn = biquad_scan_kernel<FORM, W, true>;
+   int chosen = 1;
+   for (int k = K; k >= 2; k >>= 1) {
+      if (k > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+         (void) cudaGetLastError();
+         continue;
+      }
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(k, 1);
+      cfg.blockDim = dim3(W * 32);
+      cfg.dynamicSmemBytes = smemBytes;
+      cudaLaunchAttribute attr;
+      attr.id = cudaLaunchAttributeClusterDimension;
+      attr.val.clusterDim.x = k;
+      attr.val.clusterDim.y = 1;
+      attr.val.clusterDim.z = 1;
+      cfg.attrs = &attr;
+      cfg.numAttrs = 1;
+      int n = 0;
+      if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) == cudaSuccess && n >= 1) {
+         chosen = k;
+         break;
+      }
+      (void) cudaGetLastError();
+   }
+   cached[K] = chosen;
+   return chosen;
+}
+
+template <int FORM, int W> cudaError_t launchScanShape(const BiquadLaunch &a, int want, cudaStream_t s)
+{
+   const ScanSmem lay = scanLayout<W>(a.S);
+   const int groups = (a.C + 31) / 32;
+   dim3 block(W * 32);
    cudaError_t e;
-   if (K == 1) {
-      auto fn = biquad_scan_kernel<FORM, false>;
-      if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) lay.total)) != cudaSuccess)
+   auto fn1 = biquad_scan_kernel<FORM, W, false>;
+   auto fnK = biquad_scan_kernel<FORM, W, true>;
+   static bool attrSet = false;
+   static size_t attrBytes = 0;
+   if (!attrSet || attrBytes < lay.total) {
+      if ((e = cudaFuncSetAttribute(fn1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) lay.total)) != cudaSuccess)
          return e;
-      fn<<<grid, block, lay.total, s>>>(a);
+      if ((e = cudaFuncSetAttribute(fnK, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) lay.total)) != cudaSuccess)
+         return e;
+      attrSet = true;
+      attrBytes = lay.total;
+   }
+   const int K = want > 1 ? pickCluster<FORM, W>(want, lay.total) : 1;
+   dim3 grid(K, groups);
+   if (K == 1) {
+      fn1<<<grid, block, lay.total, s>>>(a);
    }
    else {
-      auto fn = biquad_scan_kernel<FORM, true>;
-      if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) lay.total)) != cudaSuccess)
-         return e;
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = grid;
       cfg.blockDim = block;
@@ -504,10 +632,28 @@ template <int FORM> cudaError_t launchScanForm(const BiquadLaunch &a, cudaStream
       attr[0].val.clusterDim.z = 1;
       cfg.attrs = attr;
       cfg.numAttrs = 1;
-      if ((e = cudaLaunchKernelEx(&cfg, fn, a)) != cudaSuccess) return e;
+      if ((e = cudaLaunchKernelEx(&cfg, fnK, a)) != cudaSuccess) return e;
    }
    countLaunch();
    return cudaGetLastError();
+}
+
+// Launch shape: few channel groups -> 16-warp CTAs and clusters of up to 16
+// CTAs along time (latency); many groups -> 8-warp CTAs (two per SM) with
+// clusters sized to fill one wave of the 148 SMs (throughput).
+template <int FORM> cudaError_t launchScanForm(const BiquadLaunch &a, cudaStream_t s)
+{
+   const int groups = (a.C + 31) / 32;
+   const long long chunks = (a.N + kScanL - 1) / kScanL;
+   constexpr int kSMs = 148;
+   if (groups * 4 <= kSMs) {
+      int want = (int) ((chunks + 15) / 16);
+      return launchScanShape<FORM, 16>(a, want < 1 ? 1 : want, s);
+   }
+   int want = (int) ((chunks + 7) / 8);
+   const int fill = (2 * kSMs) / groups;
+   if (want > fill) want = fill;
+   return launchScanShape<FORM, 8>(a, want < 1 ? 1 : want, s);
 }
 
 template <int FORM> cudaError_t launchSeqForm(const BiquadLaunch &a, cudaStream_t s)
@@ -530,13 +676,14 @@ cudaError_t launchBiquadSequential(const BiquadLaunch &a, cudaStream_t s)
    return cudaErrorInvalidValue;
 }
 
-// Largest stage count whose scan tables fit in shared memory; deeper
-// cascades use the sequential kernel.
-static int scanMaxStages(int form) { return form == DSPLIB_BIQUAD_DF1 ? 16 : 32; }
+// Deepest cascade whose coefficient and carry tables fit the scan kernel's
+// shared memory budget (36 B per stage and channel); deeper cascades use
+// the sequential kernel.
+static int scanMaxStages() { return 160; }
 
 cudaError_t launchBiquadScan(const BiquadLaunch &a, cudaStream_t s)
 {
-   if (a.S > scanMaxStages(a.form)) return launchBiquadSequential(a, s);
+   if (a.S > scanMaxStages()) return launchBiquadSequential(a, s);
    switch (a.form) {
    case DSPLIB_BIQUAD_DF1: return launchScanForm<DSPLIB_BIQUAD_DF1>(a, s);
    case DSPLIB_BIQUAD_DF2: return launchScanForm<DSPLIB_BIQUAD_DF2>(a, s);

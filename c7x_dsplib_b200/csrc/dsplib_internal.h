@@ -99,13 +99,20 @@ struct FirLaunch {
 };
 
 enum FirKernelKind {
-   FIR_NATC = 0,      // bit-exact natural-C semantics (wrap / sequential float)
-   FIR_QMODE = 1,     // exact accumulator, round/shift/saturate
-   FIR_F32_SIMT = 2,  // FP32 FMA register-tiled CUDA-core kernel
-   FIR_F32_BF16X3 = 3 // tcgen05 split-BF16x3 tensor-core kernel
+   FIR_NATC = 0,       // bit-exact natural-C semantics (wrap / sequential float), CUDA cores
+   FIR_QMODE = 1,      // exact accumulator, round/shift/saturate, CUDA cores
+   FIR_F32_SIMT = 2,   // FP32 FMA register-tiled CUDA-core kernel
+   FIR_F32_BF16X3 = 3, // tcgen05 split-BF16x3 tensor-core kernel
+   FIR_INT_WRAP_TC = 4, // tcgen05 kind::i8 kernel, int8/int16, natural-C wrap output
+   FIR_INT_Q_TC = 5     // tcgen05 kind::i8 kernel, int8/int16, Q-mode output
 };
 
 cudaError_t launchFir(const FirLaunch &a, FirKernelKind kind, cudaStream_t s);
+bool firIntTcSupported(const FirLaunch &a);
+cudaError_t launchFirIntTc(const FirLaunch &a, bool qmode, cudaStream_t s);
+// Error word written by the tensor-core kernels when a bounded wait gives up
+// (-1: could not be read).
+int firTcErrorFlag(bool clear);
 
 struct BiquadLaunch {
    const float *x;

@@ -196,10 +196,17 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
    a.outPitch = p->outPitch;
    a.filtPitch = nch ? filtPitch : 0; // staging keeps the caller's row pitch
    a.shift = (int) ia.shift;
+   // Optimized 8/16-bit integers run on the tensor cores when the taps fit the band buffer.
+   if (!natc && (p->dtype == DSPLIB_INT8 || p->dtype == DSPLIB_INT16) && firIntTcSupported(a))
+      kind = hc->firQMode ? FIR_INT_Q_TC : FIR_INT_WRAP_TC;
    if ((e = launchFir(a, kind, s)) != cudaSuccess) return cudaFail(hc, e, "FIR kernel launch");
    if ((e = regionOut(rout, s)) != cudaSuccess) return cudaFail(hc, e, "copy output");
    if (!hc->async || rin.staged || rf.staged || rout.staged) {
       if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, "FIR execution");
+      if ((kind == FIR_INT_WRAP_TC || kind == FIR_INT_Q_TC || kind == FIR_F32_BF16X3) && firTcErrorFlag(true) != 0) {
+         setError(hc, "tensor-core FIR: a bounded wait for MMA completion expired; outputs are incomplete");
+         return DSPLIB_ERR_FAILURE;
+      }
    }
    return DSPLIB_SUCCESS;
 }

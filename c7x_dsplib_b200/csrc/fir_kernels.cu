@@ -193,6 +193,10 @@ cudaError_t launchFir(const FirLaunch &a, FirKernelKind kind, cudaStream_t s)
    case FIR_F32_BF16X3:
       if (a.dtype != DSPLIB_FLOAT32) return cudaErrorInvalidValue;
       return launchFirBf16x3(a, s);
+   case FIR_INT_WRAP_TC:
+   case FIR_INT_Q_TC:
+      if (!firIntTcSupported(a)) return cudaErrorInvalidValue;
+      return launchFirIntTc(a, kind == FIR_INT_Q_TC, s);
    }
    return cudaErrorInvalidValue;
 }

@@ -1,0 +1,118 @@
+// Small inline-PTX helpers for tcgen05 (5th-generation tensor cores), TMEM
+// and mbarriers on sm_100a.  Encodings follow the PTX ISA for sm_100a:
+//   shared-memory matrix descriptor: start>>4 [0,14), LBO>>4 [16,30),
+//     SBO>>4 [32,46), version 1 at [46,48), layout type [61,64) (0 = no swizzle);
+//   instruction descriptor (kind::i8 / kind::f16): D format [4,6),
+//     A format [7,10), B format [10,13), A/B major [15]/[16], N>>3 [17,23),
+//     M>>4 [24,29).
+#pragma once
+
+#include <cstdint>
+
+namespace dsplib {
+namespace tc {
+
+__device__ __forceinline__ uint32_t smemAddr(const void *p) { return (uint32_t) __cvta_generic_to_shared(p); }
+
+// K-major operand without swizzle: 8-row core matrices of 16-byte rows.
+// lbo = byte distance between the two 16-byte K halves of a core-matrix pair,
+// sbo = byte distance between consecutive 8-row groups.
+__device__ __forceinline__ uint64_t descNoSwizzle(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+   uint64_t d = 0;
+   d |= (uint64_t) ((saddr >> 4) & 0x3FFF);
+   d |= (uint64_t) ((lbo >> 4) & 0x3FFF) << 16;
+   d |= (uint64_t) ((sbo >> 4) & 0x3FFF) << 32;
+   d |= (uint64_t) 1 << 46; // descriptor version for sm_100
+   return d;                // layout type 0: no swizzle
+}
+
+// Instruction descriptor.  dfmt: 1 = F32, 2 = S32.  afmt/bfmt: kind::i8 -> 0 unsigned, 1 signed;
+// kind::f16 -> 0 F16, 1 BF16.  Both operands K-major.
+__host__ __device__ constexpr uint32_t idesc(uint32_t dfmt, uint32_t afmt, uint32_t bfmt, uint32_t M, uint32_t N)
+{
+   return (dfmt << 4) | (afmt << 7) | (bfmt << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mmaI8(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t id, bool accum)
+{
+   asm volatile("{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+                "l"(adesc), "l"(bdesc), "r"(id), "r"((uint32_t) accum));
+}
+
+__device__ __forceinline__ void mmaF16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t id, bool accum)
+{
+   asm volatile("{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+                "l"(adesc), "l"(bdesc), "r"(id), "r"((uint32_t) accum));
+}
+
+// Arrive on an mbarrier once all previously issued tcgen05.mma of this thread complete.
+__device__ __forceinline__ void commit(uint64_t *mbar)
+{
+   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smemAddr(mbar))
+                : "memory");
+}
+
+__device__ __forceinline__ void fenceBeforeSync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fenceAfterSync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Make generic-proxy shared-memory writes visible to the tensor core (async proxy).
+__device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbarInit(uint64_t *mbar, uint32_t count)
+{
+   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(mbar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbarTryWait(uint64_t *mbar, uint32_t parity)
+{
+   uint32_t ok;
+   asm volatile("{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.b32 %0, 1, 0, p;\n\t}\n"
+                : "=r"(ok)
+                : "r"(smemAddr(mbar)), "r"(parity)
+                : "memory");
+   return ok != 0;
+}
+
+// Bounded wait: returns false if the phase did not complete within the limit.
+__device__ __forceinline__ bool mbarWait(uint64_t *mbar, uint32_t parity, uint32_t limit = 1u << 22)
+{
+   for (uint32_t i = 0; i < limit; i++)
+      if (mbarTryWait(mbar, parity)) return true;
+   return false;
+}
+
+// TMEM allocation by one full warp; the base address is written to *slot (shared memory).
+__device__ __forceinline__ void tmemAlloc(uint32_t *slot, uint32_t ncols)
+{
+   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(slot)),
+                "r"(ncols)
+                : "memory");
+   asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmemFree(uint32_t taddr, uint32_t ncols)
+{
+   asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// 32 lanes x 16 consecutive 32-bit columns: thread t of the warp receives lane (base lane + t).
+__device__ __forceinline__ void tmemLoad16(uint32_t taddr, uint32_t (&r)[16])
+{
+   asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmemWaitLoad() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+} // namespace tc
+} // namespace dsplib

@@ -82,6 +82,44 @@ def test_qmode_bitexact(dt, shift):
         assert np.array_equal(got, oracle.fir_q(x, h, T, shift, nch=1)), (B, N, T)
 
 
+@pytest.mark.parametrize("dt", [np.int8, np.int16])
+@pytest.mark.parametrize("qmode", [False, True])
+def test_int_tensor_core_edges(dt, qmode):
+    """Tensor-core integer path: partial tiles, odd pitches, extreme values, long filters
+    (T <= 2048 on the tensor cores, beyond that the CUDA-core kernel)."""
+    rng = np.random.default_rng(21)
+    info = np.iinfo(dt)
+    for (B, N, T, nch) in [(1, 16, 1, 0), (2, 2047 + 30, 31, 1), (3, 5000, 2048, 0), (2, 4500, 2100, 1),
+                           (5, 2049 + 127, 128, 1), (1, 70000, 97, 0)]:
+        x = rand(dt, (B, N), rng)
+        h = rand(dt, (B if nch else 1, T), rng)
+        x[:, :8] = info.min  # the hi/lo split must handle the extremes
+        h[:, :3] = info.min
+        h[:, -2:] = info.max
+        shift = 7 if dt == np.int8 else 15
+        got = host(D.fir(dev(x), dev(h), T, nch=nch, func_style=D.OPTIMIZED, qmode=qmode, shift=shift))
+        want = oracle.fir_q(x, h, T, shift, nch=nch) if qmode else oracle.fir(x, h, T, nch=nch)
+        assert np.array_equal(got, want), (B, N, T, nch)
+
+
+def test_int_tensor_core_unaligned_rows():
+    """Row pitch not a multiple of 16 bytes (vector loads must not be used)."""
+    rng = np.random.default_rng(22)
+    B, N, T, pitch = 3, 3001, 64, 3003
+    x = np.zeros((B, pitch), np.int8)
+    x[:, :N] = rand(np.int8, (B, N), rng)
+    hh = rand(np.int8, (1, T), rng)
+    args, pin, pfilt, pout = D.fir_setup(D.INT8, B, N, T, nch=0, in_pitch=pitch, out_pitch=N - T + 5)
+    out = np.zeros((B, N - T + 5), np.int8)
+    h = D.FirHandle()
+    assert h.init(args, pin, pfilt, pout) == D.SUCCESS
+    h.set_qmode(True)
+    xd, hd, od = dev(x), dev(hh), dev(out)
+    assert h.exec(xd, hd, od) == D.SUCCESS, h.last_error()
+    want = oracle.fir_q(np.ascontiguousarray(x[:, :N]), hh, T, 0, nch=0)
+    assert np.array_equal(host(od)[:, : N - T + 1], want)
+
+
 def _relerr(y, y64):
     return np.max(np.abs(y.astype(np.float64) - y64), axis=1) / np.maximum(np.max(np.abs(y64), axis=1), 1e-30)
 
