@@ -109,6 +109,7 @@ enum FirKernelKind {
 
 cudaError_t launchFir(const FirLaunch &a, FirKernelKind kind, cudaStream_t s);
 bool firIntTcSupported(const FirLaunch &a);
+bool firBf16x3Supported(const FirLaunch &a);
 cudaError_t launchFirIntTc(const FirLaunch &a, bool qmode, cudaStream_t s);
 // Error word written by the tensor-core kernels when a bounded wait gives up
 // (-1: could not be read).

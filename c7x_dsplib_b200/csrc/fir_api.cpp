@@ -199,6 +199,8 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
    // Optimized 8/16-bit integers run on the tensor cores when the taps fit the band buffer.
    if (!natc && (p->dtype == DSPLIB_INT8 || p->dtype == DSPLIB_INT16) && firIntTcSupported(a))
       kind = hc->firQMode ? FIR_INT_Q_TC : FIR_INT_WRAP_TC;
+   // Split-BF16x3 covers up to 512 taps; longer filters run the FP32 CUDA-core kernel.
+   if (kind == FIR_F32_BF16X3 && !firBf16x3Supported(a)) kind = FIR_F32_SIMT;
    if ((e = launchFir(a, kind, s)) != cudaSuccess) return cudaFail(hc, e, "FIR kernel launch");
    if ((e = regionOut(rout, s)) != cudaSuccess) return cudaFail(hc, e, "copy output");
    if (!hc->async || rin.staged || rf.staged || rout.staged) {

@@ -1,28 +1,38 @@
 // Tensor-core (tcgen05) FIR kernels for sm_100a.
 //
-// FIR as a Toeplitz contraction.  One tile = 2048 consecutive outputs of one
-// channel, computed by M = 128 rows x N = 16 phases:
-//     D[a][b] = sum_m A[a][m] * B[m][b] = y[j0 + 16a + b]
-//     A[a][m] = x[j0 + 16a + m]            (data, Hankel: row a starts 16 samples after row a-1)
+// FIR as a Toeplitz contraction.  A tile of consecutive outputs of one channel
+// is computed by an M = 128 (rows) x N (phases) accumulator in TMEM:
+//     D[a][b] = sum_m A[a][m] * B[m][b] = y[j0 + P*a + b]
+//     A[a][m] = x[j0 + P*a + m]            (data, Hankel: row a starts P samples after row a-1)
 //     B[m][b] = g[m - b], g[c] = h[T-1-c]  (taps band, zero outside 0 <= m-b < T)
-// with K = T + 15 rounded up to the MMA depth.  For 8-bit operands a 16-byte
-// core-matrix row holds exactly 16 samples, so the Hankel matrix A is read by
-// the tensor core straight from the raw signal segment in shared memory: the
-// no-swizzle K-major descriptor with row pitch 16 B, LBO = 16 B (next 16
-// samples) and SBO = 128 B (next 8 rows) makes consecutive rows overlap.  No
-// expanded copy of the signal is ever written.  The taps band B (16 x K) is
-// built once per CTA and channel.  Accumulators live in TMEM and are drained
-// by 4 warps with tcgen05.ld (thread a receives the 16 consecutive outputs of
-// row a, so the stores are contiguous).
+// The Hankel matrix A is never expanded: the shared-memory descriptors make
+// consecutive rows overlap inside the raw signal segment.
 //
-// int8:  one s8 x s8 product, int32 accumulator.
-// int16: x = 256*xh + xl, g = 256*gh + gl (xh, gh signed bytes; xl, gl
-//        unsigned bytes); y = 65536*hh + 256*(hl + lh) + ll, each term an
-//        exact int32 kind::i8 accumulation, recombined exactly in 64 bits.
-//        Modulo 2^16 the hh term vanishes, so the natural-C (wrap) mode
-//        issues three products instead of four.
-// Output stage: wrap (natural-C semantics) or Q mode (round half up, shift,
-// saturate), both exact.
+// int8/int16 (kind::i8, P = 16, N = 16, tile 2048): an 8-bit core-matrix row
+//   is 16 bytes = 16 samples, so the no-swizzle K-major descriptor with
+//   LBO = 16 B and SBO = 128 B reads row a at byte 16a of the segment.
+//   int8: one s8 x s8 product.  int16: x = 256*xh + xl, g = 256*gh + gl (xh, gh
+//   signed bytes, xl, gl unsigned); y = 65536*hh + 256*(hl + lh) + ll, each an
+//   exact int32 kind::i8 accumulation recombined exactly in 64 bits; modulo
+//   2^16 the hh term vanishes, so the wrap mode issues three products.
+//   Output stage: wrap (natural-C) or Q mode (round half up, shift, saturate).
+//
+// float (split-BF16x3, kind::f16, P = 64, N = 128, tile 8192): each operand is
+//   split into BF16 hi + lo (lo = bf16(v - hi)); the signal planes are stored
+//   as consecutive 128-byte blocks of 64 samples in the 128-byte-swizzle
+//   K-major layout, whose 8-row atoms have a 128-byte row pitch, so with the
+//   descriptor starting at block kb row a reads block a + kb.  B rows 0..63
+//   hold g_hi by phase, rows 64..127 g_lo:
+//     MMA 1: D[:, 0:128] += A_hi x B        (x_hi*g_hi | x_hi*g_lo)
+//     MMA 2: D[:, 0:64]  += A_lo x B[0:64]  (x_lo*g_hi)
+//     y[j0 + 64a + b] = D[a][b] + D[a][64 + b]
+//
+// Each CTA owns consecutive tiles of one channel: the taps are staged into
+// shared memory once and the band built from there; the next tile's signal is
+// staged into the second buffer while the tensor core works on the current
+// one.  All waits on the tensor core are bounded; on expiry the kernel raises
+// g_firTcError, frees its TMEM and exits.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "dsplib_internal.h"
@@ -35,8 +45,11 @@ __device__ int g_firTcError; // set when a bounded wait for the tensor core give
 namespace {
 
 constexpr int kRows = 128;
+
+// ------------------------------------------------------------------ integer
+
 constexpr int kPhases = 16;
-constexpr int kTile = kRows * kPhases; // outputs per tile
+constexpr int kTile = kRows * kPhases;
 constexpr int kThreads = 128;
 constexpr int kMaxTapsTc = 2048;
 
@@ -56,6 +69,48 @@ __device__ __forceinline__ T outStage(long long acc, int shift)
    return (T) acc;
 }
 
+// Stage seg samples of xs into the byte plane(s): int8 -> A0; int16 -> A0 = high
+// (signed) bytes, A1 = low (unsigned) bytes.  16-byte vectors when aligned.
+template <typename T>
+__device__ __forceinline__ void intStage(const T *xs, long long j0, long long inExtent, int seg, unsigned char *A0,
+                                         unsigned char *A1, int tid)
+{
+   constexpr bool SPLIT = sizeof(T) == 2;
+   constexpr int per = 16 / sizeof(T); // samples per 16-byte vector
+   const bool full = j0 + seg <= inExtent;
+   if (full && (((uintptr_t) xs) & 15) == 0) {
+      for (int k = tid; k < seg / per; k += kThreads) {
+         const int4 v = ((const int4 *) xs)[k];
+         if (!SPLIT) {
+            ((int4 *) A0)[k] = v;
+         }
+         else {
+            const int16_t *e = (const int16_t *) &v;
+            __align__(8) unsigned char hb[8], lb[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+               hb[i] = (unsigned char) (e[i] >> 8);
+               lb[i] = (unsigned char) (e[i] & 0xFF);
+            }
+            ((uint2 *) A0)[k] = *(uint2 *) hb;
+            ((uint2 *) A1)[k] = *(uint2 *) lb;
+         }
+      }
+   }
+   else {
+      for (int k = tid; k < seg; k += kThreads) {
+         const int v = (j0 + k < inExtent) ? (int) xs[k] : 0;
+         if (SPLIT) {
+            A0[k] = (unsigned char) (v >> 8);
+            A1[k] = (unsigned char) (v & 0xFF);
+         }
+         else {
+            A0[k] = (unsigned char) v;
+         }
+      }
+   }
+}
+
 template <typename T, int QMODE>
 __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int tilesPerCta)
 {
@@ -63,14 +118,17 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
    constexpr uint32_t kCols = SPLIT ? 64 : 32; // TMEM columns (accumulators of 16 columns each)
    const int T_ = a.T;
    const int Kt = bandK(T_);
-   const int seg = kTile + Kt; // signal samples one tile reads (bytes per byte-plane)
+   const int seg = kTile + Kt;            // samples one tile reads (multiple of 32)
+   const int nplane = SPLIT ? 2 : 1;
    extern __shared__ __align__(128) unsigned char sm[];
    uint64_t *mbar = (uint64_t *) sm;
    uint32_t *tslot = (uint32_t *) (sm + 8);
-   unsigned char *B0 = sm + 16;
+   int *gtaps = (int *) (sm + 16);        // reversed taps g[c], c < T
+   unsigned char *B0 = sm + 16 + ((T_ * 4 + 15) & ~15);
    unsigned char *B1 = B0 + (size_t) Kt * 16;
-   unsigned char *A0 = B0 + (size_t) Kt * 16 * (SPLIT ? 2 : 1);
-   unsigned char *A1 = A0 + seg;
+   unsigned char *Abase = B0 + (size_t) Kt * 16 * nplane;
+   // A[buf][plane]: seg bytes each
+   auto A = [&](int buf, int plane) { return Abase + (size_t) (buf * nplane + plane) * seg; };
 
    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
    if (warp == 0) tc::tmemAlloc(tslot, kCols);
@@ -88,13 +146,14 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
       const T *x = (const T *) a.x + (long long) l * a.inPitch;
       const T *h = (const T *) a.h + (long long) l * a.filtPitch;
       T *y = (T *) a.y + (long long) l * a.outPitch;
+      for (int c = tid; c < T_; c += kThreads) gtaps[c] = (int) h[T_ - 1 - c];
+      __syncthreads();
       // Taps band, K-major no-swizzle: byte (q*256 + i*128 + r*16 + e) holds B[m = 16q + e][b = 8i + r].
       for (int idx = tid; idx < Kt * 16; idx += kThreads) {
          const int q = idx >> 8, rem = idx & 255;
          const int b = ((rem >> 7) << 3) + ((rem >> 4) & 7);
-         const int m = (q << 4) + (rem & 15);
-         const int c = m - b;
-         const int g = (c >= 0 && c < T_) ? (int) h[T_ - 1 - c] : 0;
+         const int c = (q << 4) + (rem & 15) - b;
+         const int g = (c >= 0 && c < T_) ? gtaps[c] : 0;
          if (SPLIT) {
             B0[idx] = (unsigned char) (g >> 8);
             B1[idx] = (unsigned char) (g & 0xFF);
@@ -105,31 +164,15 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
       }
       const int t0 = blockIdx.x * tilesPerCta;
       const int t1 = min(nt, t0 + tilesPerCta);
+      if (t0 < t1) intStage<T>(x + (long long) t0 * kTile, (long long) t0 * kTile, inExtent, seg, A(0, 0), A(0, 1), tid);
       for (int t = t0; t < t1; t++) {
+         const int buf = (t - t0) & 1;
          const long long j0 = (long long) t * kTile;
-         // Signal segment of this tile (zero past the row's extent).
-         const T *xs = x + j0;
-         const bool full = j0 + seg <= inExtent;
-         if (!SPLIT && full && (((uintptr_t) xs) & 15) == 0) {
-            for (int k = tid; k < seg / 16; k += kThreads) ((int4 *) A0)[k] = ((const int4 *) xs)[k];
-         }
-         else {
-            for (int k = tid; k < seg; k += kThreads) {
-               const int v = (full || j0 + k < inExtent) ? (int) xs[k] : 0;
-               if (SPLIT) {
-                  A0[k] = (unsigned char) (v >> 8);
-                  A1[k] = (unsigned char) (v & 0xFF);
-               }
-               else {
-                  A0[k] = (unsigned char) v;
-               }
-            }
-         }
          tc::fenceProxyAsync();
-         __syncthreads();
+         __syncthreads(); // segment[buf] and band written; previous accumulators drained
          if (tid == 0) {
             tc::fenceAfterSync();
-            const uint32_t a0 = tc::smemAddr(A0), a1 = tc::smemAddr(A1);
+            const uint32_t a0 = tc::smemAddr(A(buf, 0)), a1 = tc::smemAddr(A(buf, 1));
             const uint32_t b0 = tc::smemAddr(B0), b1 = tc::smemAddr(B1);
             for (int kk = 0; kk < Kt / 32; kk++) {
                const uint64_t dA0 = tc::descNoSwizzle(a0 + 32 * kk, 16, 128);
@@ -148,6 +191,7 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
             }
             tc::commit(mbar);
          }
+         if (t + 1 < t1) intStage<T>(x + j0 + kTile, j0 + kTile, inExtent, seg, A(buf ^ 1, 0), A(buf ^ 1, 1), tid);
          const bool done = tc::mbarWait(mbar, iter & 1);
          if (!done && tid == 0) atomicExch(&g_firTcError, 1);
          failed = __syncthreads_or(!done) != 0;
@@ -198,30 +242,217 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
             }
          }
          tc::fenceBeforeSync();
-         __syncthreads();
          if (failed) break;
       }
+      __syncthreads(); // before the next channel's taps overwrite the band
    }
    __syncthreads();
    if (warp == 0) tc::tmemFree(tmem, kCols);
+}
+
+// Tiles per CTA: a whole channel when there are enough channels to fill the
+// GPU several times over, else split so that at least ~2 waves of CTAs exist.
+inline int tilesPerCtaFor(int nt, int batch, int ctasPerSm)
+{
+   int tpc = nt;
+   while (tpc > 1 && (long long) ((nt + tpc - 1) / tpc) * batch < 148LL * ctasPerSm * 2) tpc = (tpc + 1) / 2;
+   return tpc;
 }
 
 template <typename T, int QMODE> cudaError_t launchIntTc(const FirLaunch &a, cudaStream_t s)
 {
    constexpr bool SPLIT = sizeof(T) == 2;
    const int Kt = bandK(a.T);
-   const size_t smem = 16 + (size_t) Kt * 16 * (SPLIT ? 2 : 1) + (size_t) (kTile + Kt) * (SPLIT ? 2 : 1);
+   const int nplane = SPLIT ? 2 : 1;
+   const size_t smem = 16 + (((size_t) a.T * 4 + 15) & ~(size_t) 15) + (size_t) Kt * 16 * nplane +
+                       2 * (size_t) nplane * (kTile + Kt);
    auto fn = fir_int_tc_kernel<T, QMODE>;
    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
    if (e != cudaSuccess) return e;
    const int nt = (a.outSize + kTile - 1) / kTile;
-   // Enough CTAs for several waves on 148 SMs while reusing the taps band across tiles.
-   int tpc = 1;
-   while (tpc < 8 && (long long) ((nt + tpc * 2 - 1) / (tpc * 2)) * a.batch >= 148 * 8) tpc *= 2;
+   const int tpc = tilesPerCtaFor(nt, a.batch, 8);
    dim3 grid((nt + tpc - 1) / tpc, a.batch < 65535 ? a.batch : 65535);
    fn<<<grid, kThreads, smem, s>>>(a, tpc);
    countLaunch();
    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ split-BF16x3
+
+constexpr int kBfPhases = 64;
+constexpr int kBfTile = kRows * kBfPhases;
+constexpr int kBfMaxTaps = 512;
+constexpr int kBfThreads = 256;
+constexpr int kBfChunksPerThread = 5; // 16-byte plane chunks staged per thread: bfBlocks(512) * 8 / 256
+constexpr int kBfPadLeft = 64;        // zero taps ahead of the reversed taps (phase offsets)
+
+__host__ __device__ inline int bfK(int T) { return ((63 + T + 15) / 16) * 16; }
+__host__ __device__ inline int bfBlocks(int T) { return kRows + (bfK(T) + 63) / 64; }
+__host__ __device__ inline int bfTapSlots(int T) { return kBfPadLeft + bfK(T) + 8; }
+
+__device__ __forceinline__ void splitBf16(float v, uint16_t &hi, uint16_t &lo)
+{
+   const __nv_bfloat16 h = __float2bfloat16_rn(v);
+   const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+   hi = __bfloat16_as_ushort(h);
+   lo = __bfloat16_as_ushort(l);
+}
+
+// Stage one tile's signal planes: sample i of the tile (64 per 128-byte block
+// k = i / 64) goes to block k, 16-byte chunk c = (i % 64) / 8 stored at
+// k*128 + ((c ^ (k & 7)) * 16), as hi and lo BF16.  All loads of a thread are
+// issued before any conversion so they overlap.
+__device__ __forceinline__ void bfStage(const float *xs, long long j0, long long inExtent, int nb,
+                                        unsigned char *Ahi, unsigned char *Alo, int tid)
+{
+   const bool vec = ((((uintptr_t) xs) & 15) == 0);
+   float f[kBfChunksPerThread][8];
+#pragma unroll
+   for (int u = 0; u < kBfChunksPerThread; u++) {
+      const int cidx = tid + u * kBfThreads;
+      if (cidx < nb * 8) {
+         const long long i0 = (long long) (cidx >> 3) * 64 + (cidx & 7) * 8;
+         if (vec && j0 + i0 + 8 <= inExtent) {
+            *(float4 *) &f[u][0] = *(const float4 *) (xs + i0);
+            *(float4 *) &f[u][4] = *(const float4 *) (xs + i0 + 4);
+         }
+         else {
+#pragma unroll
+            for (int e = 0; e < 8; e++) f[u][e] = (j0 + i0 + e < inExtent) ? xs[i0 + e] : 0.0f;
+         }
+      }
+   }
+#pragma unroll
+   for (int u = 0; u < kBfChunksPerThread; u++) {
+      const int cidx = tid + u * kBfThreads;
+      if (cidx < nb * 8) {
+         const int k = cidx >> 3, c = cidx & 7;
+         uint16_t hv[8], lv[8];
+#pragma unroll
+         for (int e = 0; e < 8; e++) splitBf16(f[u][e], hv[e], lv[e]);
+         const int off = k * 128 + ((c ^ (k & 7)) << 4);
+         *(uint4 *) (Ahi + off) = *(uint4 *) hv;
+         *(uint4 *) (Alo + off) = *(uint4 *) lv;
+      }
+   }
+}
+
+__global__ void __launch_bounds__(kBfThreads, 1) fir_bf16x3_tc_kernel(FirLaunch a, int tilesPerCta)
+{
+   const int T_ = a.T;
+   const int Kt = bfK(T_);
+   const int nb = bfBlocks(T_);
+   const int slots = bfTapSlots(T_);
+   extern __shared__ __align__(16) unsigned char smraw[];
+   unsigned char *sm = (unsigned char *) (((uintptr_t) smraw + 1023) & ~(uintptr_t) 1023);
+   const int planeBytes = (nb * 128 + 1023) & ~1023; // each plane starts on a 1024-byte swizzle atom
+   unsigned char *Ahi[2] = {sm, sm + 2 * planeBytes};
+   unsigned char *Alo[2] = {sm + planeBytes, sm + 3 * planeBytes};
+   unsigned char *Bt = sm + 4 * planeBytes;
+   uint16_t *gHi = (uint16_t *) (Bt + (size_t) Kt * 256); // reversed, split taps with zero padding
+   uint16_t *gLo = gHi + slots;
+   uint64_t *mbar = (uint64_t *) (((uintptr_t) (gLo + slots) + 15) & ~(uintptr_t) 15);
+   uint32_t *tslot = (uint32_t *) (mbar + 1);
+
+   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+   if (warp == 0) tc::tmemAlloc(tslot, 128);
+   if (tid == 0) tc::mbarInit(mbar, 1);
+   tc::fenceBeforeSync();
+   __syncthreads();
+   tc::fenceAfterSync();
+   const uint32_t tmem = *tslot;
+
+   const int nt = (a.outSize + kBfTile - 1) / kBfTile;
+   const long long inExtent = (long long) a.outSize + T_ - 1;
+   uint32_t iter = 0;
+   bool failed = false;
+   for (int l = blockIdx.y; l < a.batch && !failed; l += gridDim.y) {
+      const float *x = (const float *) a.x + (long long) l * a.inPitch;
+      const float *h = (const float *) a.h + (long long) l * a.filtPitch;
+      float *y = (float *) a.y + (long long) l * a.outPitch;
+      // g[c] = h[T-1-c] split into hi/lo, stored at slot c + kBfPadLeft; zero elsewhere.
+      for (int sl = tid; sl < slots; sl += kBfThreads) {
+         const int c = sl - kBfPadLeft;
+         uint16_t hi = 0, lo = 0;
+         if (c >= 0 && c < T_) splitBf16(h[T_ - 1 - c], hi, lo);
+         gHi[sl] = hi;
+         gLo[sl] = lo;
+      }
+      __syncthreads();
+      // Taps band, K-major no swizzle: 16-byte chunk (q, n) at q*2048 + (n/8)*128 + (n%8)*16 holds
+      // B[8q .. 8q+7][n]; rows n < 64: g_hi[m - n], rows n >= 64: g_lo[m - (n - 64)].
+      for (int cidx = tid; cidx < (Kt / 8) * 128; cidx += kBfThreads) {
+         const int q = cidx >> 7, n = cidx & 127;
+         const uint16_t *src = (n < 64 ? gHi : gLo) + kBfPadLeft + 8 * q - (n & 63);
+         __align__(16) uint16_t v[8];
+#pragma unroll
+         for (int e = 0; e < 8; e++) v[e] = src[e];
+         *(uint4 *) (Bt + q * 2048 + (n >> 3) * 128 + (n & 7) * 16) = *(uint4 *) v;
+      }
+      const int t0 = blockIdx.x * tilesPerCta;
+      const int t1 = min(nt, t0 + tilesPerCta);
+      if (t0 < t1) bfStage(x + (long long) t0 * kBfTile, (long long) t0 * kBfTile, inExtent, nb, Ahi[0], Alo[0], tid);
+      for (int t = t0; t < t1; t++) {
+         const int buf = (t - t0) & 1;
+         const long long j0 = (long long) t * kBfTile;
+         tc::fenceProxyAsync();
+         __syncthreads(); // planes[buf] and band written; previous tile's accumulator drained
+         if (tid == 0) {
+            tc::fenceAfterSync();
+            const uint32_t ahi = tc::smemAddr(Ahi[buf]), alo = tc::smemAddr(Alo[buf]), bt = tc::smemAddr(Bt);
+            const uint32_t id128 = tc::idesc(1, 1, 1, kRows, 128), id64 = tc::idesc(1, 1, 1, kRows, 64);
+            for (int k16 = 0; k16 < Kt / 16; k16++) {
+               const int blk = k16 >> 2, sub = k16 & 3;
+               // The swizzle is applied on absolute shared-memory address bits, so a start
+               // that is not atom-aligned (block blk of the plane) keeps base offset 0.
+               const uint64_t dHi = tc::descSw128(ahi + blk * 128 + sub * 32, 1024, 0);
+               const uint64_t dLo = tc::descSw128(alo + blk * 128 + sub * 32, 1024, 0);
+               const uint64_t dB = tc::descNoSwizzle(bt + k16 * 4096, 2048, 128);
+               tc::mmaF16(tmem, dHi, dB, id128, k16 > 0);
+               tc::mmaF16(tmem, dLo, dB, id64, true);
+            }
+            tc::commit(mbar);
+         }
+         // Stage the next tile into the other buffer while the tensor core works.
+         if (t + 1 < t1)
+            bfStage(x + j0 + kBfTile, j0 + kBfTile, inExtent, nb, Ahi[buf ^ 1], Alo[buf ^ 1], tid);
+         const bool done = tc::mbarWait(mbar, iter & 1);
+         if (!done && tid == 0) atomicExch(&g_firTcError, 1);
+         failed = __syncthreads_or(!done) != 0;
+         iter++;
+         tc::fenceAfterSync();
+         if (!failed) {
+            // Warp w drains TMEM lane quadrant w % 4 (rows a) and output half w / 4:
+            // y[j0 + 64a + 32*half + b] = D[a][32*half + b] + D[a][64 + 32*half + b].
+            const int quad = warp & 3, half = warp >> 2;
+            const uint32_t lanes = (uint32_t) (quad * 32) << 16;
+            const int row = quad * 32 + lane;
+            const long long jr = j0 + (long long) row * kBfPhases + half * 32;
+            float *yr = y + jr;
+            uint32_t p[32], q[32];
+            tc::tmemLoad32(tmem + lanes + half * 32, p);
+            tc::tmemLoad32(tmem + lanes + 64 + half * 32, q);
+            tc::tmemWaitLoad();
+            __align__(16) float o[32];
+#pragma unroll
+            for (int b = 0; b < 32; b++) o[b] = __uint_as_float(p[b]) + __uint_as_float(q[b]);
+            if (jr + 32 <= a.outSize && ((((uintptr_t) yr) & 15) == 0)) {
+#pragma unroll
+               for (int v4 = 0; v4 < 8; v4++) ((float4 *) yr)[v4] = ((float4 *) o)[v4];
+            }
+            else {
+#pragma unroll
+               for (int b = 0; b < 32; b++)
+                  if (jr + b < a.outSize) yr[b] = o[b];
+            }
+         }
+         tc::fenceBeforeSync();
+         if (failed) break;
+      }
+      __syncthreads(); // before the taps band of the next channel is rebuilt
+   }
+   __syncthreads();
+   if (warp == 0) tc::tmemFree(tmem, 128);
 }
 
 } // namespace
@@ -238,6 +469,25 @@ cudaError_t launchFirIntTc(const FirLaunch &a, bool qmode, cudaStream_t s)
    return cudaErrorInvalidValue;
 }
 
+bool firBf16x3Supported(const FirLaunch &a) { return a.dtype == DSPLIB_FLOAT32 && a.T >= 1 && a.T <= kBfMaxTaps; }
+
+cudaError_t launchFirBf16x3(const FirLaunch &a, cudaStream_t s)
+{
+   if (!firBf16x3Supported(a)) return cudaErrorNotSupported;
+   const int Kt = bfK(a.T), nb = bfBlocks(a.T);
+   const size_t planes = 4 * (size_t) ((nb * 128 + 1023) & ~1023); // hi and lo, double-buffered
+   const size_t smem = 1024 + planes + (size_t) Kt * 256 + 4 * (size_t) bfTapSlots(a.T) + 32;
+   cudaError_t e =
+       cudaFuncSetAttribute(fir_bf16x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+   if (e != cudaSuccess) return e;
+   const int nt = (a.outSize + kBfTile - 1) / kBfTile;
+   const int tpc = tilesPerCtaFor(nt, a.batch, 1);
+   dim3 grid((nt + tpc - 1) / tpc, a.batch < 65535 ? a.batch : 65535);
+   fir_bf16x3_tc_kernel<<<grid, kBfThreads, smem, s>>>(a, tpc);
+   countLaunch();
+   return cudaGetLastError();
+}
+
 int firTcErrorFlag(bool clear)
 {
    int v = 0;
@@ -247,13 +497,6 @@ int firTcErrorFlag(bool clear)
       cudaMemcpyToSymbol(g_firTcError, &z, sizeof(int));
    }
    return v;
-}
-
-cudaError_t launchFirBf16x3(const FirLaunch &a, cudaStream_t s)
-{
-   (void) a;
-   (void) s;
-   return cudaErrorNotSupported;
 }
 
 } // namespace dsplib

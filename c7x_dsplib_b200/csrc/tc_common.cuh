@@ -27,6 +27,24 @@ __device__ __forceinline__ uint64_t descNoSwizzle(uint32_t saddr, uint32_t lbo, 
    return d;                // layout type 0: no swizzle
 }
 
+// K-major operand with 128-byte swizzle: 8-row atoms of 128-byte rows (row
+// pitch 128 B), 16-byte chunks permuted by chunk ^= (address bits 7..9);
+// sbo = byte distance between consecutive 8-row groups.  The permutation is
+// taken from the absolute address, so data stored swizzled by address can be
+// read from any 128-byte-aligned start with baseOffset = 0 (measured on B200:
+// a non-zero base offset for such starts reads the wrong chunks).
+__device__ __forceinline__ uint64_t descSw128(uint32_t saddr, uint32_t sbo, uint32_t baseOffset)
+{
+   uint64_t d = 0;
+   d |= (uint64_t) ((saddr >> 4) & 0x3FFF);
+   d |= (uint64_t) 1 << 16; // leading byte offset: unused for swizzled K-major, encoded as 1
+   d |= (uint64_t) ((sbo >> 4) & 0x3FFF) << 32;
+   d |= (uint64_t) 1 << 46;
+   d |= (uint64_t) (baseOffset & 7) << 49;
+   d |= (uint64_t) 2 << 61; // layout type: 128-byte swizzle
+   return d;
+}
+
 // Instruction descriptor.  dfmt: 1 = F32, 2 = S32.  afmt/bfmt: kind::i8 -> 0 unsigned, 1 signed;
 // kind::f16 -> 0 F16, 1 BF16.  Both operands K-major.
 __host__ __device__ constexpr uint32_t idesc(uint32_t dfmt, uint32_t afmt, uint32_t bfmt, uint32_t M, uint32_t N)
@@ -109,6 +127,20 @@ __device__ __forceinline__ void tmemLoad16(uint32_t taddr, uint32_t (&r)[16])
                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
                   "=r"(r[15])
+                : "r"(taddr));
+}
+
+// 32 lanes x 32 consecutive 32-bit columns.
+__device__ __forceinline__ void tmemLoad32(uint32_t taddr, uint32_t (&r)[32])
+{
+   asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
                 : "r"(taddr));
 }
 

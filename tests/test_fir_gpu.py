@@ -136,6 +136,57 @@ def test_simt_float_accuracy(nch):
         assert np.max(np.abs(y - oracle.fir(x, h, T, nch=nch))) <= TOL_REF
 
 
+def lowpass(rng, rows, T):
+    """Hamming-windowed sinc low-pass, cutoff U[0.05, 0.45], unit DC gain (stored tap order)."""
+    n = np.arange(T) - (T - 1) / 2.0
+    out = np.zeros((rows, T), np.float32)
+    for r in range(rows):
+        fc = rng.uniform(0.05, 0.45)
+        hh = fc * np.sinc(fc * n) * np.hamming(T) if T > 1 else np.ones(1)
+        out[r] = (hh / hh.sum())[::-1]
+    return out
+
+
+@pytest.mark.parametrize("nch", [0, 1])
+def test_bf16x3_accuracy(nch):
+    """Split-BF16x3 tensor-core FIR: max |y - y64| / max |y64| <= 1e-5 per channel
+    (N(0,1) input, windowed-sinc taps as in the FP32 FIR workload), and the
+    reference criterion abs 2^-10 against the natural-C result."""
+    rng = np.random.default_rng(31 + nch)
+    for (B, N, T) in [(2, 9000, 1), (3, 70000, 256), (2, 5000, 512), (2, 3000, 100), (1, 300, 255)]:
+        x = rng.standard_normal((B, N)).astype(np.float32)
+        hh = lowpass(rng, B if nch else 1, T)
+        y = host(D.fir(dev(x), dev(hh), T, nch=nch, precision=D.FIR_BF16X3))
+        y64 = oracle.fir_f64(x, hh, T, nch=nch)
+        assert np.max(_relerr(y, y64)) <= 1e-5, (B, N, T)
+        assert np.max(np.abs(y - oracle.fir(x, hh, T, nch=nch))) <= TOL_REF
+
+
+def test_bf16x3_long_filter_uses_fp32_kernel():
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((2, 3000)).astype(np.float32)
+    hh = (rng.standard_normal((2, 700)) / 30).astype(np.float32)
+    y = host(D.fir(dev(x), dev(hh), 700, nch=1, precision=D.FIR_BF16X3))
+    assert np.max(_relerr(y, oracle.fir_f64(x, hh, 700, nch=1))) <= 2e-6
+
+
+def test_bf16x3_unaligned_rows():
+    rng = np.random.default_rng(6)
+    B, N, T, pitch = 3, 20001, 64, 20003
+    x = np.zeros((B, pitch), np.float32)
+    x[:, :N] = rng.standard_normal((B, N))
+    hh = lowpass(rng, 1, T)
+    args, pin, pfilt, pout = D.fir_setup(D.FLOAT32, B, N, T, nch=0, in_pitch=pitch, out_pitch=N - T + 3)
+    out = np.zeros((B, N - T + 3), np.float32)
+    h = D.FirHandle()
+    assert h.init(args, pin, pfilt, pout) == D.SUCCESS
+    h.set_precision(D.FIR_BF16X3)
+    xd, hd, od = dev(x), dev(hh), dev(out)
+    assert h.exec(xd, hd, od) == D.SUCCESS, h.last_error()
+    y64 = oracle.fir_f64(np.ascontiguousarray(x[:, :N]), hh, T, nch=0)
+    assert np.max(_relerr(host(od)[:, : N - T + 1], y64)) <= 1e-5
+
+
 def _golden_cases():
     import os
 
