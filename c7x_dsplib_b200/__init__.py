@@ -92,6 +92,13 @@ SIGNATURES = {
     "DSPLIB_gpu_firSetPrecision": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_firSetQMode": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_kernelLaunchCount": (ctypes.c_int64, []),
+    "DSPLIB_gpu_raggedPlanCreate": (ctypes.c_int, [_P(_VP), ctypes.c_int32, _P(ctypes.c_int32),
+                                                   _P(ctypes.c_int32), _P(ctypes.c_int32)]),
+    "DSPLIB_gpu_raggedPlanSize": (ctypes.c_int64, [_VP, ctypes.c_int32]),
+    "DSPLIB_gpu_raggedPlanDestroy": (ctypes.c_int, [_VP]),
+    "DSPLIB_gpu_firBiquadBatched_fwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "DSPLIB_gpu_firBiquadBatched_bwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "DSPLIB_gpu_raggedMseGrad": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
 }
 
 

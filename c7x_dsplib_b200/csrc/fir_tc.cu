@@ -111,6 +111,51 @@ __device__ __forceinline__ void intStage(const T *xs, long long j0, long long in
    }
 }
 
+// Write n consecutive outputs dst[0..n) of one tile from shared memory, where
+// the tile's 16-byte chunk ci (bytes 16ci .. 16ci+15 of the output run) sits at
+// byte offset cpos(ci) of stage.  The accumulator drain leaves one output row
+// per lane, so storing straight from registers would make every lane of a warp
+// hit a different row (one memory transaction per lane and instruction); from
+// shared memory a warp writes contiguous 16-byte vectors instead.  The vectors
+// are aligned to the destination: when dst is not 16-byte aligned (row pitches
+// such as N - T + 1 elements), each vector is assembled from two stage chunks
+// with a funnel shift, and a head and tail of scalar stores cover the ends.
+template <typename T, typename ChunkPos>
+__device__ __forceinline__ void storeTile(T *dst, int n, const unsigned char *stage, ChunkPos cpos, int tid,
+                                          int nthreads)
+{
+   auto elem = [&](int k) {
+      const int byte = k * (int) sizeof(T);
+      return *(const T *) (stage + cpos(byte >> 4) + (byte & 15));
+   };
+   const int hb = (16 - (int) ((uintptr_t) dst & 15)) & 15; // bytes before the first 16-byte boundary
+   const int head = min(n, hb / (int) sizeof(T));
+   const int nvec = (n - head) * (int) sizeof(T) / 16;
+   if (tid < head) dst[tid] = elem(tid);
+   const int q = hb >> 2, r = (hb & 3) * 8;
+   unsigned char *dv = (unsigned char *) dst + hb;
+   for (int v = tid; v < nvec; v += nthreads) {
+      const uint4 a = *(const uint4 *) (stage + cpos(v));
+      uint4 o = a;
+      if (hb) {
+         const uint4 b = *(const uint4 *) (stage + cpos(v + 1));
+         uint32_t w0, w1, w2, w3, w4;
+         switch (q) { // uniform across the CTA
+         case 0: w0 = a.x, w1 = a.y, w2 = a.z, w3 = a.w, w4 = b.x; break;
+         case 1: w0 = a.y, w1 = a.z, w2 = a.w, w3 = b.x, w4 = b.y; break;
+         case 2: w0 = a.z, w1 = a.w, w2 = b.x, w3 = b.y, w4 = b.z; break;
+         default: w0 = a.w, w1 = b.x, w2 = b.y, w3 = b.z, w4 = b.w; break;
+         }
+         o.x = __funnelshift_r(w0, w1, r);
+         o.y = __funnelshift_r(w1, w2, r);
+         o.z = __funnelshift_r(w2, w3, r);
+         o.w = __funnelshift_r(w3, w4, r);
+      }
+      *(uint4 *) (dv + 16 * v) = o;
+   }
+   for (int k = head + nvec * (16 / (int) sizeof(T)) + tid; k < n; k += nthreads) dst[k] = elem(k);
+}
+
 template <typename T, int QMODE>
 __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int tilesPerCta)
 {
@@ -129,6 +174,7 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
    unsigned char *Abase = B0 + (size_t) Kt * 16 * nplane;
    // A[buf][plane]: seg bytes each
    auto A = [&](int buf, int plane) { return Abase + (size_t) (buf * nplane + plane) * seg; };
+   T *ostage = (T *) (Abase + (size_t) 2 * nplane * seg); // one tile of outputs, row-major
 
    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
    if (warp == 0) tc::tmemAlloc(tslot, kCols);
@@ -208,7 +254,6 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
             }
             tc::tmemWaitLoad();
             const int row = warp * 32 + lane;
-            const long long jr = j0 + (long long) row * kPhases;
             __align__(16) T out[16];
 #pragma unroll
             for (int b = 0; b < 16; b++) {
@@ -225,24 +270,15 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
                }
                out[b] = outStage<T, QMODE>(v, a.shift);
             }
-            T *yr = y + jr;
-            if (jr + 16 <= a.outSize && (((uintptr_t) yr) & 15) == 0) {
-               if (SPLIT) {
-                  ((int4 *) yr)[0] = *(int4 *) &out[0];
-                  ((int4 *) yr)[1] = *(int4 *) &out[8];
-               }
-               else {
-                  *(int4 *) yr = *(int4 *) &out[0];
-               }
-            }
-            else {
-#pragma unroll
-               for (int b = 0; b < 16; b++)
-                  if (jr + b < a.outSize) yr[b] = out[b];
-            }
+            int4 *os = (int4 *) (ostage + row * kPhases);
+            os[0] = *(int4 *) &out[0];
+            if (SPLIT) os[1] = *(int4 *) &out[8];
          }
          tc::fenceBeforeSync();
          if (failed) break;
+         __syncthreads(); // the output tile is complete in shared memory
+         storeTile<T>(y + j0, (int) min((long long) kTile, (long long) a.outSize - j0),
+                      (const unsigned char *) ostage, [](int ci) { return ci * 16; }, tid, kThreads);
       }
       __syncthreads(); // before the next channel's taps overwrite the band
    }
@@ -265,7 +301,7 @@ template <typename T, int QMODE> cudaError_t launchIntTc(const FirLaunch &a, cud
    const int Kt = bandK(a.T);
    const int nplane = SPLIT ? 2 : 1;
    const size_t smem = 16 + (((size_t) a.T * 4 + 15) & ~(size_t) 15) + (size_t) Kt * 16 * nplane +
-                       2 * (size_t) nplane * (kTile + Kt);
+                       2 * (size_t) nplane * (kTile + Kt) + (size_t) kTile * sizeof(T);
    auto fn = fir_int_tc_kernel<T, QMODE>;
    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
    if (e != cudaSuccess) return e;
@@ -427,27 +463,34 @@ __global__ void __launch_bounds__(kBfThreads, 1) fir_bf16x3_tc_kernel(FirLaunch 
             const int quad = warp & 3, half = warp >> 2;
             const uint32_t lanes = (uint32_t) (quad * 32) << 16;
             const int row = quad * 32 + lane;
-            const long long jr = j0 + (long long) row * kBfPhases + half * 32;
-            float *yr = y + jr;
             uint32_t p[32], q[32];
             tc::tmemLoad32(tmem + lanes + half * 32, p);
             tc::tmemLoad32(tmem + lanes + 64 + half * 32, q);
             tc::tmemWaitLoad();
-            __align__(16) float o[32];
+            // The planes of this buffer are free once the MMAs completed: they hold the
+            // output tile, 16-byte chunk v4 of row half (row, half) rotated to slot
+            // (v4 + row) & 7 so that eight consecutive rows store to distinct banks.
+            float *os = (float *) Ahi[buf] + row * kBfPhases + half * 32;
 #pragma unroll
-            for (int b = 0; b < 32; b++) o[b] = __uint_as_float(p[b]) + __uint_as_float(q[b]);
-            if (jr + 32 <= a.outSize && ((((uintptr_t) yr) & 15) == 0)) {
-#pragma unroll
-               for (int v4 = 0; v4 < 8; v4++) ((float4 *) yr)[v4] = ((float4 *) o)[v4];
-            }
-            else {
-#pragma unroll
-               for (int b = 0; b < 32; b++)
-                  if (jr + b < a.outSize) yr[b] = o[b];
+            for (int v4 = 0; v4 < 8; v4++) {
+               float4 o;
+               o.x = __uint_as_float(p[4 * v4 + 0]) + __uint_as_float(q[4 * v4 + 0]);
+               o.y = __uint_as_float(p[4 * v4 + 1]) + __uint_as_float(q[4 * v4 + 1]);
+               o.z = __uint_as_float(p[4 * v4 + 2]) + __uint_as_float(q[4 * v4 + 2]);
+               o.w = __uint_as_float(p[4 * v4 + 3]) + __uint_as_float(q[4 * v4 + 3]);
+               *(float4 *) (os + (((v4 + row) & 7) << 2)) = o;
             }
          }
          tc::fenceBeforeSync();
          if (failed) break;
+         __syncthreads(); // the output tile is complete in shared memory
+         storeTile<float>(y + j0, (int) min((long long) kBfTile, (long long) a.outSize - j0),
+                          (const unsigned char *) Ahi[buf],
+                          [](int ci) {
+                             const int row = ci >> 4, half = (ci >> 3) & 1, v4 = ci & 7;
+                             return (row * kBfPhases + half * 32 + (((v4 + row) & 7) << 2)) * 4;
+                          },
+                          tid, kBfThreads);
       }
       __syncthreads(); // before the taps band of the next channel is rebuilt
    }

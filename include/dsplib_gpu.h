@@ -46,6 +46,62 @@ DSPLIB_STATUS DSPLIB_gpu_firSetQMode(DSPLIB_kernelHandle handle, int32_t enable)
 /** Number of CUDA kernels this library has launched in this process. */
 int64_t DSPLIB_gpu_kernelLaunchCount(void);
 
+/* ---------------------------------------------------------------------------
+ * Batched filter bank over channels of uneven length, forward and adjoint.
+ * Per channel c (length L_c, T_c taps, S_c second-order stages):
+ *     u_c = DSPLIB_fir valid correlation of x_c with h_c      (L_c - T_c + 1 samples)
+ *     y_c = S_c cascaded direct-form-II biquads applied to u_c from a zero state
+ * Every buffer is FP32 in device memory, channels packed back to back:
+ *     x, y, gx, gy: channel c at sample offset sum_{k<c} L_k (y and gy use the
+ *                   first L_c - T_c + 1 samples; the remaining T_c - 1 of y are
+ *                   written as zero and those of gy are ignored);
+ *     taps, gtaps:  channel c at offset sum_{k<c} T_k, same tap order as DSPLIB_fir;
+ *     coefs, gcoefs: channel c at offset 5 * sum_{k<c} S_k, rows [b0 b1 b2 a1 a2]
+ *                   (a0 = 1; y[t] = b0 w[t] + b1 w[t-1] + b2 w[t-2],
+ *                    w[t] = u[t] - a1 w[t-1] - a2 w[t-2]).
+ * The reference has no counterpart: it filters one channel layout at a time and
+ * has no gradients; these entry points serve a training loop over many filters
+ * (the fused form of DSPLIB_fir followed by DSPLIB_cascadeBiquad).
+ * ------------------------------------------------------------------------- */
+typedef struct DSPLIB_gpu_raggedPlan_s *DSPLIB_gpu_raggedPlan;
+
+typedef enum {
+   DSPLIB_GPU_RAGGED_SAMPLES = 0, /* floats in x / gx (sum L_c) */
+   DSPLIB_GPU_RAGGED_TAPS = 1,    /* floats in taps / gtaps (sum T_c) */
+   DSPLIB_GPU_RAGGED_COEFS = 2,   /* floats in coefs / gcoefs (5 sum S_c) */
+   DSPLIB_GPU_RAGGED_WORK = 3,    /* floats of the forward activations (max S_c + 1) * sum L_c */
+   DSPLIB_GPU_RAGGED_SCRATCH = 4, /* floats of adjoint scratch */
+   DSPLIB_GPU_RAGGED_OUTPUTS = 5, /* valid output samples (sum L_c - T_c + 1) */
+} DSPLIB_gpu_raggedSize;
+
+/** Build a plan (per-channel offsets and work lists, uploaded to the current
+ *  device).  1 <= T_c <= 512, T_c <= L_c, 0 <= S_c <= 64, else
+ *  DSPLIB_ERR_INVALID_DIMENSION.  The plan may be used from any stream of that device. */
+DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t numChannels, const int32_t *length,
+                                          const int32_t *taps, const int32_t *stages);
+/** Buffer sizes in floats (DSPLIB_gpu_raggedSize); -1 for an unknown query. */
+int64_t DSPLIB_gpu_raggedPlanSize(DSPLIB_gpu_raggedPlan plan, int32_t what);
+DSPLIB_STATUS DSPLIB_gpu_raggedPlanDestroy(DSPLIB_gpu_raggedPlan plan);
+
+/** Forward: y from x, taps and coefs.  work receives the FIR output and every
+ *  stage's output (kept for the adjoint).  Queued on `stream`; no allocation,
+ *  no host synchronisation. */
+DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_fwd(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
+                                              const float *coefs, float *y, float *work, void *stream);
+/** Adjoint: given gy = dLoss/dy and the forward's work buffer, writes
+ *  gx = dLoss/dx, gtaps = dLoss/dtaps and gcoefs = dLoss/dcoefs.  scratch holds
+ *  DSPLIB_GPU_RAGGED_SCRATCH floats (no initial contents needed).  Reductions
+ *  run in a fixed order: results are bitwise repeatable. */
+DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
+                                              const float *coefs, const float *work, const float *gy, float *gx,
+                                              float *gtaps, float *gcoefs, float *scratch, void *stream);
+/** Mean squared error over the valid output samples and its gradient:
+ *  loss[0] = sum (y - target)^2 / n (n = DSPLIB_GPU_RAGGED_OUTPUTS, FP64 sums in
+ *  a fixed order), gy = 2 (y - target) / n, zero on the tail samples.  scratch
+ *  is a DSPLIB_GPU_RAGGED_SCRATCH buffer (the same one the adjoint takes). */
+DSPLIB_STATUS DSPLIB_gpu_raggedMseGrad(DSPLIB_gpu_raggedPlan plan, const float *y, const float *target, float *gy,
+                                       float *loss, float *scratch, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
