@@ -92,6 +92,7 @@ SIGNATURES = {
     "DSPLIB_gpu_firSetPrecision": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_firSetQMode": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_kernelLaunchCount": (ctypes.c_int64, []),
+    "DSPLIB_gpu_releaseHandle": (ctypes.c_int, [_VP]),
     "DSPLIB_gpu_raggedPlanCreate": (ctypes.c_int, [_P(_VP), ctypes.c_int32, _P(ctypes.c_int32),
                                                    _P(ctypes.c_int32), _P(ctypes.c_int32)]),
     "DSPLIB_gpu_raggedPlanSize": (ctypes.c_int64, [_VP, ctypes.c_int32]),

@@ -62,6 +62,7 @@ namespace {
 
 using scan::M2;
 
+
 constexpr int kRTile = 2048;
 constexpr int kRThreads = 256;
 constexpr int kRTaps = 256;
@@ -128,6 +129,7 @@ constexpr int kBL = 16;                 // samples per chunk
 constexpr int kBWindow = kBThreads * kBL;
 constexpr int kBPad = kBL + 1;          // padded shared row per chunk (bank-conflict free)
 constexpr int kBPowers = 10;            // M^(2^k), M = A^16, k = 0..9 (M^512 spans a window)
+constexpr int kRaggedMaxStages = 64;
 
 __device__ __forceinline__ void df2Chunk(float (&v)[kBL], const float *cf, float &w1, float &w2, bool write)
 {
@@ -152,19 +154,31 @@ __global__ void __launch_bounds__(kBThreads, 1)
 {
    __shared__ float sbuf[kBThreads * kBPad];
    __shared__ double2 sTot[kBWarps];
-   __shared__ M2 sPow[2][kBPowers];
-   extern __shared__ double2 sWin[]; // carry per stage
+   extern __shared__ __align__(16) unsigned char dyn[];
+   double2 *sWin = (double2 *) dyn;                      // carry per stage
+   M2 *sPow = (M2 *) (dyn + kRaggedMaxStages * sizeof(double2)); // M^(2^k) per stage
 
    const RaggedChan c = chans[order[blockIdx.x]];
    const int nst = BWD ? 1 : c.S;
    if (BWD && c.S <= stage) return; // uniform per CTA
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
    const int Lu = c.Lu;
-   for (int s = tid; s < nst; s += kBThreads) sWin[s] = make_double2(0.0, 0.0);
    const float *cbase = coefs + c.cOff;
+   // Per stage: zero carry and the powers M^(2^k), M = A^16, of its transition matrix.
+   for (int s = tid; s < nst; s += kBThreads) {
+      const int si = BWD ? stage : s;
+      sWin[s] = make_double2(0.0, 0.0);
+      M2 A = {-(double) cbase[si * 5 + 3], -(double) cbase[si * 5 + 4], 1.0, 0.0};
+#pragma unroll
+      for (int r = 1; r < kBL; r <<= 1) A = scan::mmul(A, A);
+      sPow[s * kBPowers] = A;
+      for (int k = 1; k < kBPowers; k++) {
+         A = scan::mmul(A, A);
+         sPow[s * kBPowers + k] = A;
+      }
+   }
    const float *src = BWD ? gin + c.xOff : planes + c.xOff;
    __syncthreads();
-   int phase = 0;
    for (int win0 = 0; win0 < Lu; win0 += kBWindow) {
       // Stage the window through shared memory (coalesced), reversed in time for the adjoint.
       for (int k = tid; k < kBWindow; k += kBThreads) {
@@ -191,22 +205,11 @@ __global__ void __launch_bounds__(kBThreads, 1)
 #pragma unroll
             for (int k = 0; k < 5; k++) cf[k] = cbase[si * 5 + k];
          }
-         M2 *P = sPow[phase & 1];
-         if (tid == 0) {
-            M2 A = {-(double) cf[3], -(double) cf[4], 1.0, 0.0};
-#pragma unroll
-            for (int r = 1; r < kBL; r <<= 1) A = scan::mmul(A, A);
-            P[0] = A;
-            for (int k = 1; k < kBPowers; k++) {
-               A = scan::mmul(A, A);
-               P[k] = A;
-            }
-         }
+         const M2 *P = sPow + s * kBPowers;
          // 1. zero-state end state of this chunk
          float w1 = 0.f, w2 = 0.f;
          df2Chunk(v, cf, w1, w2, false);
          // 2. warp-level inclusive scan over 32 chunks
-         __syncthreads(); // publishes P
          double2 val = make_double2(w1, w2);
 #pragma unroll
          for (int k = 0; k < 5; k++) {
@@ -262,7 +265,6 @@ __global__ void __launch_bounds__(kBThreads, 1)
                if (!BWD && s == nst - 1) yout[c.xOff + tau] = o;
             }
          }
-         phase++;
       }
       __syncthreads();
    }
@@ -274,75 +276,131 @@ __global__ void __launch_bounds__(kBThreads, 1)
    }
 }
 
-// Input gradient (in place over g) and the coefficient gradients of one stage.
-__global__ void __launch_bounds__(256) biquad_ragged_bwd_kernel(const RaggedChan *chans, const float *coefs,
-                                                                 const float *planes, long long planeStride,
-                                                                 const float *v, float *g, float *gcoefs, int stage)
+// Input gradient (in place over g) of one stage and per-item partial sums of
+// its five coefficient gradients (FP64, one row of 5 per item).  Item
+// (channel, tile) covers t in [j0, j0 + 2048) of the channel; the stage's v, u
+// and y around the tile are staged in shared memory.
+__global__ void __launch_bounds__(256) biquad_ragged_bwd_kernel(const RaggedChan *chans, const int2 *items,
+                                                                 const float *coefs, const float *planes,
+                                                                 long long planeStride, const float *v,
+                                                                 float *g, double *part, int stage)
 {
-   const RaggedChan c = chans[blockIdx.x];
-   if (c.S <= stage) return;
-   const float *cf = coefs + c.cOff + stage * 5;
-   const float b0 = cf[0], b1 = cf[1], b2 = cf[2];
+   __shared__ float sv[kRTile + 2], su[kRTile + 2], sy[kRTile + 2];
+   __shared__ double red[5][256];
+   const int2 it = items[blockIdx.x];
+   const RaggedChan c = chans[it.x];
+   if (c.S <= stage) return; // uniform per CTA
+   const int tid = threadIdx.x;
+   const int j0 = it.y * kRTile;
+   const int n = min(kRTile, c.Lu - j0);
    const float *u = planes + (long long) stage * planeStride + c.xOff;
    const float *y = planes + (long long) (stage + 1) * planeStride + c.xOff;
    const float *vv = v + c.xOff;
-   float *gg = g + c.xOff;
-   const int Lu = c.Lu;
-   double acc[5] = {0, 0, 0, 0, 0};
-   for (int t = threadIdx.x; t < Lu; t += blockDim.x) {
-      const float vt = vv[t];
-      const float v1 = t + 1 < Lu ? vv[t + 1] : 0.0f;
-      const float v2 = t + 2 < Lu ? vv[t + 2] : 0.0f;
-      gg[t] = fmaf(b0, vt, fmaf(b1, v1, b2 * v2));
-      acc[0] += (double) vt * u[t];
-      if (t >= 1) {
-         acc[1] += (double) vt * u[t - 1];
-         acc[3] -= (double) vt * y[t - 1];
-      }
-      if (t >= 2) {
-         acc[2] += (double) vt * u[t - 2];
-         acc[4] -= (double) vt * y[t - 2];
+   // sv[k] = v[j0 + k] (zero past the channel); su[k] = u[j0 - 2 + k], sy[k] = y[j0 - 2 + k] (zero before 0)
+   for (int k = tid; k < kRTile + 2; k += 256) {
+      const int tv = j0 + k, tu = j0 - 2 + k;
+      sv[k] = tv < c.Lu ? vv[tv] : 0.0f;
+      const bool inU = tu >= 0 && tu < j0 + n;
+      su[k] = inU ? u[tu] : 0.0f;
+      sy[k] = inU ? y[tu] : 0.0f;
+   }
+   __syncthreads();
+   const float *cf = coefs + c.cOff + stage * 5;
+   const float b0 = cf[0], b1 = cf[1], b2 = cf[2];
+   float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+   float *gg = g + c.xOff + j0;
+#pragma unroll
+   for (int i = 0; i < kRTile / 256; i++) {
+      const int k = i * 256 + tid;
+      if (k < n) {
+         const float vt = sv[k];
+         gg[k] = fmaf(b0, vt, fmaf(b1, sv[k + 1], b2 * sv[k + 2]));
+         acc[0] = fmaf(vt, su[k + 2], acc[0]);
+         acc[1] = fmaf(vt, su[k + 1], acc[1]);
+         acc[2] = fmaf(vt, su[k], acc[2]);
+         acc[3] = fmaf(-vt, sy[k + 1], acc[3]);
+         acc[4] = fmaf(-vt, sy[k], acc[4]);
       }
    }
-   __shared__ double red[5][256];
 #pragma unroll
-   for (int k = 0; k < 5; k++) red[k][threadIdx.x] = acc[k];
+   for (int q = 0; q < 5; q++) red[q][tid] = acc[q];
    __syncthreads();
    for (int w = 128; w > 0; w >>= 1) {
-      if ((int) threadIdx.x < w)
+      if (tid < w)
 #pragma unroll
-         for (int k = 0; k < 5; k++) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+         for (int q = 0; q < 5; q++) red[q][tid] += red[q][tid + w];
       __syncthreads();
    }
-   if (threadIdx.x < 5) gcoefs[c.cOff + stage * 5 + threadIdx.x] = (float) red[threadIdx.x][0];
+   if (tid < 5) part[(long long) blockIdx.x * 5 + tid] = red[tid][0];
 }
 
-// Taps gradient, partial over one (channel, tile) item: part[item][c] = sum_{j in tile} gu[j] x[j + c].
+// Coefficient gradients of one stage: the item partials of each channel summed in item order.
+__global__ void __launch_bounds__(32) biquad_coef_reduce_kernel(const RaggedChan *chans, const int *start,
+                                                                 const double *part, float *gcoefs, int stage)
+{
+   const RaggedChan c = chans[blockIdx.x];
+   if (c.S <= stage || threadIdx.x >= 5) return;
+   double s = 0.0;
+   for (int i = start[blockIdx.x]; i < start[blockIdx.x + 1]; i++) s += part[(long long) i * 5 + threadIdx.x];
+   gcoefs[c.cOff + stage * 5 + threadIdx.x] = (float) s;
+}
+
+// Taps gradient, partial over one (channel, tile) item:
+//     part[item][c] = sum_{j in tile} gu[j] x[j + c],  c < T.
+// Thread (cg, sl) accumulates 8 consecutive taps c0 = 8 cg .. c0 + 7 over slice sl
+// of the tile with a 16-sample register window (64 multiply-adds per 6 vector
+// shared-memory loads); slices are then summed in a fixed order.
 constexpr int kDhMaxT = 512;
 __global__ void __launch_bounds__(256) fir_dh_partial_kernel(const RaggedChan *chans, const int2 *items,
                                                               const float *x, const float *gu, float *part)
 {
-   __shared__ float sg[kRTile];
-   __shared__ float sx[kRTile + kDhMaxT];
+   __shared__ __align__(16) float sg[kRTile];
+   __shared__ __align__(16) float sx[kRTile + kDhMaxT + 16];
+   __shared__ float red[256 * 8];
    const int2 it = items[blockIdx.x];
    const RaggedChan c = chans[it.x];
+   const int tid = threadIdx.x;
    const int j0 = it.y * kRTile;
    const int n = min(kRTile, c.Lu - j0);
-   for (int k = threadIdx.x; k < kRTile; k += 256) sg[k] = k < n ? gu[c.xOff + j0 + k] : 0.0f;
-   for (int k = threadIdx.x; k < kRTile + c.T; k += 256) {
+   for (int k = tid; k < kRTile; k += 256) sg[k] = k < n ? gu[c.xOff + j0 + k] : 0.0f;
+   for (int k = tid; k < kRTile + kDhMaxT + 16; k += 256) {
       const int idx = j0 + k;
       sx[k] = idx < c.L ? x[c.xOff + idx] : 0.0f;
    }
    __syncthreads();
-   for (int cc = threadIdx.x; cc < c.T; cc += 256) {
-      float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-      for (int j = 0; j < n; j += 4) {
-         a0 = fmaf(sg[j], sx[j + cc], a0);
-         a1 = fmaf(sg[j + 1], sx[j + 1 + cc], a1);
-         a2 = fmaf(sg[j + 2], sx[j + 2 + cc], a2);
-         a3 = fmaf(sg[j + 3], sx[j + 3 + cc], a3);
+   const int ncg = (c.T + 7) >> 3;
+   int ncp = 1;
+   while (ncp < ncg) ncp <<= 1; // <= 64
+   const int slices = 256 / ncp, slen = kRTile / slices;
+   const int cg = tid & (ncp - 1), sl = tid / ncp;
+   float acc[8];
+#pragma unroll
+   for (int r = 0; r < 8; r++) acc[r] = 0.0f;
+   if (cg < ncg) {
+      const int c0 = cg * 8;
+      const int jb = sl * slen, je = min(jb + slen, (n + 7) & ~7);
+      for (int j = jb; j < je; j += 8) {
+         float w[16], gv[8];
+         const float *xw = sx + j + c0;
+         *(float4 *) &w[0] = *(const float4 *) &xw[0];
+         *(float4 *) &w[4] = *(const float4 *) &xw[4];
+         *(float4 *) &w[8] = *(const float4 *) &xw[8];
+         *(float4 *) &w[12] = *(const float4 *) &xw[12];
+         *(float4 *) &gv[0] = *(const float4 *) &sg[j];
+         *(float4 *) &gv[4] = *(const float4 *) &sg[j + 4];
+#pragma unroll
+         for (int i = 0; i < 8; i++)
+#pragma unroll
+            for (int r = 0; r < 8; r++) acc[r] = fmaf(gv[i], w[r + i], acc[r]);
       }
-      part[(long long) blockIdx.x * kDhMaxT + cc] = (a0 + a1) + (a2 + a3);
+   }
+#pragma unroll
+   for (int r = 0; r < 8; r++) red[sl * ncp * 8 + cg * 8 + r] = acc[r];
+   __syncthreads();
+   for (int cc = tid; cc < c.T; cc += 256) {
+      float sum = 0.0f;
+      for (int q = 0; q < slices; q++) sum += red[q * ncp * 8 + cc];
+      part[(long long) blockIdx.x * kDhMaxT + cc] = sum;
    }
 }
 
@@ -440,7 +498,7 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    long long xo = 0, ho = 0, co = 0;
    for (int c = 0; c < numChannels; c++) {
       const int L = length[c], T = taps[c], S = stages[c];
-      if (T < 1 || T > 512 || L < T || S < 0 || S > 64) {
+      if (T < 1 || T > kDhMaxT || L < T || S < 0 || S > kRaggedMaxStages) {
          delete p;
          return DSPLIB_ERR_INVALID_DIMENSION;
       }
@@ -503,8 +561,11 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_fwd(DSPLIB_gpu_raggedPlan plan, const 
    if (!p || !x || !taps || (!coefs && p->totalCoefs) || !y || !work) return DSPLIB_ERR_NULL_POINTER;
    cudaStream_t s = (cudaStream_t) stream;
    fir_ragged_kernel<false><<<p->nFwdItems, kRThreads, 0, s>>>(p->dChan, p->dFwdItems, x, taps, work);
-   const size_t carry = (size_t) std::max(1, p->Smax) * sizeof(double2);
-   biquad_ragged_kernel<false><<<p->C, kBThreads, carry, s>>>(p->dChan, p->dOrder, coefs, nullptr, work,
+   const size_t dyn = kRaggedMaxStages * sizeof(double2) + (size_t) std::max(1, p->Smax) * kBPowers * sizeof(M2);
+   if (cudaFuncSetAttribute(biquad_ragged_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dyn) !=
+       cudaSuccess)
+      return DSPLIB_ERR_FAILURE;
+   biquad_ragged_kernel<false><<<p->C, kBThreads, dyn, s>>>(p->dChan, p->dOrder, coefs, nullptr, work,
                                                               p->totalLen, y, 0, nullptr);
    countLaunch(2);
    return cudaGetLastError() == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
@@ -524,12 +585,15 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
    cudaError_t e = cudaMemcpyAsync(g, gy, (size_t) p->totalLen * sizeof(float), cudaMemcpyDeviceToDevice, s);
    if (e != cudaSuccess) return DSPLIB_ERR_FAILURE;
    int launches = 0;
+   const size_t dynBwd = kRaggedMaxStages * sizeof(double2) + kBPowers * sizeof(M2);
    for (int st = p->Smax - 1; st >= 0; st--) {
-      biquad_ragged_kernel<true><<<p->C, kBThreads, sizeof(double2), s>>>(p->dChan, p->dOrder, coefs, g,
+      biquad_ragged_kernel<true><<<p->C, kBThreads, dynBwd, s>>>(p->dChan, p->dOrder, coefs, g,
                                                                           (float *) work, p->totalLen, nullptr,
                                                                           st, v);
-      biquad_ragged_bwd_kernel<<<p->C, 256, 0, s>>>(p->dChan, coefs, work, p->totalLen, v, g, gcoefs, st);
-      launches += 2;
+      biquad_ragged_bwd_kernel<<<p->nFwdItems, 256, 0, s>>>(p->dChan, p->dFwdItems, coefs, work, p->totalLen,
+                                                            v, g, (double *) part, st);
+      biquad_coef_reduce_kernel<<<p->C, 32, 0, s>>>(p->dChan, p->dFwdStart, (const double *) part, gcoefs, st);
+      launches += 3;
    }
    fir_ragged_kernel<true><<<p->nDxItems, kRThreads, 0, s>>>(p->dChan, p->dDxItems, g, taps, gx);
    fir_dh_partial_kernel<<<p->nFwdItems, 256, 0, s>>>(p->dChan, p->dFwdItems, x, g, part);

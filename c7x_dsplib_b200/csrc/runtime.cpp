@@ -151,4 +151,14 @@ DSPLIB_STATUS DSPLIB_gpu_firSetQMode(DSPLIB_kernelHandle handle, int32_t enable)
 
 int64_t DSPLIB_gpu_kernelLaunchCount(void) { return g_launches.load(); }
 
+DSPLIB_STATUS DSPLIB_gpu_releaseHandle(DSPLIB_kernelHandle handle)
+{
+   HandleCommon *c = common(handle);
+   if (!c) return DSPLIB_ERR_NULL_POINTER;
+   // Work queued by an asynchronous exec may still read buffers the caller is about to free.
+   const cudaError_t e = c->async ? cudaStreamSynchronize(c->stream) : cudaSuccess;
+   c->magic = 0;
+   return e == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
+}
+
 } // extern "C"

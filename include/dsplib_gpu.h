@@ -46,6 +46,13 @@ DSPLIB_STATUS DSPLIB_gpu_firSetQMode(DSPLIB_kernelHandle handle, int32_t enable)
 /** Number of CUDA kernels this library has launched in this process. */
 int64_t DSPLIB_gpu_kernelLaunchCount(void);
 
+/** End of a handle's life (the reference API has no destructor: callers free
+ *  the handle memory themselves).  Waits for work an asynchronous exec queued
+ *  on the handle's stream, then marks the handle uninitialised so later calls
+ *  on it fail with DSPLIB_ERR_NULL_POINTER; the caller may then free it.
+ *  Handles own no device memory, so skipping this call leaks nothing. */
+DSPLIB_STATUS DSPLIB_gpu_releaseHandle(DSPLIB_kernelHandle handle);
+
 /* ---------------------------------------------------------------------------
  * Batched filter bank over channels of uneven length, forward and adjoint.
  * Per channel c (length L_c, T_c taps, S_c second-order stages):

@@ -255,3 +255,16 @@ def test_exec_without_init_fails_cleanly():
     assert h.exec(x, x, x) == D.ERR_FAILURE
     b = D.BiquadHandle()
     assert b.exec(x, x, x, x) == D.ERR_FAILURE
+
+
+def test_release_handle():
+    """DSPLIB_gpu_releaseHandle ends a handle's life: later calls on it fail as on an uninitialised handle."""
+    args, pin, pf, po = D.fir_setup(D.FLOAT32, 2, 64, 8, nch=0)
+    h = D.FirHandle()
+    assert h.init(args, pin, pf, po) == D.SUCCESS
+    assert D.lib().DSPLIB_gpu_releaseHandle(h.h) == D.SUCCESS
+    assert D.lib().DSPLIB_gpu_releaseHandle(h.h) == D.ERR_NULL_POINTER
+    assert D.lib().DSPLIB_gpu_setAsync(h.h, 1) == D.ERR_NULL_POINTER
+    x = np.zeros(8, np.float32)
+    assert h.exec(x, x, x) == D.ERR_FAILURE
+    assert D.lib().DSPLIB_gpu_releaseHandle(None) == D.ERR_NULL_POINTER
