@@ -33,6 +33,7 @@ ERR_INVALID_DIMENSION = 4
 ERR_NULL_POINTER = 5
 ERR_NOT_IMPLEMENTED = 6
 ERR_NOT_ALIGNED_WIDTHS = 9
+ERR_BUFFER_TOO_SMALL = 10
 
 # DSPLIB_data_type_e (include/DSPLIB_bufParams.h)
 INT8, INT16, INT32, INT64, UINT8, UINT16, UINT32, UINT64, FLOAT32, FLOAT64 = 0, 1, 2, 3, 5, 6, 8, 9, 12, 13
@@ -100,6 +101,8 @@ SIGNATURES = {
     "DSPLIB_gpu_firBiquadBatched_fwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_gpu_firBiquadBatched_bwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_gpu_raggedMseGrad": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "DSPLIB_gpu_firBiquadBatched_bwdStaticScratch": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
+                                                                    _VP]),
 }
 
 

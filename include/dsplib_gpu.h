@@ -109,6 +109,29 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
 DSPLIB_STATUS DSPLIB_gpu_raggedMseGrad(DSPLIB_gpu_raggedPlan plan, const float *y, const float *target, float *gy,
                                        float *loss, float *scratch, void *stream);
 
+/** Size, in floats, of the scratch array built into the library for
+ *  DSPLIB_gpu_firBiquadBatched_bwdStaticScratch (16 MiB per device). */
+#define DSPLIB_GPU_STATIC_SCRATCH_FLOATS (4u << 20)
+
+/** The adjoint of DSPLIB_gpu_firBiquadBatched_bwd without a scratch argument
+ *  and without allocating: its scratch is a fixed array inside the library, one
+ *  per device.  No counterpart in the reference (which has no adjoint); it is
+ *  for callers that cannot allocate device memory while they run (deadline-bound
+ *  processing threads, memory reserved up front, buffers owned by an allocator
+ *  they do not control).
+ *  - Plans needing more than DSPLIB_GPU_STATIC_SCRATCH_FLOATS floats of scratch
+ *    (DSPLIB_GPU_RAGGED_SCRATCH) return DSPLIB_ERR_BUFFER_TOO_SMALL, nothing queued.
+ *  - All calls on a device share the array: calls that overlap in time race and
+ *    corrupt each other's results; order them (same stream or events).
+ *  - No part of the array needs to start at zero.
+ *  - The first call on a device does a one-time lookup of the array's address with
+ *    that device current; make it before any stream capture begins.
+ *  Results are those of DSPLIB_gpu_firBiquadBatched_bwd with the same inputs. */
+DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwdStaticScratch(DSPLIB_gpu_raggedPlan plan, const float *x,
+                                                           const float *taps, const float *coefs, const float *work,
+                                                           const float *gy, float *gx, float *gtaps, float *gcoefs,
+                                                           void *stream);
+
 #ifdef __cplusplus
 }
 #endif
