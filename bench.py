@@ -121,7 +121,8 @@ class BiquadWorkload(Workload):
         nv = 4 if form == 1 else 2
         self.alg_bytes = 4 * (2 * N * C) + 4 * 5 * S + 2 * 4 * (S * nv * C)
         self.bound = "hbm"
-        self.kernel = "biquad_scan_kernel"
+        # up to 148 channels: one CTA per channel along time; beyond: lane = channel
+        self.kernel = "biquad_chan_kernel" if C <= 148 else "biquad_scan_kernel"
 
     def config(self):
         return {"workload": self.name, "channels": self.C, "samples_per_channel": self.N, "stages": self.S,
@@ -201,7 +202,10 @@ class FirWorkload(Workload):
         self.alg_bytes = elt * (B * N + B * self.out_size + self.hh.size)
         self.alg_flops = 2.0 * T * self.samples
         self.bound = "tensor" if precision == 1 else "hbm"
-        self.kernel = "fir_f32_simt_kernel" if dtype == np.float32 else "fir_direct_kernel"
+        if dtype == np.float32:
+            self.kernel = "fir_bf16x3_tc_kernel" if precision == 1 else "fir_f32_simt_kernel"
+        else:
+            self.kernel = "fir_int_tc_kernel" if T <= 2048 else "fir_direct_kernel"
 
     def config(self):
         return {"workload": self.name, "channels": self.B, "samples_per_channel": self.N, "taps": self.T,

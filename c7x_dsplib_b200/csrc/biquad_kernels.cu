@@ -415,11 +415,6 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
       }
       sWin[s * 32 + lane] = st0;
    }
-   float xd1_0 = 0.f, yd1_0 = 0.f; // DF1 with a single sample: the old xd1/yd1 shift into xd2/yd2
-   if (FORM == DSPLIB_BIQUAD_DF1 && active && a.N == 1) {
-      xd1_0 = a.state[ch];
-      yd1_0 = a.state[2 * a.varPitch + ch];
-   }
    if (CLUSTER) cg::this_cluster().sync();
    else __syncthreads();
 
@@ -518,6 +513,9 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
          float *sp = a.state + (long long) (s * nv) * a.varPitch + ch;
          if (len > 0 && t0 + len == a.N) { // chunk holding the last sample: final state
             if (FORM == DSPLIB_BIQUAD_DF1) {
+               // With a single sample the stage's old xd1 / yd1 shift into xd2 / yd2: read
+               // them before they are overwritten (no other thread writes this stage's state).
+               const float oxd1 = sp[0], oyd1 = sp[2 * a.varPitch];
                sp[0] = tail.x;
                sp[2 * a.varPitch] = tail.z;
                if (len >= 2) {
@@ -525,8 +523,8 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
                   sp[3 * a.varPitch] = tail.w;
                }
                else if (a.N == 1) {
-                  sp[a.varPitch] = xd1_0;
-                  sp[3 * a.varPitch] = yd1_0;
+                  sp[a.varPitch] = oxd1;
+                  sp[3 * a.varPitch] = oyd1;
                }
             }
             else {
@@ -555,6 +553,171 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
    }
    // Keep every CTA's shared memory alive until the cluster's last remote read.
    if (CLUSTER) cg::this_cluster().sync();
+}
+
+// ------------------------------------------------------------ per-channel scan
+//
+// biquad_chan_kernel: for batches of few channels, where lane = channel would
+// leave most of the GPU idle, one CTA per channel scans along time instead:
+// lane = chunk of 16 samples, 512 chunks per CTA = one 8192-sample window,
+// windows in sequence with the state carried.  Per stage: zero-state chunk end
+// states, a warp-shuffle scan over 32 chunks (powers M^(2^k) of M = A^16), a
+// scan over the 16 warp totals by warp 0 together with the window carry, then
+// every chunk reruns from its true initial state.  Each sample is read and
+// written once by the thread that owns its chunk (the channel's samples are a
+// column of the time-major buffer, so no access pattern coalesces across a
+// warp; the other channels of the same rows are read by the other CTAs out of L2).
+constexpr int kChL = 16;
+constexpr int kChWarps = 16;
+constexpr int kChThreads = kChWarps * 32;
+constexpr int kChWindow = kChThreads * kChL;
+constexpr int kChPowers = 10; // M^(2^k), k = 0..9: M^512 spans a window
+constexpr int kChanKernelMaxChannels = 148;
+
+size_t chanSmemBytes(int S) { return (size_t) S * (kChPowers * sizeof(M2) + sizeof(double2) + 5 * sizeof(float)); }
+
+template <int FORM> __global__ void __launch_bounds__(kChThreads, 1) biquad_chan_kernel(BiquadLaunch a)
+{
+   constexpr int nv = FORM == DSPLIB_BIQUAD_DF1 ? 4 : 2;
+   __shared__ double2 sTot[2][kChWarps];
+   extern __shared__ __align__(16) unsigned char chsm[];
+   M2 *sPow = (M2 *) chsm;                                   // [S][kChPowers]
+   double2 *sWin = (double2 *) (sPow + a.S * kChPowers);     // [S] state carried into the window
+   float *sCf = (float *) (sWin + a.S);                      // [S][5]
+   const int ch = blockIdx.x;
+   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+   for (int s = tid; s < a.S; s += kChThreads) {
+      const Coef c = loadCoef(a, s, ch);
+#pragma unroll
+      for (int k = 0; k < 5; k++) sCf[s * 5 + k] = c.k[k];
+      M2 P = transition<FORM>(c);
+#pragma unroll
+      for (int r = 1; r < kChL; r <<= 1) P = mmul(P, P);
+      sPow[s * kChPowers] = P;
+      for (int k = 1; k < kChPowers; k++) {
+         P = mmul(P, P);
+         sPow[s * kChPowers + k] = P;
+      }
+      const float *sp = a.state + (long long) (s * nv) * a.varPitch + ch;
+      double2 st0;
+      if (FORM == DSPLIB_BIQUAD_DF1) { // DF1 (xd1, xd2, yd1, yd2) -> transposed-form state
+         const double xd1 = sp[0], xd2 = sp[a.varPitch], yd1 = sp[2 * a.varPitch], yd2 = sp[3 * a.varPitch];
+         st0.x = c.k[1] * xd1 + c.k[2] * xd2 - c.k[3] * yd1 - c.k[4] * yd2;
+         st0.y = c.k[2] * xd1 - c.k[4] * yd1;
+      }
+      else {
+         st0 = make_double2(sp[0], sp[a.varPitch]);
+      }
+      sWin[s] = st0;
+   }
+   __syncthreads();
+
+   const double2 zero = make_double2(0.0, 0.0);
+   int phase = 0;
+   for (long long win0 = 0; win0 < a.N; win0 += kChWindow) {
+      const long long t0 = win0 + (long long) tid * kChL;
+      const int len = t0 < a.N ? (int) ((a.N - t0) < kChL ? (a.N - t0) : kChL) : 0;
+      float v[kChL];
+      {
+         const float *xp = a.x + t0 * a.inPitch + ch;
+#pragma unroll
+         for (int i = 0; i < kChL; i++) v[i] = i < len ? xp[i * a.inPitch] : 0.0f;
+      }
+      for (int s = 0; s < a.S; s++, phase++) {
+         Coef c;
+#pragma unroll
+         for (int k = 0; k < 5; k++) c.k[k] = sCf[s * 5 + k];
+         const M2 *P = sPow + s * kChPowers;
+         double2 *tot = sTot[phase & 1];
+         // 1. zero-state end state of this chunk
+         float2 e = make_float2(0.f, 0.f);
+         runChunkAny<FORM, kChL, false>(v, len, c, e, nullptr);
+         // 2. inclusive scan over the warp's 32 chunks
+         double2 val = make_double2(e.x, e.y);
+#pragma unroll
+         for (int k = 0; k < 5; k++) {
+            double2 o;
+            o.x = __shfl_up_sync(0xffffffffu, val.x, 1 << k);
+            o.y = __shfl_up_sync(0xffffffffu, val.y, 1 << k);
+            if (lane >= (1 << k)) val = affine(P[k], o, val);
+         }
+         if (lane == 31) tot[warp] = val;
+         __syncthreads();
+         // 3. warp 0: entry state of every warp (M^(32 w) carry + totals of the warps before), new carry
+         if (warp == 0) {
+            double2 tv = lane < kChWarps ? tot[lane] : zero;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+               double2 o;
+               o.x = __shfl_up_sync(0xffffffffu, tv.x, 1 << k);
+               o.y = __shfl_up_sync(0xffffffffu, tv.y, 1 << k);
+               if (lane >= (1 << k) && lane < kChWarps) tv = affine(P[5 + k], o, tv);
+            }
+            const double2 win = sWin[s];
+            double2 before, last;
+            before.x = __shfl_up_sync(0xffffffffu, tv.x, 1);
+            before.y = __shfl_up_sync(0xffffffffu, tv.y, 1);
+            last.x = __shfl_sync(0xffffffffu, tv.x, kChWarps - 1);
+            last.y = __shfl_sync(0xffffffffu, tv.y, kChWarps - 1);
+            if (lane < kChWarps) {
+               double2 en = win;
+#pragma unroll
+               for (int k = 0; k < 4; k++)
+                  if ((lane >> k) & 1) en = affine(P[5 + k], en, zero);
+               if (lane > 0) en = make_double2(en.x + before.x, en.y + before.y);
+               tot[lane] = en;
+            }
+            if (lane == 0) sWin[s] = affine(P[9], win, last);
+         }
+         __syncthreads();
+         // 4. this chunk's initial state: M^lane entry(warp) + exclusive prefix within the warp
+         double2 ex;
+         ex.x = __shfl_up_sync(0xffffffffu, val.x, 1);
+         ex.y = __shfl_up_sync(0xffffffffu, val.y, 1);
+         if (lane == 0) ex = zero;
+         double2 stv = tot[warp];
+#pragma unroll
+         for (int k = 0; k < 5; k++)
+            if ((lane >> k) & 1) stv = affine(P[k], stv, zero);
+         float2 st = make_float2((float) (stv.x + ex.x), (float) (stv.y + ex.y));
+         float4 tail = make_float4(0.f, 0.f, 0.f, 0.f);
+         runChunkAny<FORM, kChL, true>(v, len, c, st, &tail);
+         if (FORM == DSPLIB_BIQUAD_TIF && c.k[4] != 1.0f) {
+            const float g = c.k[4];
+#pragma unroll
+            for (int i = 0; i < kChL; i++) v[i] *= g;
+         }
+         float *sp = a.state + (long long) (s * nv) * a.varPitch + ch;
+         if (len > 0 && t0 + len == a.N) { // chunk holding the last sample: final state
+            if (FORM == DSPLIB_BIQUAD_DF1) {
+               const float oxd1 = sp[0], oyd1 = sp[2 * a.varPitch]; // read before overwritten
+               sp[0] = tail.x;
+               sp[2 * a.varPitch] = tail.z;
+               if (len >= 2) {
+                  sp[a.varPitch] = tail.y;
+                  sp[3 * a.varPitch] = tail.w;
+               }
+               else if (a.N == 1) {
+                  sp[a.varPitch] = oxd1;
+                  sp[3 * a.varPitch] = oyd1;
+               }
+            }
+            else {
+               sp[0] = st.x;
+               sp[a.varPitch] = st.y;
+            }
+         }
+         if (FORM == DSPLIB_BIQUAD_DF1 && len == kChL && t0 + kChL == a.N - 1) { // next chunk holds one sample
+            sp[a.varPitch] = tail.x;
+            sp[3 * a.varPitch] = tail.z;
+         }
+      }
+      float *yp = a.y + t0 * a.outPitch + ch;
+#pragma unroll
+      for (int i = 0; i < kChL; i++)
+         if (i < len) yp[i * a.outPitch] = v[i];
+   }
 }
 
 // Largest power-of-two cluster <= want that can be resident (<= 8 portable, 16 opt-in).
@@ -641,8 +804,23 @@ template <int FORM, int W> cudaError_t launchScanShape(const BiquadLaunch &a, in
 // Launch shape: few channel groups -> 16-warp CTAs and clusters of up to 16
 // CTAs along time (latency); many groups -> 8-warp CTAs (two per SM) with
 // clusters sized to fill one wave of the 148 SMs (throughput).
+template <int FORM> cudaError_t launchChanForm(const BiquadLaunch &a, cudaStream_t s)
+{
+   const size_t smem = chanSmemBytes(a.S);
+   if (smem > 48 * 1024) {
+      const cudaError_t e =
+          cudaFuncSetAttribute(biquad_chan_kernel<FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+      if (e != cudaSuccess) return e;
+   }
+   biquad_chan_kernel<FORM><<<a.C, kChThreads, smem, s>>>(a);
+   countLaunch();
+   return cudaGetLastError();
+}
+
 template <int FORM> cudaError_t launchScanForm(const BiquadLaunch &a, cudaStream_t s)
 {
+   // Up to one wave of CTAs: one CTA per channel along time; beyond, lane = channel.
+   if (a.C <= kChanKernelMaxChannels) return launchChanForm<FORM>(a, s);
    const int groups = (a.C + 31) / 32;
    const long long chunks = (a.N + kScanL - 1) / kScanL;
    constexpr int kSMs = 148;

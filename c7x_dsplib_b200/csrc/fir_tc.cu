@@ -59,6 +59,14 @@ template <typename T> struct IntLimits;
 template <> struct IntLimits<int8_t> { static constexpr long long lo = -128, hi = 127; };
 template <> struct IntLimits<int16_t> { static constexpr long long lo = -32768, hi = 32767; };
 
+// int8: |acc| <= 2048 * 2^14 fits 32 bits, so the output stage stays in 32-bit arithmetic.
+template <int QMODE> __device__ __forceinline__ int8_t outStage8(int acc, int shift)
+{
+   if (!QMODE) return (int8_t) acc; // modulo 2^8
+   if (shift > 0) acc = (acc + (1 << (shift - 1))) >> shift;
+   return (int8_t) max(-128, min(127, acc));
+}
+
 template <typename T, int QMODE>
 __device__ __forceinline__ T outStage(long long acc, int shift)
 {
@@ -168,8 +176,12 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
    extern __shared__ __align__(128) unsigned char sm[];
    uint64_t *mbar = (uint64_t *) sm;
    uint32_t *tslot = (uint32_t *) (sm + 8);
-   int *gtaps = (int *) (sm + 16);        // reversed taps g[c], c < T
-   unsigned char *B0 = sm + 16 + ((T_ * 4 + 15) & ~15);
+   // Reversed taps g[c] = h[T-1-c] as bytes (int16: high and low byte planes) at
+   // byte 16 + c of gb0 / gb1, zero elsewhere: one 32-bit word per thread to build.
+   const int gbWords = (Kt + 20) / 4;
+   uint32_t *gb0 = (uint32_t *) (sm + 16);
+   uint32_t *gb1 = gb0 + gbWords;
+   unsigned char *B0 = sm + 16 + ((gbWords * 4 * nplane + 15) & ~15);
    unsigned char *B1 = B0 + (size_t) Kt * 16;
    unsigned char *Abase = B0 + (size_t) Kt * 16 * nplane;
    // A[buf][plane]: seg bytes each
@@ -192,20 +204,40 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
       const T *x = (const T *) a.x + (long long) l * a.inPitch;
       const T *h = (const T *) a.h + (long long) l * a.filtPitch;
       T *y = (T *) a.y + (long long) l * a.outPitch;
-      for (int c = tid; c < T_; c += kThreads) gtaps[c] = (int) h[T_ - 1 - c];
-      __syncthreads();
-      // Taps band, K-major no-swizzle: byte (q*256 + i*128 + r*16 + e) holds B[m = 16q + e][b = 8i + r].
-      for (int idx = tid; idx < Kt * 16; idx += kThreads) {
-         const int q = idx >> 8, rem = idx & 255;
-         const int b = ((rem >> 7) << 3) + ((rem >> 4) & 7);
-         const int c = (q << 4) + (rem & 15) - b;
-         const int g = (c >= 0 && c < T_) ? gtaps[c] : 0;
-         if (SPLIT) {
-            B0[idx] = (unsigned char) (g >> 8);
-            B1[idx] = (unsigned char) (g & 0xFF);
+      for (int wd = tid; wd < gbWords; wd += kThreads) {
+         uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+         for (int j = 0; j < 4; j++) {
+            const int c = 4 * wd + j - 16;
+            const int g = (c >= 0 && c < T_) ? (int) h[T_ - 1 - c] : 0;
+            if (SPLIT) {
+               w0 |= (uint32_t) ((g >> 8) & 0xFF) << (8 * j);
+               w1 |= (uint32_t) (g & 0xFF) << (8 * j);
+            }
+            else {
+               w0 |= (uint32_t) (g & 0xFF) << (8 * j);
+            }
          }
-         else {
-            B0[idx] = (unsigned char) g;
+         gb0[wd] = w0;
+         if (SPLIT) gb1[wd] = w1;
+      }
+      __syncthreads();
+      // Taps band, K-major no-swizzle: 16-byte chunk ch = 16q + 8i + r (byte 16 ch) holds
+      // B[m = 16q + e][b = 8i + r] = g[16q + e - 8i - r], e < 16: bytes gb[16 + 16q - 8i - r + e],
+      // gathered from five words with funnel shifts.
+      for (int ch = tid; ch < Kt; ch += kThreads) {
+         const int base = 16 + 16 * (ch >> 4) - 8 * ((ch >> 3) & 1) - (ch & 7);
+         const int w = base >> 2, sh = (base & 3) * 8;
+#pragma unroll
+         for (int pl = 0; pl < (SPLIT ? 2 : 1); pl++) {
+            const uint32_t *gb = pl ? gb1 : gb0;
+            const uint32_t v0 = gb[w], v1 = gb[w + 1], v2 = gb[w + 2], v3 = gb[w + 3], v4 = gb[w + 4];
+            uint4 o;
+            o.x = __funnelshift_r(v0, v1, sh);
+            o.y = __funnelshift_r(v1, v2, sh);
+            o.z = __funnelshift_r(v2, v3, sh);
+            o.w = __funnelshift_r(v3, v4, sh);
+            *(uint4 *) ((pl ? B1 : B0) + 16 * ch) = o;
          }
       }
       const int t0 = blockIdx.x * tilesPerCta;
@@ -259,9 +291,10 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
             for (int b = 0; b < 16; b++) {
                long long v;
                if (!SPLIT) {
-                  v = (int) acc[0][b];
+                  out[b] = (T) outStage8<QMODE>((int) acc[0][b], a.shift);
+                  continue;
                }
-               else if (QMODE) {
+               if (QMODE) {
                   v = ((long long) (int) acc[0][b] << 16) + ((long long) (int) acc[1][b] << 8) +
                       (long long) (int) acc[2][b];
                }
@@ -300,7 +333,8 @@ template <typename T, int QMODE> cudaError_t launchIntTc(const FirLaunch &a, cud
    constexpr bool SPLIT = sizeof(T) == 2;
    const int Kt = bandK(a.T);
    const int nplane = SPLIT ? 2 : 1;
-   const size_t smem = 16 + (((size_t) a.T * 4 + 15) & ~(size_t) 15) + (size_t) Kt * 16 * nplane +
+   const size_t gbBytes = (size_t) ((Kt + 20) / 4) * 4 * nplane;
+   const size_t smem = 16 + ((gbBytes + 15) & ~(size_t) 15) + (size_t) Kt * 16 * nplane +
                        2 * (size_t) nplane * (kTile + Kt) + (size_t) kTile * sizeof(T);
    auto fn = fir_int_tc_kernel<T, QMODE>;
    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);

@@ -135,7 +135,9 @@ def test_natc_bitexact_vs_reference_cn():
 @pytest.mark.parametrize("nch", [0, 1])
 def test_opt_scan_accuracy(form, nch):
     rng = np.random.default_rng(100 + form * 3 + nch)
-    for (N, C, S) in [(1, 1, 1), (31, 3, 2), (8192, 32, 4), (40000, 40, 3), (3001, 65, 8), (700, 5, 13)]:
+    # C <= 148: one CTA per channel along time; C > 148: lane = channel with clusters
+    for (N, C, S) in [(1, 1, 1), (31, 3, 2), (8192, 32, 4), (40000, 40, 3), (3001, 65, 8), (700, 5, 13),
+                      (2000, 200, 3), (17000, 149, 2)]:
         x = rng.standard_normal((N, C)).astype(np.float32)
         nat = stable_sections(rng, C if nch else 1, S)
         st = np.zeros((S * nv(form), C), np.float32)
@@ -184,6 +186,25 @@ def test_opt_nonzero_initial_state():
         y64 = oracle.biquad_f64(form, x, nat, s64, nch=1)
         check_accuracy(y, want, y64, form)
         assert np.max(np.abs(host(sd) - s64)) <= 1e-3 * max(1.0, float(np.max(np.abs(s64))))
+
+
+@pytest.mark.parametrize("C", [5, 160])
+def test_opt_single_sample_multi_stage(C):
+    """N = 1 with several stages and a nonzero state: every stage's old state shifts
+    (DF1: xd1/yd1 move into xd2/yd2 of the same stage)."""
+    rng = np.random.default_rng(C)
+    for form in (D.DF1, D.DF2, D.TDF2):
+        N, S = 1, 3
+        x = rng.standard_normal((N, C)).astype(np.float32)
+        nat = stable_sections(rng, C, S)
+        st = (rng.standard_normal((S * nv(form), C)) * 0.5).astype(np.float32)
+        opt, _ = D.opt_coefficients(nat, form, 1, C)
+        sd = dev(st)
+        y = host(D.cascade_biquad(dev(x), dev(opt), sd, form=form, nch=1))
+        s_ref = st.copy()
+        want = oracle.biquad(form, x, nat, s_ref, nch=1)
+        assert np.max(np.abs(y - want)) <= 1e-5 * max(1.0, float(np.max(np.abs(want)))), form
+        assert np.max(np.abs(host(sd) - s_ref)) <= 1e-5 * max(1.0, float(np.max(np.abs(s_ref)))), form
 
 
 def test_opt_in_place():
