@@ -121,8 +121,8 @@ class BiquadWorkload(Workload):
         nv = 4 if form == 1 else 2
         self.alg_bytes = 4 * (2 * N * C) + 4 * 5 * S + 2 * 4 * (S * nv * C)
         self.bound = "hbm"
-        # up to 148 channels: one CTA per channel along time; beyond: lane = channel
-        self.kernel = "biquad_chan_kernel" if C <= 148 else "biquad_scan_kernel"
+        # up to 16 channels: one CTA per channel along time; beyond: lane = channel
+        self.kernel = "biquad_chan_kernel" if C <= 16 else "biquad_scan_kernel"
 
     def config(self):
         return {"workload": self.name, "channels": self.C, "samples_per_channel": self.N, "stages": self.S,

@@ -302,8 +302,9 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_exec(DSPLIB_kernelHandle handle,
    cudaStream_t s = hc->stream;
    Region rin{pIn, nullptr, (size_t) C * 4, (size_t) N, (size_t) p->inPitch * 4, false};
    Region rout{pOut, nullptr, (size_t) C * 4, (size_t) N, (size_t) p->outPitch * 4, false};
-   Region rst{pFilterVar, nullptr, (size_t) C * 4, (size_t) S * nv, (size_t) p->varPitch * 4, false};
-   Region rc{pFilterCoeff, nullptr, cw, ch, cp, false};
+   // states and coefficients are read (states also written) about once per channel and stage
+   Region rst{pFilterVar, nullptr, (size_t) C * 4, (size_t) S * nv, (size_t) p->varPitch * 4, false, true};
+   Region rc{pFilterCoeff, nullptr, cw, ch, cp, false, true};
    cudaError_t e;
    if ((e = regionIn(rin, 0, true, s)) != cudaSuccess) return cudaFail(hc, e, "stage input");
    if ((e = regionIn(rc, 1, true, s)) != cudaSuccess) return cudaFail(hc, e, "stage coefficients");

@@ -572,7 +572,7 @@ constexpr int kChWarps = 16;
 constexpr int kChThreads = kChWarps * 32;
 constexpr int kChWindow = kChThreads * kChL;
 constexpr int kChPowers = 10; // M^(2^k), k = 0..9: M^512 spans a window
-constexpr int kChanKernelMaxChannels = 148;
+constexpr int kChanKernelMaxChannels = 16;
 
 size_t chanSmemBytes(int S) { return (size_t) S * (kChPowers * sizeof(M2) + sizeof(double2) + 5 * sizeof(float)); }
 
@@ -817,21 +817,23 @@ template <int FORM> cudaError_t launchChanForm(const BiquadLaunch &a, cudaStream
    return cudaGetLastError();
 }
 
+// Shape choice, from timings of 1 .. 4096 channels x 8192 samples x 4 stages on B200:
+//  * up to 16 channels, lane = channel leaves most lanes idle: one CTA per channel
+//    scanning along time;
+//  * otherwise 32 channels per CTA (W = 16 warps: one CTA per SM at 128 registers),
+//    and time split over a cluster of K CTAs: the largest power of two <= 16 that keeps
+//    groups x K <= 128 CTAs resident in one wave; clusters of 16 are only taken while at
+//    most 7 of them are needed (no more are co-resident).  Fewer windows per CTA beat
+//    more CTAs once a second wave would be needed.
 template <int FORM> cudaError_t launchScanForm(const BiquadLaunch &a, cudaStream_t s)
 {
-   // Up to one wave of CTAs: one CTA per channel along time; beyond, lane = channel.
    if (a.C <= kChanKernelMaxChannels) return launchChanForm<FORM>(a, s);
    const int groups = (a.C + 31) / 32;
    const long long chunks = (a.N + kScanL - 1) / kScanL;
-   constexpr int kSMs = 148;
-   if (groups * 4 <= kSMs) {
-      int want = (int) ((chunks + 15) / 16);
-      return launchScanShape<FORM, 16>(a, want < 1 ? 1 : want, s);
-   }
-   int want = (int) ((chunks + 7) / 8);
-   const int fill = (2 * kSMs) / groups;
-   if (want > fill) want = fill;
-   return launchScanShape<FORM, 8>(a, want < 1 ? 1 : want, s);
+   int K = 1;
+   while (K < 16 && (long long) K * 2 * 16 <= chunks && groups * K * 2 <= 128 && !(K * 2 == 16 && groups > 7))
+      K *= 2;
+   return launchScanShape<FORM, 16>(a, K, s);
 }
 
 template <int FORM> cudaError_t launchSeqForm(const BiquadLaunch &a, cudaStream_t s)

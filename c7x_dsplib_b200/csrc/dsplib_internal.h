@@ -72,15 +72,37 @@ struct Region {
    size_t height;     // rows
    size_t pitch;      // bytes between rows
    bool staged;       // host buffer copied through a staging buffer
+   bool zeroCopy;     // the kernel touches each element about once: a small pinned buffer may be used in place
    size_t bytes() const { return height ? (height - 1) * pitch + width : 0; }
 };
 
-// Prepare a region: device pointers are used in place, host pointers are
+// Prepare a region: device pointers, and (zeroCopy regions) pinned host buffers
+// of at most kZeroCopyMaxBytes, are used in place; other host pointers are
 // staged (copied in when copyIn).  Returns cudaSuccess or the failure.
+constexpr size_t kZeroCopyMaxBytes = 64 * 1024;
 cudaError_t regionIn(Region &r, int slot, bool copyIn, cudaStream_t s);
 // Copy a staged region back to the caller's host buffer (row by row, leaving
 // the bytes between rows untouched).
 cudaError_t regionOut(const Region &r, cudaStream_t s);
+
+// Copy `rows` rows of `width` bytes, `pitch` bytes apart, in one call.
+cudaError_t copyRows(void *dst, const void *src, size_t width, size_t rows, size_t pitch, cudaMemcpyKind kind,
+                     cudaStream_t s);
+
+// Streams and events of the host-buffer pipeline (per host thread and device):
+// block b is copied in on `in`, computed on `comp`, copied out on `out`, so
+// the copies of neighbouring blocks overlap the kernels (and each other: the
+// two directions use separate copy engines).
+constexpr int kPipeMaxBlocks = 8;
+constexpr size_t kFirPipeMinBytes = 8u << 20;    // host in + out bytes from which FIR exec pipelines
+constexpr size_t kFirPipeBlockBytes = 16u << 20; // in + out bytes per block (2 .. kPipeMaxBlocks blocks)
+struct PipeContext {
+   bool ready = false;
+   cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
+   cudaEvent_t start = nullptr, done = nullptr;
+   cudaEvent_t copied[kPipeMaxBlocks] = {}, computed[kPipeMaxBlocks] = {};
+};
+PipeContext *pipeContext();
 
 // ---------------------------------------------------------------- kernels
 
@@ -114,6 +136,22 @@ cudaError_t launchFirIntTc(const FirLaunch &a, bool qmode, cudaStream_t s);
 // Error word written by the tensor-core kernels when a bounded wait gives up
 // (-1: could not be read).
 int firTcErrorFlag(bool clear);
+
+// One channel of the batched filter bank: samples at xOff (length L; the FIR
+// output and the biquad signals use the first Lu = L - T + 1), T taps at hOff,
+// S biquad stages (5 coefficients each) at cOff.
+struct RaggedChan {
+   long long xOff, hOff, cOff;
+   int L, T, S, Lu;
+};
+// Split-BF16x3 tensor-core FIR over a list of runs {channel, first tile, tiles, 0}
+// of kFirBfTile outputs: forward (valid correlation of the channel's x with its
+// taps) or dx (full convolution of the output gradient with the taps).
+constexpr int kFirBfTile = 8192;
+constexpr int kFirBfRunTiles = 4;
+constexpr int kFirBfMaxTaps = 512;
+cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *in,
+                                  const float *taps, float *out, bool dx, int Tmax, cudaStream_t s);
 
 struct BiquadLaunch {
    const float *x;

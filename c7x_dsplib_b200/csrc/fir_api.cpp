@@ -179,10 +179,21 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
    Region rf{(char *) pFilter + tapOffset * elt, nullptr, (size_t) (T > 0 ? T : 1) * elt, (size_t) (nch ? batch : 1),
              (size_t) (nch ? filtPitch : (T > 0 ? T : 1)) * elt, false};
    Region rout{pOut, nullptr, (size_t) outSize * elt, (size_t) batch, (size_t) p->outPitch * elt, false};
+   // Large host buffers: copy in, compute and copy out channel blocks in a pipeline.
+   PipeContext *pc = nullptr;
+   if (batch >= 2 && rin.bytes() + rout.bytes() >= kFirPipeMinBytes && !isDevicePtr(pIn) && !isDevicePtr(pOut))
+      pc = pipeContext();
+   cudaStream_t sIn = pc ? pc->in : s;
    cudaError_t e;
-   if ((e = regionIn(rin, 0, true, s)) != cudaSuccess) return cudaFail(hc, e, "stage input");
-   if ((e = regionIn(rf, 1, true, s)) != cudaSuccess) return cudaFail(hc, e, "stage filter");
-   if ((e = regionIn(rout, 2, false, s)) != cudaSuccess) return cudaFail(hc, e, "stage output");
+   if (pc) {
+      // after whatever the caller queued on the handle's stream
+      if ((e = cudaEventRecord(pc->start, s)) != cudaSuccess || (e = cudaStreamWaitEvent(pc->in, pc->start, 0)) ||
+          (e = cudaStreamWaitEvent(pc->comp, pc->start, 0)) || (e = cudaStreamWaitEvent(pc->out, pc->start, 0)))
+         return cudaFail(hc, e, "pipeline set-up");
+   }
+   if ((e = regionIn(rin, 0, pc == nullptr, sIn)) != cudaSuccess) return cudaFail(hc, e, "stage input");
+   if ((e = regionIn(rf, 1, true, sIn)) != cudaSuccess) return cudaFail(hc, e, "stage filter");
+   if ((e = regionIn(rout, 2, false, sIn)) != cudaSuccess) return cudaFail(hc, e, "stage output");
 
    FirLaunch a;
    a.x = rin.dev;
@@ -201,8 +212,38 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
       kind = hc->firQMode ? FIR_INT_Q_TC : FIR_INT_WRAP_TC;
    // Split-BF16x3 covers up to 512 taps; longer filters run the FP32 CUDA-core kernel.
    if (kind == FIR_F32_BF16X3 && !firBf16x3Supported(a)) kind = FIR_F32_SIMT;
-   if ((e = launchFir(a, kind, s)) != cudaSuccess) return cudaFail(hc, e, "FIR kernel launch");
-   if ((e = regionOut(rout, s)) != cudaSuccess) return cudaFail(hc, e, "copy output");
+   if (!pc) {
+      if ((e = launchFir(a, kind, s)) != cudaSuccess) return cudaFail(hc, e, "FIR kernel launch");
+      if ((e = regionOut(rout, s)) != cudaSuccess) return cudaFail(hc, e, "copy output");
+   }
+   else {
+      const size_t total = rin.bytes() + rout.bytes();
+      int nblk = (int) (total / kFirPipeBlockBytes);
+      nblk = nblk < 2 ? 2 : (nblk > kPipeMaxBlocks ? kPipeMaxBlocks : nblk);
+      const int rowsPer = (batch + nblk - 1) / nblk;
+      for (int b = 0; b * rowsPer < batch; b++) {
+         const int r0 = b * rowsPer, rows = (batch - r0) < rowsPer ? (batch - r0) : rowsPer;
+         const size_t inOff = (size_t) r0 * rin.pitch, outOff = (size_t) r0 * rout.pitch;
+         if ((e = copyRows((char *) rin.dev + inOff, (const char *) rin.host + inOff, rin.width, rows, rin.pitch,
+                           cudaMemcpyHostToDevice, pc->in)) != cudaSuccess ||
+             (e = cudaEventRecord(pc->copied[b], pc->in)) != cudaSuccess ||
+             (e = cudaStreamWaitEvent(pc->comp, pc->copied[b], 0)) != cudaSuccess)
+            return cudaFail(hc, e, "copy input block");
+         FirLaunch blk = a;
+         blk.x = (const char *) a.x + inOff;
+         blk.y = (char *) a.y + outOff;
+         blk.h = (const char *) a.h + (nch ? (size_t) r0 * filtPitch * elt : 0);
+         blk.batch = rows;
+         if ((e = launchFir(blk, kind, pc->comp)) != cudaSuccess) return cudaFail(hc, e, "FIR kernel launch");
+         if ((e = cudaEventRecord(pc->computed[b], pc->comp)) != cudaSuccess ||
+             (e = cudaStreamWaitEvent(pc->out, pc->computed[b], 0)) != cudaSuccess ||
+             (e = copyRows((char *) rout.host + outOff, (const char *) rout.dev + outOff, rout.width, rows,
+                           rout.pitch, cudaMemcpyDeviceToHost, pc->out)) != cudaSuccess)
+            return cudaFail(hc, e, "copy output block");
+      }
+      if ((e = cudaEventRecord(pc->done, pc->out)) != cudaSuccess || (e = cudaStreamWaitEvent(s, pc->done, 0)))
+         return cudaFail(hc, e, "pipeline join");
+   }
    if (!hc->async || rin.staged || rf.staged || rout.staged) {
       if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, "FIR execution");
       if ((kind == FIR_INT_WRAP_TC || kind == FIR_INT_Q_TC || kind == FIR_F32_BF16X3) && firTcErrorFlag(true) != 0) {

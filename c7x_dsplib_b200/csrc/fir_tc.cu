@@ -351,7 +351,8 @@ template <typename T, int QMODE> cudaError_t launchIntTc(const FirLaunch &a, cud
 
 constexpr int kBfPhases = 64;
 constexpr int kBfTile = kRows * kBfPhases;
-constexpr int kBfMaxTaps = 512;
+constexpr int kBfMaxTaps = kFirBfMaxTaps;
+static_assert(kBfTile == kFirBfTile, "ragged run tiles and kernel tiles must agree");
 constexpr int kBfThreads = 256;
 constexpr int kBfChunksPerThread = 5; // 16-byte plane chunks staged per thread: bfBlocks(512) * 8 / 256
 constexpr int kBfPadLeft = 64;        // zero taps ahead of the reversed taps (phase offsets)
@@ -370,25 +371,25 @@ __device__ __forceinline__ void splitBf16(float v, uint16_t &hi, uint16_t &lo)
 
 // Stage one tile's signal planes: sample i of the tile (64 per 128-byte block
 // k = i / 64) goes to block k, 16-byte chunk c = (i % 64) / 8 stored at
-// k*128 + ((c ^ (k & 7)) * 16), as hi and lo BF16.  All loads of a thread are
-// issued before any conversion so they overlap.
-__device__ __forceinline__ void bfStage(const float *xs, long long j0, long long inExtent, int nb,
-                                        unsigned char *Ahi, unsigned char *Alo, int tid)
+// k*128 + ((c ^ (k & 7)) * 16), as hi and lo BF16.  Sample i is input index
+// q0 + i of x, zero outside [0, inLen).  All loads of a thread are issued
+// before any conversion so they overlap.
+__device__ __forceinline__ void bfStage(const float *x, long long q0, long long inLen, int nb, unsigned char *Ahi,
+                                        unsigned char *Alo, int tid)
 {
-   const bool vec = ((((uintptr_t) xs) & 15) == 0);
    float f[kBfChunksPerThread][8];
 #pragma unroll
    for (int u = 0; u < kBfChunksPerThread; u++) {
       const int cidx = tid + u * kBfThreads;
       if (cidx < nb * 8) {
-         const long long i0 = (long long) (cidx >> 3) * 64 + (cidx & 7) * 8;
-         if (vec && j0 + i0 + 8 <= inExtent) {
-            *(float4 *) &f[u][0] = *(const float4 *) (xs + i0);
-            *(float4 *) &f[u][4] = *(const float4 *) (xs + i0 + 4);
+         const long long q = q0 + (long long) (cidx >> 3) * 64 + (cidx & 7) * 8;
+         if (q >= 0 && q + 8 <= inLen && ((((uintptr_t) (x + q)) & 15) == 0)) {
+            *(float4 *) &f[u][0] = *(const float4 *) (x + q);
+            *(float4 *) &f[u][4] = *(const float4 *) (x + q + 4);
          }
          else {
 #pragma unroll
-            for (int e = 0; e < 8; e++) f[u][e] = (j0 + i0 + e < inExtent) ? xs[i0 + e] : 0.0f;
+            for (int e = 0; e < 8; e++) f[u][e] = (q + e >= 0 && q + e < inLen) ? x[q + e] : 0.0f;
          }
       }
    }
@@ -407,127 +408,213 @@ __device__ __forceinline__ void bfStage(const float *xs, long long j0, long long
    }
 }
 
-__global__ void __launch_bounds__(kBfThreads, 1) fir_bf16x3_tc_kernel(FirLaunch a, int tilesPerCta)
+// A run of consecutive output tiles [t0, t1) of one channel:
+//     y[j] = sum_{c<T} x[inShift + j + c] * g(c),  x zero outside [0, inLen),
+//     g(c) = h[T-1-c] (reverse = 1: DSPLIB_fir correlation order) or h[c] (reverse = 0).
+struct BfRun {
+   const float *x;
+   const float *h;
+   float *y;
+   long long inShift, inLen;
+   int outLen, T, reverse, t0, t1;
+};
+
+// Shared-memory layout for taps up to Tmax (planes sized for the widest band).
+struct BfSmem {
+   unsigned char *A; // planes: hi of buffer 0, lo of buffer 0, hi of buffer 1, lo of buffer 1
+   size_t pb;        // bytes per plane
+   unsigned char *Bt;
+   __device__ unsigned char *hi(int buf) const { return A + (size_t) (2 * buf) * pb; }
+   __device__ unsigned char *lo(int buf) const { return A + (size_t) (2 * buf + 1) * pb; }
+   uint16_t *gHi, *gLo;
+   uint64_t *mbar;
+   uint32_t *tslot;
+};
+
+__host__ __device__ inline size_t bfPlaneBytes(int Tmax) { return (size_t) ((bfBlocks(Tmax) * 128 + 1023) & ~1023); }
+__host__ __device__ inline size_t bfSmemBytes(int Tmax)
 {
-   const int T_ = a.T;
+   return 1024 + 4 * bfPlaneBytes(Tmax) + (size_t) bfK(Tmax) * 256 + 4 * (size_t) bfTapSlots(Tmax) + 32;
+}
+
+__device__ __forceinline__ BfSmem bfSmemLayout(unsigned char *smraw, int Tmax)
+{
+   BfSmem L;
+   unsigned char *sm = (unsigned char *) (((uintptr_t) smraw + 1023) & ~(uintptr_t) 1023);
+   const size_t planeBytes = bfPlaneBytes(Tmax); // each plane starts on a 1024-byte swizzle atom
+   L.A = sm;
+   L.pb = planeBytes;
+   L.Bt = sm + 4 * planeBytes;
+   L.gHi = (uint16_t *) (L.Bt + (size_t) bfK(Tmax) * 256); // split taps with zero padding
+   L.gLo = L.gHi + bfTapSlots(Tmax);
+   L.mbar = (uint64_t *) (((uintptr_t) (L.gLo + bfTapSlots(Tmax)) + 15) & ~(uintptr_t) 15);
+   L.tslot = (uint32_t *) (L.mbar + 1);
+   return L;
+}
+
+// Build the taps band of run r, then stream its tiles through the tensor core.
+// Returns false when a bounded wait for the tensor core gave up.
+__device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint32_t tmem, uint32_t &iter, int tid)
+{
+   const int warp = tid >> 5, lane = tid & 31;
+   const int T_ = r.T;
    const int Kt = bfK(T_);
    const int nb = bfBlocks(T_);
    const int slots = bfTapSlots(T_);
-   extern __shared__ __align__(16) unsigned char smraw[];
-   unsigned char *sm = (unsigned char *) (((uintptr_t) smraw + 1023) & ~(uintptr_t) 1023);
-   const int planeBytes = (nb * 128 + 1023) & ~1023; // each plane starts on a 1024-byte swizzle atom
-   unsigned char *Ahi[2] = {sm, sm + 2 * planeBytes};
-   unsigned char *Alo[2] = {sm + planeBytes, sm + 3 * planeBytes};
-   unsigned char *Bt = sm + 4 * planeBytes;
-   uint16_t *gHi = (uint16_t *) (Bt + (size_t) Kt * 256); // reversed, split taps with zero padding
-   uint16_t *gLo = gHi + slots;
-   uint64_t *mbar = (uint64_t *) (((uintptr_t) (gLo + slots) + 15) & ~(uintptr_t) 15);
-   uint32_t *tslot = (uint32_t *) (mbar + 1);
+   // g[c] split into hi/lo, stored at slot c + kBfPadLeft; zero elsewhere.
+   for (int sl = tid; sl < slots; sl += kBfThreads) {
+      const int c = sl - kBfPadLeft;
+      uint16_t hi = 0, lo = 0;
+      if (c >= 0 && c < T_) splitBf16(r.reverse ? r.h[T_ - 1 - c] : r.h[c], hi, lo);
+      L.gHi[sl] = hi;
+      L.gLo[sl] = lo;
+   }
+   __syncthreads();
+   // Taps band, K-major no swizzle: 16-byte chunk (q, n) at q*2048 + (n/8)*128 + (n%8)*16 holds
+   // B[8q .. 8q+7][n]; rows n < 64: g_hi[m - n], rows n >= 64: g_lo[m - (n - 64)].
+   for (int cidx = tid; cidx < (Kt / 8) * 128; cidx += kBfThreads) {
+      const int q = cidx >> 7, n = cidx & 127;
+      const uint16_t *src = (n < 64 ? L.gHi : L.gLo) + kBfPadLeft + 8 * q - (n & 63);
+      __align__(16) uint16_t v[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) v[e] = src[e];
+      *(uint4 *) (L.Bt + q * 2048 + (n >> 3) * 128 + (n & 7) * 16) = *(uint4 *) v;
+   }
+   bool failed = false;
+   if (r.t0 < r.t1)
+      bfStage(r.x, r.inShift + (long long) r.t0 * kBfTile, r.inLen, nb, L.hi(0), L.lo(0), tid);
+   for (int t = r.t0; t < r.t1; t++) {
+      const int buf = (t - r.t0) & 1;
+      const long long j0 = (long long) t * kBfTile;
+      tc::fenceProxyAsync();
+      __syncthreads(); // planes[buf] and band written; previous tile's accumulator drained
+      if (tid == 0) {
+         tc::fenceAfterSync();
+         const uint32_t ahi = tc::smemAddr(L.hi(buf)), alo = tc::smemAddr(L.lo(buf)), bt = tc::smemAddr(L.Bt);
+         const uint32_t id128 = tc::idesc(1, 1, 1, kRows, 128), id64 = tc::idesc(1, 1, 1, kRows, 64);
+         for (int k16 = 0; k16 < Kt / 16; k16++) {
+            const int blk = k16 >> 2, sub = k16 & 3;
+            // The swizzle is applied on absolute shared-memory address bits, so a start
+            // that is not atom-aligned (block blk of the plane) keeps base offset 0.
+            const uint64_t dHi = tc::descSw128(ahi + blk * 128 + sub * 32, 1024, 0);
+            const uint64_t dLo = tc::descSw128(alo + blk * 128 + sub * 32, 1024, 0);
+            const uint64_t dB = tc::descNoSwizzle(bt + k16 * 4096, 2048, 128);
+            tc::mmaF16(tmem, dHi, dB, id128, k16 > 0);
+            tc::mmaF16(tmem, dLo, dB, id64, true);
+         }
+         tc::commit(L.mbar);
+      }
+      // Stage the next tile into the other buffer while the tensor core works.
+      if (t + 1 < r.t1)
+         bfStage(r.x, r.inShift + j0 + kBfTile, r.inLen, nb, L.hi(buf ^ 1), L.lo(buf ^ 1), tid);
+      const bool done = tc::mbarWait(L.mbar, iter & 1);
+      if (!done && tid == 0) atomicExch(&g_firTcError, 1);
+      failed = __syncthreads_or(!done) != 0;
+      iter++;
+      tc::fenceAfterSync();
+      if (!failed) {
+         // Warp w drains TMEM lane quadrant w % 4 (rows a) and output half w / 4:
+         // y[j0 + 64a + 32*half + b] = D[a][32*half + b] + D[a][64 + 32*half + b].
+         const int quad = warp & 3, half = warp >> 2;
+         const uint32_t lanes = (uint32_t) (quad * 32) << 16;
+         const int row = quad * 32 + lane;
+         uint32_t p[32], q[32];
+         tc::tmemLoad32(tmem + lanes + half * 32, p);
+         tc::tmemLoad32(tmem + lanes + 64 + half * 32, q);
+         tc::tmemWaitLoad();
+         // The planes of this buffer are free once the MMAs completed: they hold the
+         // output tile, 16-byte chunk v4 of row half (row, half) rotated to slot
+         // (v4 + row) & 7 so that eight consecutive rows store to distinct banks.
+         float *os = (float *) L.hi(buf) + row * kBfPhases + half * 32;
+#pragma unroll
+         for (int v4 = 0; v4 < 8; v4++) {
+            float4 o;
+            o.x = __uint_as_float(p[4 * v4 + 0]) + __uint_as_float(q[4 * v4 + 0]);
+            o.y = __uint_as_float(p[4 * v4 + 1]) + __uint_as_float(q[4 * v4 + 1]);
+            o.z = __uint_as_float(p[4 * v4 + 2]) + __uint_as_float(q[4 * v4 + 2]);
+            o.w = __uint_as_float(p[4 * v4 + 3]) + __uint_as_float(q[4 * v4 + 3]);
+            *(float4 *) (os + (((v4 + row) & 7) << 2)) = o;
+         }
+      }
+      tc::fenceBeforeSync();
+      if (failed) break;
+      __syncthreads(); // the output tile is complete in shared memory
+      storeTile<float>(r.y + j0, (int) min((long long) kBfTile, (long long) r.outLen - j0),
+                       (const unsigned char *) L.hi(buf),
+                       [](int ci) {
+                          const int row = ci >> 4, half = (ci >> 3) & 1, v4 = ci & 7;
+                          return (row * kBfPhases + half * 32 + (((v4 + row) & 7) << 2)) * 4;
+                       },
+                       tid, kBfThreads);
+   }
+   __syncthreads(); // before the taps band of the next run is rebuilt
+   return !failed;
+}
 
-   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-   if (warp == 0) tc::tmemAlloc(tslot, 128);
-   if (tid == 0) tc::mbarInit(mbar, 1);
+__global__ void __launch_bounds__(kBfThreads, 1) fir_bf16x3_tc_kernel(FirLaunch a, int tilesPerCta)
+{
+   extern __shared__ __align__(16) unsigned char smraw[];
+   const BfSmem L = bfSmemLayout(smraw, a.T);
+   const int tid = threadIdx.x, warp = tid >> 5;
+   if (warp == 0) tc::tmemAlloc(L.tslot, 128);
+   if (tid == 0) tc::mbarInit(L.mbar, 1);
    tc::fenceBeforeSync();
    __syncthreads();
    tc::fenceAfterSync();
-   const uint32_t tmem = *tslot;
+   const uint32_t tmem = *L.tslot;
 
    const int nt = (a.outSize + kBfTile - 1) / kBfTile;
-   const long long inExtent = (long long) a.outSize + T_ - 1;
    uint32_t iter = 0;
-   bool failed = false;
-   for (int l = blockIdx.y; l < a.batch && !failed; l += gridDim.y) {
-      const float *x = (const float *) a.x + (long long) l * a.inPitch;
-      const float *h = (const float *) a.h + (long long) l * a.filtPitch;
-      float *y = (float *) a.y + (long long) l * a.outPitch;
-      // g[c] = h[T-1-c] split into hi/lo, stored at slot c + kBfPadLeft; zero elsewhere.
-      for (int sl = tid; sl < slots; sl += kBfThreads) {
-         const int c = sl - kBfPadLeft;
-         uint16_t hi = 0, lo = 0;
-         if (c >= 0 && c < T_) splitBf16(h[T_ - 1 - c], hi, lo);
-         gHi[sl] = hi;
-         gLo[sl] = lo;
-      }
-      __syncthreads();
-      // Taps band, K-major no swizzle: 16-byte chunk (q, n) at q*2048 + (n/8)*128 + (n%8)*16 holds
-      // B[8q .. 8q+7][n]; rows n < 64: g_hi[m - n], rows n >= 64: g_lo[m - (n - 64)].
-      for (int cidx = tid; cidx < (Kt / 8) * 128; cidx += kBfThreads) {
-         const int q = cidx >> 7, n = cidx & 127;
-         const uint16_t *src = (n < 64 ? gHi : gLo) + kBfPadLeft + 8 * q - (n & 63);
-         __align__(16) uint16_t v[8];
-#pragma unroll
-         for (int e = 0; e < 8; e++) v[e] = src[e];
-         *(uint4 *) (Bt + q * 2048 + (n >> 3) * 128 + (n & 7) * 16) = *(uint4 *) v;
-      }
-      const int t0 = blockIdx.x * tilesPerCta;
-      const int t1 = min(nt, t0 + tilesPerCta);
-      if (t0 < t1) bfStage(x + (long long) t0 * kBfTile, (long long) t0 * kBfTile, inExtent, nb, Ahi[0], Alo[0], tid);
-      for (int t = t0; t < t1; t++) {
-         const int buf = (t - t0) & 1;
-         const long long j0 = (long long) t * kBfTile;
-         tc::fenceProxyAsync();
-         __syncthreads(); // planes[buf] and band written; previous tile's accumulator drained
-         if (tid == 0) {
-            tc::fenceAfterSync();
-            const uint32_t ahi = tc::smemAddr(Ahi[buf]), alo = tc::smemAddr(Alo[buf]), bt = tc::smemAddr(Bt);
-            const uint32_t id128 = tc::idesc(1, 1, 1, kRows, 128), id64 = tc::idesc(1, 1, 1, kRows, 64);
-            for (int k16 = 0; k16 < Kt / 16; k16++) {
-               const int blk = k16 >> 2, sub = k16 & 3;
-               // The swizzle is applied on absolute shared-memory address bits, so a start
-               // that is not atom-aligned (block blk of the plane) keeps base offset 0.
-               const uint64_t dHi = tc::descSw128(ahi + blk * 128 + sub * 32, 1024, 0);
-               const uint64_t dLo = tc::descSw128(alo + blk * 128 + sub * 32, 1024, 0);
-               const uint64_t dB = tc::descNoSwizzle(bt + k16 * 4096, 2048, 128);
-               tc::mmaF16(tmem, dHi, dB, id128, k16 > 0);
-               tc::mmaF16(tmem, dLo, dB, id64, true);
-            }
-            tc::commit(mbar);
-         }
-         // Stage the next tile into the other buffer while the tensor core works.
-         if (t + 1 < t1)
-            bfStage(x + j0 + kBfTile, j0 + kBfTile, inExtent, nb, Ahi[buf ^ 1], Alo[buf ^ 1], tid);
-         const bool done = tc::mbarWait(mbar, iter & 1);
-         if (!done && tid == 0) atomicExch(&g_firTcError, 1);
-         failed = __syncthreads_or(!done) != 0;
-         iter++;
-         tc::fenceAfterSync();
-         if (!failed) {
-            // Warp w drains TMEM lane quadrant w % 4 (rows a) and output half w / 4:
-            // y[j0 + 64a + 32*half + b] = D[a][32*half + b] + D[a][64 + 32*half + b].
-            const int quad = warp & 3, half = warp >> 2;
-            const uint32_t lanes = (uint32_t) (quad * 32) << 16;
-            const int row = quad * 32 + lane;
-            uint32_t p[32], q[32];
-            tc::tmemLoad32(tmem + lanes + half * 32, p);
-            tc::tmemLoad32(tmem + lanes + 64 + half * 32, q);
-            tc::tmemWaitLoad();
-            // The planes of this buffer are free once the MMAs completed: they hold the
-            // output tile, 16-byte chunk v4 of row half (row, half) rotated to slot
-            // (v4 + row) & 7 so that eight consecutive rows store to distinct banks.
-            float *os = (float *) Ahi[buf] + row * kBfPhases + half * 32;
-#pragma unroll
-            for (int v4 = 0; v4 < 8; v4++) {
-               float4 o;
-               o.x = __uint_as_float(p[4 * v4 + 0]) + __uint_as_float(q[4 * v4 + 0]);
-               o.y = __uint_as_float(p[4 * v4 + 1]) + __uint_as_float(q[4 * v4 + 1]);
-               o.z = __uint_as_float(p[4 * v4 + 2]) + __uint_as_float(q[4 * v4 + 2]);
-               o.w = __uint_as_float(p[4 * v4 + 3]) + __uint_as_float(q[4 * v4 + 3]);
-               *(float4 *) (os + (((v4 + row) & 7) << 2)) = o;
-            }
-         }
-         tc::fenceBeforeSync();
-         if (failed) break;
-         __syncthreads(); // the output tile is complete in shared memory
-         storeTile<float>(y + j0, (int) min((long long) kBfTile, (long long) a.outSize - j0),
-                          (const unsigned char *) Ahi[buf],
-                          [](int ci) {
-                             const int row = ci >> 4, half = (ci >> 3) & 1, v4 = ci & 7;
-                             return (row * kBfPhases + half * 32 + (((v4 + row) & 7) << 2)) * 4;
-                          },
-                          tid, kBfThreads);
-      }
-      __syncthreads(); // before the taps band of the next channel is rebuilt
+   for (int l = blockIdx.y; l < a.batch; l += gridDim.y) {
+      BfRun r;
+      r.x = (const float *) a.x + (long long) l * a.inPitch;
+      r.h = (const float *) a.h + (long long) l * a.filtPitch;
+      r.y = (float *) a.y + (long long) l * a.outPitch;
+      r.inShift = 0;
+      r.inLen = (long long) a.outSize + a.T - 1;
+      r.outLen = a.outSize;
+      r.T = a.T;
+      r.reverse = 1;
+      r.t0 = blockIdx.x * tilesPerCta;
+      r.t1 = min(nt, r.t0 + tilesPerCta);
+      if (!bfProcess(r, L, tmem, iter, tid)) break;
    }
+   __syncthreads();
+   if (warp == 0) tc::tmemFree(tmem, 128);
+}
+
+// Work lists of the batched filter bank: one run of up to kFirBfRunTiles tiles of
+// one channel per CTA.  DX = false: forward, y = valid correlation of x with
+// the taps (DSPLIB_fir order); DX = true: input gradient, the full convolution
+// of the output gradient with the taps.
+__global__ void __launch_bounds__(kBfThreads, 1)
+    fir_bf16x3_ragged_kernel(const RaggedChan *chans, const int4 *runs, const float *in, const float *taps,
+                             float *out, int dx, int Tmax)
+{
+   extern __shared__ __align__(16) unsigned char smraw[];
+   const BfSmem L = bfSmemLayout(smraw, Tmax);
+   const int tid = threadIdx.x, warp = tid >> 5;
+   if (warp == 0) tc::tmemAlloc(L.tslot, 128);
+   if (tid == 0) tc::mbarInit(L.mbar, 1);
+   tc::fenceBeforeSync();
+   __syncthreads();
+   tc::fenceAfterSync();
+   const uint32_t tmem = *L.tslot;
+   const int4 it = runs[blockIdx.x];
+   const RaggedChan c = chans[it.x];
+   BfRun r;
+   r.x = in + c.xOff;
+   r.h = taps + c.hOff;
+   r.y = out + c.xOff;
+   r.T = c.T;
+   r.inShift = dx ? -(long long) (c.T - 1) : 0;
+   r.inLen = dx ? c.L - c.T + 1 : c.L;
+   r.outLen = dx ? c.L : c.L - c.T + 1;
+   r.reverse = dx ? 0 : 1;
+   r.t0 = it.y;
+   r.t1 = it.y + it.z;
+   uint32_t iter = 0;
+   bfProcess(r, L, tmem, iter, tid);
    __syncthreads();
    if (warp == 0) tc::tmemFree(tmem, 128);
 }
@@ -551,9 +638,7 @@ bool firBf16x3Supported(const FirLaunch &a) { return a.dtype == DSPLIB_FLOAT32 &
 cudaError_t launchFirBf16x3(const FirLaunch &a, cudaStream_t s)
 {
    if (!firBf16x3Supported(a)) return cudaErrorNotSupported;
-   const int Kt = bfK(a.T), nb = bfBlocks(a.T);
-   const size_t planes = 4 * (size_t) ((nb * 128 + 1023) & ~1023); // hi and lo, double-buffered
-   const size_t smem = 1024 + planes + (size_t) Kt * 256 + 4 * (size_t) bfTapSlots(a.T) + 32;
+   const size_t smem = bfSmemBytes(a.T);
    cudaError_t e =
        cudaFuncSetAttribute(fir_bf16x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
    if (e != cudaSuccess) return e;
@@ -561,6 +646,20 @@ cudaError_t launchFirBf16x3(const FirLaunch &a, cudaStream_t s)
    const int tpc = tilesPerCtaFor(nt, a.batch, 1);
    dim3 grid((nt + tpc - 1) / tpc, a.batch < 65535 ? a.batch : 65535);
    fir_bf16x3_tc_kernel<<<grid, kBfThreads, smem, s>>>(a, tpc);
+   countLaunch();
+   return cudaGetLastError();
+}
+
+cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *in,
+                                  const float *taps, float *out, bool dx, int Tmax, cudaStream_t s)
+{
+   if (Tmax < 1 || Tmax > kBfMaxTaps) return cudaErrorNotSupported;
+   if (nRuns <= 0) return cudaSuccess;
+   const size_t smem = bfSmemBytes(Tmax);
+   cudaError_t e =
+       cudaFuncSetAttribute(fir_bf16x3_ragged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+   if (e != cudaSuccess) return e;
+   fir_bf16x3_ragged_kernel<<<nRuns, kBfThreads, smem, s>>>(chans, runs, in, taps, out, dx ? 1 : 0, Tmax);
    countLaunch();
    return cudaGetLastError();
 }

@@ -39,6 +39,17 @@ bool isDevicePtr(const void *p)
    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
 }
 
+// Device-side address of page-locked (pinned) host memory, nullptr otherwise.
+static void *pinnedDevicePtr(const void *p)
+{
+   cudaPointerAttributes attr;
+   if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+      (void) cudaGetLastError();
+      return nullptr;
+   }
+   return attr.type == cudaMemoryTypeHost ? attr.devicePointer : nullptr;
+}
+
 namespace {
 constexpr int kMaxDevices = 16;
 constexpr int kSlots = 6;
@@ -77,6 +88,14 @@ cudaError_t regionIn(Region &r, int slot, bool copyIn, cudaStream_t s)
    r.dev = r.host;
    if (r.height == 0 || r.width == 0) return cudaSuccess;
    if (isDevicePtr(r.host)) return cudaSuccess;
+   // Small pinned buffers (coefficients, states, taps) are read and written in place by
+   // the kernels: a staging copy each way would cost more than the few accesses.
+   if (r.zeroCopy && r.bytes() <= kZeroCopyMaxBytes) {
+      if (void *d = pinnedDevicePtr(r.host)) {
+         r.dev = d;
+         return cudaSuccess;
+      }
+   }
    void *buf = stagingBuffer(slot, r.bytes());
    if (!buf) return cudaErrorMemoryAllocation;
    r.dev = buf;
@@ -93,6 +112,38 @@ cudaError_t regionOut(const Region &r, cudaStream_t s)
    if (r.pitch <= r.width || r.height == 1)
       return cudaMemcpyAsync(r.host, r.dev, r.bytes(), cudaMemcpyDeviceToHost, s);
    return cudaMemcpy2DAsync(r.host, r.pitch, r.dev, r.pitch, r.width, r.height, cudaMemcpyDeviceToHost, s);
+}
+
+PipeContext *pipeContext()
+{
+   static thread_local PipeContext ctx[kMaxDevices];
+   int dev = 0;
+   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+   PipeContext &c = ctx[dev];
+   if (!c.ready) {
+      bool ok = cudaStreamCreateWithFlags(&c.in, cudaStreamNonBlocking) == cudaSuccess &&
+                cudaStreamCreateWithFlags(&c.comp, cudaStreamNonBlocking) == cudaSuccess &&
+                cudaStreamCreateWithFlags(&c.out, cudaStreamNonBlocking) == cudaSuccess &&
+                cudaEventCreateWithFlags(&c.start, cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) == cudaSuccess;
+      for (int b = 0; ok && b < kPipeMaxBlocks; b++)
+         ok = cudaEventCreateWithFlags(&c.copied[b], cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c.computed[b], cudaEventDisableTiming) == cudaSuccess;
+      if (!ok) {
+         (void) cudaGetLastError();
+         return nullptr;
+      }
+      c.ready = true;
+   }
+   return &c;
+}
+
+cudaError_t copyRows(void *dst, const void *src, size_t width, size_t rows, size_t pitch, cudaMemcpyKind kind,
+                     cudaStream_t s)
+{
+   if (rows == 0 || width == 0) return cudaSuccess;
+   if (pitch <= width || rows == 1) return cudaMemcpyAsync(dst, src, (rows - 1) * pitch + width, kind, s);
+   return cudaMemcpy2DAsync(dst, pitch, src, pitch, width, rows, kind, s);
 }
 
 static HandleCommon *common(DSPLIB_kernelHandle h)

@@ -258,3 +258,28 @@ def test_async_stream_device():
     s.synchronize()
     assert D.kernel_launch_count() == n0 + 1
     assert np.max(np.abs(host(yd) - oracle.fir(x, hh, 100, nch=0))) <= TOL_REF
+
+
+@pytest.mark.parametrize("dt,precision,qmode,B,N,T", [
+    (np.int16, D.FIR_SIMT, False, 96, 65536, 64),   # tensor-core wrap, even blocks
+    (np.int8, D.FIR_SIMT, True, 130, 65536, 128),   # tensor-core Q mode
+    (np.float32, D.FIR_SIMT, False, 37, 65536, 33),  # odd batch: unequal blocks
+    (np.float32, D.FIR_BF16X3, False, 37, 65536, 256),
+])
+@pytest.mark.parametrize("pinned", [False, True])
+def test_host_buffers_pipelined(dt, precision, qmode, B, N, T, pinned):
+    """Host buffers of 8 MB and more run as a copy-in / compute / copy-out
+    pipeline over channel blocks: results equal the device-buffer call bit for bit."""
+    rng = np.random.default_rng(B + T)
+    x = rand(dt, (B, N), rng)
+    h = rand(dt, (B, T), rng) if dt != np.float32 else (rng.standard_normal((B, T)) / T).astype(np.float32)
+    shift = 7 if dt == np.int8 else 0
+    want = host(D.fir(dev(x), dev(h), T, nch=1, precision=precision, qmode=qmode, shift=shift))
+    if pinned:
+        xh = torch.from_numpy(x).pin_memory()
+        hh = torch.from_numpy(h).pin_memory()
+        out = torch.zeros((B, N - T + 1), dtype=xh.dtype).pin_memory()
+        got = D.fir(xh, hh, T, nch=1, precision=precision, qmode=qmode, shift=shift, out=out).numpy()
+    else:
+        got = D.fir(x, h, T, nch=1, precision=precision, qmode=qmode, shift=shift)
+    assert np.array_equal(got, want)
