@@ -408,6 +408,31 @@ __device__ __forceinline__ void bfStage(const float *x, long long q0, long long 
    }
 }
 
+// Raw FP32 tiles (nb blocks of 64 samples) are bulk-copied by the TMA engine
+// when the whole tile lies inside the input and is 16-byte aligned, then split
+// in shared memory; other tiles (row edges, unaligned rows) are staged by the
+// threads straight into the planes (bfStage).
+// Split a raw tile into the signal planes: sample i (64 per 128-byte block
+// k = i / 64) goes to block k, 16-byte chunk c = (i % 64) / 8 stored at
+// k*128 + ((c ^ (k & 7)) * 16), as hi and lo BF16.  A thread takes 4 samples
+// (one 16-byte read; consecutive lanes, consecutive addresses) and writes half
+// a chunk of each plane.
+__device__ __forceinline__ void bfSplit(const float *raw, int nb, unsigned char *Ahi, unsigned char *Alo, int tid)
+{
+   for (int f = tid; f < nb * 16; f += kBfThreads) {
+      const float4 v = ((const float4 *) raw)[f];
+      const int k = f >> 4, c = (f >> 1) & 7, half = f & 1;
+      uint16_t hv[4], lv[4];
+      splitBf16(v.x, hv[0], lv[0]);
+      splitBf16(v.y, hv[1], lv[1]);
+      splitBf16(v.z, hv[2], lv[2]);
+      splitBf16(v.w, hv[3], lv[3]);
+      const int off = k * 128 + ((c ^ (k & 7)) << 4) + half * 8;
+      *(uint2 *) (Ahi + off) = *(uint2 *) hv;
+      *(uint2 *) (Alo + off) = *(uint2 *) lv;
+   }
+}
+
 // A run of consecutive output tiles [t0, t1) of one channel:
 //     y[j] = sum_{c<T} x[inShift + j + c] * g(c),  x zero outside [0, inLen),
 //     g(c) = h[T-1-c] (reverse = 1: DSPLIB_fir correlation order) or h[c] (reverse = 0).
@@ -419,48 +444,129 @@ struct BfRun {
    int outLen, T, reverse, t0, t1;
 };
 
-// Shared-memory layout for taps up to Tmax (planes sized for the widest band).
-struct BfSmem {
-   unsigned char *A; // planes: hi of buffer 0, lo of buffer 0, hi of buffer 1, lo of buffer 1
-   size_t pb;        // bytes per plane
-   unsigned char *Bt;
-   __device__ unsigned char *hi(int buf) const { return A + (size_t) (2 * buf) * pb; }
-   __device__ unsigned char *lo(int buf) const { return A + (size_t) (2 * buf + 1) * pb; }
-   uint16_t *gHi, *gLo;
-   uint64_t *mbar;
-   uint32_t *tslot;
-};
-
+// Shared memory for taps up to Tmax: the hi/lo signal planes of the current
+// tile (also the output staging area once its MMAs completed), a ring of raw
+// FP32 tiles in flight (two when they fit beside the band, else one), the taps
+// band and the split taps.
+constexpr size_t kBfSmemLimit = 227 * 1024;
 __host__ __device__ inline size_t bfPlaneBytes(int Tmax) { return (size_t) ((bfBlocks(Tmax) * 128 + 1023) & ~1023); }
-__host__ __device__ inline size_t bfSmemBytes(int Tmax)
+__host__ __device__ inline size_t bfRawBytes(int Tmax) { return (size_t) bfBlocks(Tmax) * 256; }
+__host__ __device__ inline size_t bfSmemBytesFor(int Tmax, int stages)
 {
-   return 1024 + 4 * bfPlaneBytes(Tmax) + (size_t) bfK(Tmax) * 256 + 4 * (size_t) bfTapSlots(Tmax) + 32;
+   return 1024 + 2 * bfPlaneBytes(Tmax) + stages * bfRawBytes(Tmax) + (size_t) bfK(Tmax) * 256 +
+          4 * (size_t) bfTapSlots(Tmax) + 64;
 }
+__host__ __device__ inline int bfStages(int Tmax) { return bfSmemBytesFor(Tmax, 2) <= kBfSmemLimit ? 2 : 1; }
+__host__ __device__ inline size_t bfSmemBytes(int Tmax) { return bfSmemBytesFor(Tmax, bfStages(Tmax)); }
+
+struct BfSmem {
+   unsigned char *hi, *lo; // planes, each on a 1024-byte swizzle atom
+   float *raw;             // stages x bfBlocks(Tmax) * 64 floats
+   int rawFloats, stages;
+   unsigned char *Bt;
+   uint16_t *gHi, *gLo;
+   uint64_t *mbar, *full; // MMA completion; raw-tile arrival per stage
+   uint32_t *tslot;
+   __device__ float *slot(int k) const { return raw + (size_t) k * rawFloats; }
+};
 
 __device__ __forceinline__ BfSmem bfSmemLayout(unsigned char *smraw, int Tmax)
 {
    BfSmem L;
    unsigned char *sm = (unsigned char *) (((uintptr_t) smraw + 1023) & ~(uintptr_t) 1023);
-   const size_t planeBytes = bfPlaneBytes(Tmax); // each plane starts on a 1024-byte swizzle atom
-   L.A = sm;
-   L.pb = planeBytes;
-   L.Bt = sm + 4 * planeBytes;
+   const size_t pb = bfPlaneBytes(Tmax);
+   L.stages = bfStages(Tmax);
+   L.hi = sm;
+   L.lo = sm + pb;
+   L.raw = (float *) (sm + 2 * pb);
+   L.rawFloats = bfBlocks(Tmax) * 64;
+   L.Bt = (unsigned char *) L.raw + (size_t) L.stages * bfRawBytes(Tmax);
    L.gHi = (uint16_t *) (L.Bt + (size_t) bfK(Tmax) * 256); // split taps with zero padding
    L.gLo = L.gHi + bfTapSlots(Tmax);
    L.mbar = (uint64_t *) (((uintptr_t) (L.gLo + bfTapSlots(Tmax)) + 15) & ~(uintptr_t) 15);
-   L.tslot = (uint32_t *) (L.mbar + 1);
+   L.full = L.mbar + 1;
+   L.tslot = (uint32_t *) (L.full + 2);
    return L;
 }
 
-// Build the taps band of run r, then stream its tiles through the tensor core.
-// Returns false when a bounded wait for the tensor core gave up.
-__device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint32_t tmem, uint32_t &iter, int tid)
+// Barrier phases and copies in flight, carried across the runs of one CTA.
+struct BfPipe {
+   uint32_t iter = 0;    // MMA barrier phase
+   uint32_t par = 0;     // raw-tile barrier phase, one bit per stage
+   uint32_t pending = 0; // stages with a bulk copy issued and not yet waited for
+};
+
+// Drain the accumulator (the MMAs of output tile t) through the planes into y.
+// Returns false when the bounded wait gave up.
+__device__ __forceinline__ bool bfDrain(const BfRun &r, const BfSmem &L, uint32_t tmem, BfPipe &pp, int t, int tid)
 {
    const int warp = tid >> 5, lane = tid & 31;
+   const bool done = tid == 0 ? tc::mbarWait(L.mbar, pp.iter & 1) : true; // the barrier releases the rest
+   pp.iter++;
+   if (!done && tid == 0) atomicExch(&g_firTcError, 1);
+   if (__syncthreads_or(!done)) return false;
+   tc::fenceAfterSync();
+   const long long j0 = (long long) t * kBfTile;
+   {
+      // Warp w drains TMEM lane quadrant w % 4 (rows a) and output half w / 4:
+      // y[j0 + 64a + 32*half + b] = D[a][32*half + b] + D[a][64 + 32*half + b].
+      const int quad = warp & 3, half = warp >> 2;
+      const uint32_t acc = tmem + ((uint32_t) (quad * 32) << 16);
+      const int row = quad * 32 + lane;
+      uint32_t a[32], b[32];
+      tc::tmemLoad32(acc + half * 32, a);
+      tc::tmemLoad32(acc + 64 + half * 32, b);
+      tc::tmemWaitLoad();
+      // The planes are free once the MMAs completed: they hold the output tile,
+      // 16-byte chunk v4 of row half (row, half) rotated to slot (v4 + row) & 7 so
+      // that eight consecutive rows store to distinct banks.
+      float *os = (float *) L.hi + row * kBfPhases + half * 32;
+#pragma unroll
+      for (int v4 = 0; v4 < 8; v4++) {
+         float4 o;
+         o.x = __uint_as_float(a[4 * v4 + 0]) + __uint_as_float(b[4 * v4 + 0]);
+         o.y = __uint_as_float(a[4 * v4 + 1]) + __uint_as_float(b[4 * v4 + 1]);
+         o.z = __uint_as_float(a[4 * v4 + 2]) + __uint_as_float(b[4 * v4 + 2]);
+         o.w = __uint_as_float(a[4 * v4 + 3]) + __uint_as_float(b[4 * v4 + 3]);
+         *(float4 *) (os + (((v4 + row) & 7) << 2)) = o;
+      }
+   }
+   tc::fenceBeforeSync();
+   __syncthreads(); // the output tile is complete in shared memory; the accumulator is free
+   storeTile<float>(r.y + j0, (int) min((long long) kBfTile, (long long) r.outLen - j0),
+                    (const unsigned char *) L.hi,
+                    [](int ci) {
+                       const int row = ci >> 4, half = (ci >> 3) & 1, v4 = ci & 7;
+                       return (row * kBfPhases + half * 32 + (((v4 + row) & 7) << 2)) * 4;
+                    },
+                    tid, kBfThreads);
+   return true;
+}
+
+// Build the taps band of run r, then stream its tiles through the tensor core.
+// Returns false when a bounded wait gave up.
+__device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint32_t tmem, BfPipe &pp, int tid)
+{
    const int T_ = r.T;
    const int Kt = bfK(T_);
    const int nb = bfBlocks(T_);
    const int slots = bfTapSlots(T_);
+   const int S = L.stages;
+   const uint32_t rawBytes = (uint32_t) nb * 256;
+   auto q0 = [&](int t) { return r.inShift + (long long) t * kBfTile; };
+   auto bulkOk = [&](int t) {
+      const long long q = q0(t);
+      return q >= 0 && q + (long long) nb * 64 <= r.inLen && ((((uintptr_t) (r.x + q)) & 15) == 0);
+   };
+   // The first raw tiles are fetched while the taps band is built.
+   if (tid == 0)
+      for (int k = 0; k < S && r.t0 + k < r.t1; k++)
+         if (bulkOk(r.t0 + k)) {
+            tc::mbarExpectTx(L.full + k, rawBytes);
+            tc::bulkLoad(L.slot(k), r.x + q0(r.t0 + k), rawBytes, L.full + k);
+         }
+   for (int k = 0; k < S && r.t0 + k < r.t1; k++)
+      if (bulkOk(r.t0 + k)) pp.pending |= 1u << k;
    // g[c] split into hi/lo, stored at slot c + kBfPadLeft; zero elsewhere.
    for (int sl = tid; sl < slots; sl += kBfThreads) {
       const int c = sl - kBfPadLeft;
@@ -480,18 +586,34 @@ __device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint3
       for (int e = 0; e < 8; e++) v[e] = src[e];
       *(uint4 *) (L.Bt + q * 2048 + (n >> 3) * 128 + (n & 7) * 16) = *(uint4 *) v;
    }
-   bool failed = false;
-   if (r.t0 < r.t1)
-      bfStage(r.x, r.inShift + (long long) r.t0 * kBfTile, r.inLen, nb, L.hi(0), L.lo(0), tid);
    for (int t = r.t0; t < r.t1; t++) {
-      const int buf = (t - r.t0) & 1;
-      const long long j0 = (long long) t * kBfTile;
+      const int k = (t - r.t0) % S;
+      bool ok = true;
+      const bool viaBulk = bulkOk(t);
+      if (viaBulk) {
+         ok = tid == 0 ? tc::mbarWait(L.full + k, (pp.par >> k) & 1) : true; // the barrier below releases the rest
+         pp.par ^= 1u << k;
+         pp.pending &= ~(1u << k);
+      }
+      if (!ok && tid == 0) atomicExch(&g_firTcError, 1);
+      // raw tile landed; the previous tile's outputs have left the planes
+      if (__syncthreads_or(!ok)) return false;
+      if (viaBulk) bfSplit(L.slot(k), nb, L.hi, L.lo, tid);
+      else bfStage(r.x, q0(t), r.inLen, nb, L.hi, L.lo, tid); // straight from global memory
       tc::fenceProxyAsync();
-      __syncthreads(); // planes[buf] and band written; previous tile's accumulator drained
+      __syncthreads(); // planes and band written; the raw stage is free again
+      if (t + S < r.t1 && bulkOk(t + S)) {
+         if (tid == 0) {
+            tc::mbarExpectTx(L.full + k, rawBytes);
+            tc::bulkLoad(L.slot(k), r.x + q0(t + S), rawBytes, L.full + k);
+         }
+         pp.pending |= 1u << k;
+      }
       if (tid == 0) {
          tc::fenceAfterSync();
-         const uint32_t ahi = tc::smemAddr(L.hi(buf)), alo = tc::smemAddr(L.lo(buf)), bt = tc::smemAddr(L.Bt);
+         const uint32_t ahi = tc::smemAddr(L.hi), alo = tc::smemAddr(L.lo), bt = tc::smemAddr(L.Bt);
          const uint32_t id128 = tc::idesc(1, 1, 1, kRows, 128), id64 = tc::idesc(1, 1, 1, kRows, 64);
+         const uint32_t d = tmem;
          for (int k16 = 0; k16 < Kt / 16; k16++) {
             const int blk = k16 >> 2, sub = k16 & 3;
             // The swizzle is applied on absolute shared-memory address bits, so a start
@@ -499,72 +621,49 @@ __device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint3
             const uint64_t dHi = tc::descSw128(ahi + blk * 128 + sub * 32, 1024, 0);
             const uint64_t dLo = tc::descSw128(alo + blk * 128 + sub * 32, 1024, 0);
             const uint64_t dB = tc::descNoSwizzle(bt + k16 * 4096, 2048, 128);
-            tc::mmaF16(tmem, dHi, dB, id128, k16 > 0);
-            tc::mmaF16(tmem, dLo, dB, id64, true);
+            tc::mmaF16(d, dHi, dB, id128, k16 > 0);
+            tc::mmaF16(d, dLo, dB, id64, true);
          }
          tc::commit(L.mbar);
       }
-      // Stage the next tile into the other buffer while the tensor core works.
-      if (t + 1 < r.t1)
-         bfStage(r.x, r.inShift + j0 + kBfTile, r.inLen, nb, L.hi(buf ^ 1), L.lo(buf ^ 1), tid);
-      const bool done = tc::mbarWait(L.mbar, iter & 1);
-      if (!done && tid == 0) atomicExch(&g_firTcError, 1);
-      failed = __syncthreads_or(!done) != 0;
-      iter++;
-      tc::fenceAfterSync();
-      if (!failed) {
-         // Warp w drains TMEM lane quadrant w % 4 (rows a) and output half w / 4:
-         // y[j0 + 64a + 32*half + b] = D[a][32*half + b] + D[a][64 + 32*half + b].
-         const int quad = warp & 3, half = warp >> 2;
-         const uint32_t lanes = (uint32_t) (quad * 32) << 16;
-         const int row = quad * 32 + lane;
-         uint32_t p[32], q[32];
-         tc::tmemLoad32(tmem + lanes + half * 32, p);
-         tc::tmemLoad32(tmem + lanes + 64 + half * 32, q);
-         tc::tmemWaitLoad();
-         // The planes of this buffer are free once the MMAs completed: they hold the
-         // output tile, 16-byte chunk v4 of row half (row, half) rotated to slot
-         // (v4 + row) & 7 so that eight consecutive rows store to distinct banks.
-         float *os = (float *) L.hi(buf) + row * kBfPhases + half * 32;
-#pragma unroll
-         for (int v4 = 0; v4 < 8; v4++) {
-            float4 o;
-            o.x = __uint_as_float(p[4 * v4 + 0]) + __uint_as_float(q[4 * v4 + 0]);
-            o.y = __uint_as_float(p[4 * v4 + 1]) + __uint_as_float(q[4 * v4 + 1]);
-            o.z = __uint_as_float(p[4 * v4 + 2]) + __uint_as_float(q[4 * v4 + 2]);
-            o.w = __uint_as_float(p[4 * v4 + 3]) + __uint_as_float(q[4 * v4 + 3]);
-            *(float4 *) (os + (((v4 + row) & 7) << 2)) = o;
-         }
-      }
-      tc::fenceBeforeSync();
-      if (failed) break;
-      __syncthreads(); // the output tile is complete in shared memory
-      storeTile<float>(r.y + j0, (int) min((long long) kBfTile, (long long) r.outLen - j0),
-                       (const unsigned char *) L.hi(buf),
-                       [](int ci) {
-                          const int row = ci >> 4, half = (ci >> 3) & 1, v4 = ci & 7;
-                          return (row * kBfPhases + half * 32 + (((v4 + row) & 7) << 2)) * 4;
-                       },
-                       tid, kBfThreads);
+      if (!bfDrain(r, L, tmem, pp, t, tid)) return false;
    }
    __syncthreads(); // before the taps band of the next run is rebuilt
-   return !failed;
+   return true;
+}
+
+// Set-up and tear-down shared by the bf16x3 kernels.
+__device__ __forceinline__ uint32_t bfBegin(const BfSmem &L, int tid)
+{
+   if ((tid >> 5) == 0) tc::tmemAlloc(L.tslot, 128);
+   if (tid == 0) {
+      tc::mbarInit(L.mbar, 1);
+      for (int k = 0; k < 2; k++) tc::mbarInit(L.full + k, 1);
+      tc::fenceMbarInit();
+   }
+   tc::fenceBeforeSync();
+   __syncthreads();
+   tc::fenceAfterSync();
+   return *L.tslot;
+}
+
+__device__ __forceinline__ void bfEnd(const BfSmem &L, const BfPipe &pp, uint32_t tmem, int tid)
+{
+   // After a failure, let the copies still in flight land before the shared memory is released.
+   for (int k = 0; k < 2; k++)
+      if (tid == 0 && ((pp.pending >> k) & 1)) (void) tc::mbarWait(L.full + k, (pp.par >> k) & 1);
+   __syncthreads();
+   if ((tid >> 5) == 0) tc::tmemFree(tmem, 128);
 }
 
 __global__ void __launch_bounds__(kBfThreads, 1) fir_bf16x3_tc_kernel(FirLaunch a, int tilesPerCta)
 {
    extern __shared__ __align__(16) unsigned char smraw[];
    const BfSmem L = bfSmemLayout(smraw, a.T);
-   const int tid = threadIdx.x, warp = tid >> 5;
-   if (warp == 0) tc::tmemAlloc(L.tslot, 128);
-   if (tid == 0) tc::mbarInit(L.mbar, 1);
-   tc::fenceBeforeSync();
-   __syncthreads();
-   tc::fenceAfterSync();
-   const uint32_t tmem = *L.tslot;
-
+   const int tid = threadIdx.x;
+   const uint32_t tmem = bfBegin(L, tid);
    const int nt = (a.outSize + kBfTile - 1) / kBfTile;
-   uint32_t iter = 0;
+   BfPipe pp;
    for (int l = blockIdx.y; l < a.batch; l += gridDim.y) {
       BfRun r;
       r.x = (const float *) a.x + (long long) l * a.inPitch;
@@ -577,10 +676,9 @@ __global__ void __launch_bounds__(kBfThreads, 1) fir_bf16x3_tc_kernel(FirLaunch 
       r.reverse = 1;
       r.t0 = blockIdx.x * tilesPerCta;
       r.t1 = min(nt, r.t0 + tilesPerCta);
-      if (!bfProcess(r, L, tmem, iter, tid)) break;
+      if (!bfProcess(r, L, tmem, pp, tid)) break;
    }
-   __syncthreads();
-   if (warp == 0) tc::tmemFree(tmem, 128);
+   bfEnd(L, pp, tmem, tid);
 }
 
 // Work lists of the batched filter bank: one run of up to kFirBfRunTiles tiles of
@@ -593,13 +691,8 @@ __global__ void __launch_bounds__(kBfThreads, 1)
 {
    extern __shared__ __align__(16) unsigned char smraw[];
    const BfSmem L = bfSmemLayout(smraw, Tmax);
-   const int tid = threadIdx.x, warp = tid >> 5;
-   if (warp == 0) tc::tmemAlloc(L.tslot, 128);
-   if (tid == 0) tc::mbarInit(L.mbar, 1);
-   tc::fenceBeforeSync();
-   __syncthreads();
-   tc::fenceAfterSync();
-   const uint32_t tmem = *L.tslot;
+   const int tid = threadIdx.x;
+   const uint32_t tmem = bfBegin(L, tid);
    const int4 it = runs[blockIdx.x];
    const RaggedChan c = chans[it.x];
    BfRun r;
@@ -613,10 +706,9 @@ __global__ void __launch_bounds__(kBfThreads, 1)
    r.reverse = dx ? 0 : 1;
    r.t0 = it.y;
    r.t1 = it.y + it.z;
-   uint32_t iter = 0;
-   bfProcess(r, L, tmem, iter, tid);
-   __syncthreads();
-   if (warp == 0) tc::tmemFree(tmem, 128);
+   BfPipe pp;
+   bfProcess(r, L, tmem, pp, tid);
+   bfEnd(L, pp, tmem, tid);
 }
 
 } // namespace

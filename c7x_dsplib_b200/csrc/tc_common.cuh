@@ -78,6 +78,8 @@ __device__ __forceinline__ void commit(uint64_t *mbar)
 __device__ __forceinline__ void fenceBeforeSync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fenceAfterSync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 // Make generic-proxy shared-memory writes visible to the tensor core (async proxy).
+// Make mbarrier initialisation visible to the asynchronous (TMA) proxy.
+__device__ __forceinline__ void fenceMbarInit() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 __device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 __device__ __forceinline__ void mbarInit(uint64_t *mbar, uint32_t count)
@@ -106,6 +108,24 @@ __device__ __forceinline__ bool mbarWait(uint64_t *mbar, uint32_t parity, uint32
 }
 
 // TMEM allocation by one full warp; the base address is written to *slot (shared memory).
+// Announce `bytes` of transaction traffic on mbar (this thread's arrival included).
+__device__ __forceinline__ void mbarExpectTx(uint64_t *mbar, uint32_t bytes)
+{
+   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(mbar)), "r"(bytes)
+                : "memory");
+}
+
+// Bulk copy (TMA engine, no tensor map) of `bytes` from global memory to this
+// CTA's shared memory, completing as transaction bytes on mbar.  Both addresses
+// must be 16-byte aligned and bytes a multiple of 16; callers check.
+__device__ __forceinline__ void bulkLoad(void *dst, const void *src, uint32_t bytes, uint64_t *mbar)
+{
+   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smemAddr(dst)),
+                "l"(src), "r"(bytes), "r"(smemAddr(mbar))
+                : "memory");
+}
+
 __device__ __forceinline__ void tmemAlloc(uint32_t *slot, uint32_t ncols)
 {
    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(slot)),
