@@ -139,9 +139,10 @@ int firTcErrorFlag(bool clear);
 
 // One channel of the batched filter bank: samples at xOff (length L; the FIR
 // output and the biquad signals use the first Lu = L - T + 1), T taps at hOff,
-// S biquad stages (5 coefficients each) at cOff.
+// S biquad stages (5 coefficients each) at cOff; its slice of every work plane
+// (FIR output, stage outputs) at pOff, a multiple of 16 floats, round16(Lu) long.
 struct RaggedChan {
-   long long xOff, hOff, cOff;
+   long long xOff, hOff, cOff, pOff;
    int L, T, S, Lu;
 };
 // Split-BF16x3 tensor-core FIR over a list of runs {channel, first tile, tiles, 0}

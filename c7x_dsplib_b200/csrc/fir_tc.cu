@@ -698,7 +698,7 @@ __global__ void __launch_bounds__(kBfThreads, 1)
    BfRun r;
    r.x = in + c.xOff;
    r.h = taps + c.hOff;
-   r.y = out + c.xOff;
+   r.y = out + (dx ? c.xOff : c.pOff); // forward: plane 0 of the work buffer
    r.T = c.T;
    r.inShift = dx ? -(long long) (c.T - 1) : 0;
    r.inLen = dx ? c.L - c.T + 1 : c.L;

@@ -39,12 +39,14 @@
 
 #include "dsplib_internal.h"
 #include "scan_common.cuh"
+#include "tc_common.cuh"
 
 namespace dsplib {
 
 struct RaggedPlan {
    int C = 0;
    long long totalLen = 0, totalTaps = 0, totalCoefs = 0, totalOut = 0;
+   long long planeStride = 0; // floats per work plane: sum of round16(Lu)
    int Smax = 0, Tmax = 0;
    int nFwdItems = 0, nFirFwdRuns = 0, nFirDxRuns = 0;
    RaggedChan *dChan = nullptr;
@@ -74,10 +76,10 @@ constexpr int kBPad = kBL + 1;           // padded shared row per chunk (bank-co
 constexpr int kBPowers = 6 + kBLogWarps; // M^(2^k), M = A^16: lanes (k < 5), warps, and the window (last)
 constexpr int kRaggedMaxStages = 64;
 // Dynamic shared memory of biquad_ragged_kernel: per-stage carry, powers, coefficients and
-// (adjoint) FP64 coefficient-gradient sums; the adjoint adds two padded plane windows.
+// (adjoint) FP64 coefficient-gradient sums; the adjoint adds each thread's u / y chunk.
 constexpr size_t kBDynCommon = kRaggedMaxStages * sizeof(double2) + kRaggedMaxStages * kBPowers * sizeof(M2) +
-                               (kRaggedMaxStages * 5 + 2) * sizeof(float) + kRaggedMaxStages * 5 * sizeof(double);
-constexpr size_t kBDynPlanes = 2 * (size_t) (kBThreads + 1) * kBPad * sizeof(float);
+                               (kRaggedMaxStages * 5 + 4) * sizeof(float) + kRaggedMaxStages * 5 * sizeof(double);
+constexpr size_t kBDynPlanes = (size_t) kBThreads * 40 * sizeof(float);
 
 // DF2 over one chunk; WRITE: outputs replace v and, when w0 is given, the
 // recursion's internal sequence w0[i] is kept too.
@@ -99,19 +101,6 @@ __device__ __forceinline__ void df2Chunk(float (&v)[kBL], const float *cf, float
 
 // Padded shared-memory index of window sample k (one 17-float row per 16-sample chunk).
 __device__ __forceinline__ int padIdx(int k) { return (k >> 4) * kBPad + (k & 15); }
-
-// Load window samples [win0, win0 + n) of a channel plane into shared memory
-// (padded rows), time-reversed for the adjoint: sample k is src[Lu-1-(win0+k)].
-template <bool REV>
-__device__ __forceinline__ void stageWindow(float *dst, const float *src, int Lu, int win0, int n, int tid)
-{
-   for (int k = tid; k < n; k += kBThreads) {
-      const int tau = win0 + k;
-      float val = 0.0f;
-      if (tau < Lu) val = src[REV ? (Lu - 1 - tau) : tau];
-      dst[padIdx(k)] = val;
-   }
-}
 
 // One stage of the chunked scan over a window: v (this thread's 16 samples)
 // is filtered from the stage's carried state, the carry is advanced.  P: the
@@ -169,6 +158,9 @@ __device__ __forceinline__ void scanStage(float (&v)[kBL], const float *cf, cons
 }
 
 // One CTA per channel, longest first; windows of 8192 samples in sequence.
+// Work planes hold each channel's slice at pOff (a multiple of 16 floats), so a
+// thread's 16-sample chunk is one aligned 64-byte run: stage outputs go to and
+// come from the planes as 16-byte vectors, without a pass through shared memory.
 //
 // Forward (BWD = false): the cascade s = 0 .. S-1 over plane 0 (the FIR
 // output); stage s's output is stored to plane s+1 (the activations the
@@ -178,10 +170,14 @@ __device__ __forceinline__ void scanStage(float (&v)[kBL], const float *cf, cons
 // section run backwards in time (w0 = g - a1 w0[t+1] - a2 w0[t+2], gu = b0 w0 +
 // b1 w0[t+1] + b2 w0[t+2]), so the whole cascade adjoint is the cascade over
 // the time-reversed output gradient with the stages in reverse order; gu of
-// stage 0 goes to gout.  On the way, with v = that stage's w0 sequence, u its
+// stage 0 goes to gout.  Reversed time runs over the padded length
+// LuP = round16(Lu) (tau = LuP-1-t, zero input for t >= Lu), so its chunks are
+// the forward chunks.  On the way, with v = that stage's w0 sequence, u its
 // forward input (plane s) and y its output (plane s+1):
 //     dL/db_i = sum_t v[t] u[t-i],  dL/da_i = -sum_t v[t] y[t-i]
-// summed per chunk in FP32, per window and channel in FP64 in a fixed order.
+// summed per chunk in FP32, per window and channel in FP64 in a fixed order;
+// each thread fetches its chunk of u and y (plus the two samples before it)
+// with asynchronous copies issued before the stage's scan.
 template <bool BWD>
 __global__ void __launch_bounds__(kBThreads, 1)
     biquad_ragged_kernel(const RaggedChan *chans, const int *order, const float *coefs, const float *gin,
@@ -194,14 +190,14 @@ __global__ void __launch_bounds__(kBThreads, 1)
    double2 *sWin = (double2 *) dyn;                     // carry per stage
    M2 *sPow = (M2 *) (sWin + kRaggedMaxStages);         // M^(2^k) per stage
    float *sCf = (float *) (sPow + kRaggedMaxStages * kBPowers); // coefficients per stage
-   double *sAcc = (double *) (sCf + kRaggedMaxStages * 5 + 2);  // BWD: coefficient gradients per stage
-   float *sU = (float *) (sAcc + kRaggedMaxStages * 5);  // BWD: planes u / y of the stage, windows + 2
-   float *sY = sU + (kBThreads + 1) * kBPad;
+   double *sAcc = (double *) (sCf + kRaggedMaxStages * 5 + 4);  // BWD: coefficient gradients per stage
+   float *sUY = (float *) (sAcc + kRaggedMaxStages * 5);  // BWD: per thread, u and y of its chunk (20 + 20 floats)
 
    const RaggedChan c = chans[order[blockIdx.x]];
    const int S = c.S;
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
    const int Lu = c.Lu;
+   const int LuP = (Lu + 15) & ~15;
    const float *cbase = coefs + c.cOff;
    for (int s = tid; s < S; s += kBThreads) {
       sWin[s] = make_double2(0.0, 0.0);
@@ -221,43 +217,74 @@ __global__ void __launch_bounds__(kBThreads, 1)
          sPow[s * kBPowers + k] = A;
       }
    }
-   const float *src = BWD ? gin + c.xOff : planes + c.xOff;
-   float *dst = BWD ? gout + c.xOff : yout + c.xOff;
+   float *plane0 = planes + c.pOff;
+   // The FIR leaves plane 0 past Lu unwritten: zero it (the adjoint reads u there, times zero).
+   if (!BWD && tid < LuP - Lu) plane0[Lu + tid] = 0.0f;
+   float *uy = sUY + tid * 40; // u[tb-4 .. tb+15] then y[tb-4 .. tb+15]
    __syncthreads();
    int phase = 0;
-   for (int win0 = 0; win0 < Lu; win0 += kBWindow) {
-      stageWindow<BWD>(sbuf, src, Lu, win0, kBWindow, tid);
-      if (BWD && S > 0) stageWindow<true>(sY, planes + (long long) S * planeStride + c.xOff, Lu, win0, kBWindow + 2, tid);
-      __syncthreads();
+   for (int win0 = 0; win0 < LuP; win0 += kBWindow) {
+      const int c0 = win0 + tid * kBL; // chunk start: forward t, adjoint tau
+      const bool inChunk = c0 < LuP;
+      const int tb = LuP - kBL - c0;   // adjoint: the chunk's first t (a multiple of 16)
       float v[kBL];
+      if (BWD) {
+         // output gradient, time-reversed, zero past Lu
+         for (int k = tid; k < kBWindow; k += kBThreads) {
+            const int t = LuP - 1 - (win0 + k);
+            sbuf[padIdx(k)] = (t >= 0 && t < Lu) ? gin[c.xOff + t] : 0.0f;
+         }
+         __syncthreads();
 #pragma unroll
-      for (int i = 0; i < kBL; i++) v[i] = sbuf[tid * kBPad + i];
+         for (int i = 0; i < kBL; i++) v[i] = sbuf[tid * kBPad + i];
+      }
+      else if (inChunk) {
+#pragma unroll
+         for (int i4 = 0; i4 < kBL / 4; i4++) {
+            const float4 f = *(const float4 *) (plane0 + c0 + 4 * i4);
+            v[4 * i4 + 0] = c0 + 4 * i4 + 0 < Lu ? f.x : 0.0f;
+            v[4 * i4 + 1] = c0 + 4 * i4 + 1 < Lu ? f.y : 0.0f;
+            v[4 * i4 + 2] = c0 + 4 * i4 + 2 < Lu ? f.z : 0.0f;
+            v[4 * i4 + 3] = c0 + 4 * i4 + 3 < Lu ? f.w : 0.0f;
+         }
+      }
+      else {
+#pragma unroll
+         for (int i = 0; i < kBL; i++) v[i] = 0.0f;
+      }
       for (int q = 0; q < S; q++, phase++) {
          const int s = BWD ? S - 1 - q : q;
-         if (BWD) // this stage's forward input; its output (plane s+1) is already in sY
-            stageWindow<true>(sU, planes + (long long) s * planeStride + c.xOff, Lu, win0, kBWindow + 2, tid);
+         if (BWD && inChunk) {
+            // u = plane s, y = plane s+1 over [tb-4, tb+16): fetched while the scan runs
+            const float *pu = planes + (long long) s * planeStride + c.pOff + tb;
+            const float *py = pu + planeStride;
+#pragma unroll
+            for (int i4 = 0; i4 < 5; i4++) {
+               if (i4 > 0 || tb >= 4) {
+                  tc::cpAsync16(uy + 4 * i4, pu + 4 * i4 - 4);
+                  tc::cpAsync16(uy + 20 + 4 * i4, py + 4 * i4 - 4);
+               }
+               else {
+                  *(float4 *) uy = make_float4(0.f, 0.f, 0.f, 0.f); // before the channel's start
+                  *(float4 *) (uy + 20) = make_float4(0.f, 0.f, 0.f, 0.f);
+               }
+            }
+            tc::cpAsyncCommit();
+         }
          float w0s[kBL];
          scanStage<BWD>(v, sCf + s * 5, sPow + s * kBPowers, sWin + s, sTot[phase & 1], w0s, lane, warp);
          if (BWD) {
-            // reversed time: u[t-i] and y[t-i] are the samples i places later in the window
+            // chunk element i is t = tb + 15 - i: u[t-j] = uy[19 - i - j], y[t-j] = uy[39 - i - j]
             float p[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-            const int k0 = tid * kBL;
-            {
-               float uu[kBL + 2];
-#pragma unroll
-               for (int i = 0; i < kBL + 2; i++) uu[i] = sU[padIdx(k0 + i)];
+            if (inChunk) {
+               tc::cpAsyncWaitAll();
 #pragma unroll
                for (int i = 0; i < kBL; i++) {
-                  p[0] = fmaf(w0s[i], uu[i], p[0]);
-                  p[1] = fmaf(w0s[i], uu[i + 1], p[1]);
-                  p[2] = fmaf(w0s[i], uu[i + 2], p[2]);
-               }
-#pragma unroll
-               for (int i = 1; i < kBL + 2; i++) uu[i] = sY[padIdx(k0 + i)];
-#pragma unroll
-               for (int i = 0; i < kBL; i++) {
-                  p[3] = fmaf(-w0s[i], uu[i + 1], p[3]);
-                  p[4] = fmaf(-w0s[i], uu[i + 2], p[4]);
+                  p[0] = fmaf(w0s[i], uy[19 - i], p[0]);
+                  p[1] = fmaf(w0s[i], uy[18 - i], p[1]);
+                  p[2] = fmaf(w0s[i], uy[17 - i], p[2]);
+                  p[3] = fmaf(-w0s[i], uy[38 - i], p[3]);
+                  p[4] = fmaf(-w0s[i], uy[37 - i], p[4]);
                }
             }
 #pragma unroll
@@ -268,37 +295,29 @@ __global__ void __launch_bounds__(kBThreads, 1)
             if (lane == 0)
 #pragma unroll
                for (int q5 = 0; q5 < 5; q5++) sRed[warp][q5] = p[q5];
-            __syncthreads(); // sRed complete; every thread is done with sU / sY of this stage
+            __syncthreads(); // sRed complete
             if (tid < 5) {
                double acc = 0.0;
                for (int w = 0; w < kBWarps; w++) acc += (double) sRed[w][tid];
                sAcc[s * 5 + tid] += acc;
             }
-            float *t = sU; // plane s is the next stage's output plane
-            sU = sY;
-            sY = t;
          }
-         else {
-            // store this stage's output for the window (coalesced through shared memory)
-            __syncthreads(); // everyone has read sbuf
+         else if (inChunk) {
+            float *pl = planes + (long long) (s + 1) * planeStride + c.pOff + c0;
 #pragma unroll
-            for (int i = 0; i < kBL; i++) sbuf[tid * kBPad + i] = v[i];
-            __syncthreads();
-            float *pl = planes + (long long) (s + 1) * planeStride + c.xOff;
-            for (int k = tid; k < kBWindow; k += kBThreads) {
-               const int tau = win0 + k;
-               if (tau < Lu) pl[tau] = sbuf[padIdx(k)];
-            }
+            for (int i4 = 0; i4 < kBL / 4; i4++)
+               *(float4 *) (pl + 4 * i4) = make_float4(v[4 * i4], v[4 * i4 + 1], v[4 * i4 + 2], v[4 * i4 + 3]);
          }
       }
-      // window result: forward -> yout (the last stage's plane is also written above); adjoint -> gout
-      __syncthreads();
+      // window result (coalesced through shared memory): forward -> yout; adjoint -> gout, time order restored
+      __syncthreads(); // everyone has read sbuf
 #pragma unroll
       for (int i = 0; i < kBL; i++) sbuf[tid * kBPad + i] = v[i];
       __syncthreads();
+      float *dst = BWD ? gout + c.xOff : yout + c.xOff;
       for (int k = tid; k < kBWindow; k += kBThreads) {
-         const int tau = win0 + k;
-         if (tau < Lu) dst[BWD ? (Lu - 1 - tau) : tau] = sbuf[padIdx(k)];
+         const int t = BWD ? LuP - 1 - (win0 + k) : win0 + k;
+         if (t >= 0 && t < Lu) dst[t] = sbuf[padIdx(k)];
       }
       __syncthreads();
    }
@@ -471,14 +490,15 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
       const int tiles = (outLen + kFirBfTile - 1) / kFirBfTile;
       for (int t = 0; t < tiles; t += kFirBfRunTiles) runs.push_back(make_int4(c, t, std::min(kFirBfRunTiles, tiles - t), 0));
    };
-   long long xo = 0, ho = 0, co = 0;
+   long long xo = 0, ho = 0, co = 0, po = 0;
    for (int c = 0; c < numChannels; c++) {
       const int L = length[c], T = taps[c], S = stages[c];
       if (T < 1 || T > kFirBfMaxTaps || L < T || S < 0 || S > kRaggedMaxStages) {
          delete p;
          return DSPLIB_ERR_INVALID_DIMENSION;
       }
-      ch[c] = RaggedChan{xo, ho, co, L, T, S, L - T + 1};
+      ch[c] = RaggedChan{xo, ho, co, po, L, T, S, L - T + 1};
+      po += (L - T + 1 + 15) & ~15;
       xo += L;
       p->totalOut += L - T + 1;
       ho += T;
@@ -498,6 +518,7 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    std::stable_sort(firDx.begin(), firDx.end(), longer);
    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ch[a].Lu > ch[b].Lu; });
    p->totalLen = xo;
+   p->planeStride = po;
    p->totalTaps = ho;
    p->totalCoefs = co;
    p->nFwdItems = (int) fwd.size();
@@ -523,7 +544,7 @@ int64_t DSPLIB_gpu_raggedPlanSize(DSPLIB_gpu_raggedPlan plan, int32_t what)
    case DSPLIB_GPU_RAGGED_SAMPLES: return p->totalLen;
    case DSPLIB_GPU_RAGGED_TAPS: return p->totalTaps;
    case DSPLIB_GPU_RAGGED_COEFS: return p->totalCoefs;
-   case DSPLIB_GPU_RAGGED_WORK: return (long long) (p->Smax + 1) * p->totalLen;
+   case DSPLIB_GPU_RAGGED_WORK: return (long long) (p->Smax + 1) * p->planeStride;
    case DSPLIB_GPU_RAGGED_SCRATCH: return 2LL * p->totalLen + (long long) p->nFwdItems * kDhMaxT;
    case DSPLIB_GPU_RAGGED_OUTPUTS: return p->totalOut;
    default: return -1;
@@ -549,7 +570,7 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_fwd(DSPLIB_gpu_raggedPlan plan, const 
                             (int) kBDynCommon) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
    biquad_ragged_kernel<false><<<p->C, kBThreads, kBDynCommon, s>>>(p->dChan, p->dOrder, coefs, nullptr, work,
-                                                                      p->totalLen, y, nullptr, nullptr);
+                                                                      p->planeStride, y, nullptr, nullptr);
    countLaunch(1);
    return cudaGetLastError() == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
 }
@@ -569,7 +590,7 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
        cudaSuccess)
       return DSPLIB_ERR_FAILURE;
    biquad_ragged_kernel<true><<<p->C, kBThreads, dyn, s>>>(p->dChan, p->dOrder, coefs, gy, (float *) work,
-                                                            p->totalLen, nullptr, g, gcoefs);
+                                                            p->planeStride, nullptr, g, gcoefs);
    if (launchFirBf16x3Ragged(p->dChan, p->dFirDxRuns, p->nFirDxRuns, g, taps, gx, true, p->Tmax, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
    fir_dh_partial_kernel<<<p->nFwdItems, 256, 0, s>>>(p->dChan, p->dFwdItems, x, g, part);

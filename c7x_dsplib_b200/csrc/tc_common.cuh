@@ -126,6 +126,14 @@ __device__ __forceinline__ void bulkLoad(void *dst, const void *src, uint32_t by
                 : "memory");
 }
 
+// 16-byte asynchronous copy global -> shared (both addresses 16-byte aligned).
+__device__ __forceinline__ void cpAsync16(void *dst, const void *src)
+{
+   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smemAddr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void tmemAlloc(uint32_t *slot, uint32_t ncols)
 {
    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(slot)),

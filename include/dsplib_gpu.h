@@ -76,7 +76,8 @@ typedef enum {
    DSPLIB_GPU_RAGGED_SAMPLES = 0, /* floats in x / gx (sum L_c) */
    DSPLIB_GPU_RAGGED_TAPS = 1,    /* floats in taps / gtaps (sum T_c) */
    DSPLIB_GPU_RAGGED_COEFS = 2,   /* floats in coefs / gcoefs (5 sum S_c) */
-   DSPLIB_GPU_RAGGED_WORK = 3,    /* floats of the forward activations (max S_c + 1) * sum L_c */
+   DSPLIB_GPU_RAGGED_WORK = 3,    /* floats of the forward activations: (max S_c + 1) planes of
+                                     sum_c round16(L_c - T_c + 1) floats */
    DSPLIB_GPU_RAGGED_SCRATCH = 4, /* floats of adjoint scratch */
    DSPLIB_GPU_RAGGED_OUTPUTS = 5, /* valid output samples (sum L_c - T_c + 1) */
 } DSPLIB_gpu_raggedSize;
@@ -90,9 +91,9 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
 int64_t DSPLIB_gpu_raggedPlanSize(DSPLIB_gpu_raggedPlan plan, int32_t what);
 DSPLIB_STATUS DSPLIB_gpu_raggedPlanDestroy(DSPLIB_gpu_raggedPlan plan);
 
-/** Forward: y from x, taps and coefs.  work receives the FIR output and every
- *  stage's output (kept for the adjoint).  Queued on `stream`; no allocation,
- *  no host synchronisation. */
+/** Forward: y from x, taps and coefs.  work (16-byte aligned) receives the FIR
+ *  output and every stage's output (kept for the adjoint).  Queued on `stream`;
+ *  no allocation, no host synchronisation. */
 DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_fwd(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
                                               const float *coefs, float *y, float *work, void *stream);
 /** Adjoint: given gy = dLoss/dy and the forward's work buffer, writes
