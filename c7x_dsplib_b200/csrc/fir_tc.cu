@@ -165,7 +165,7 @@ __device__ __forceinline__ void storeTile(T *dst, int n, const unsigned char *st
 }
 
 template <typename T, int QMODE>
-__global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int tilesPerCta)
+__global__ void __launch_bounds__(kThreads, 8) fir_int_tc_kernel(FirLaunch a, int tilesPerCta)
 {
    constexpr bool SPLIT = sizeof(T) == 2;
    constexpr uint32_t kCols = SPLIT ? 64 : 32; // TMEM columns (accumulators of 16 columns each)
@@ -269,7 +269,20 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
             }
             tc::commit(mbar);
          }
-         if (t + 1 < t1) intStage<T>(x + j0 + kTile, j0 + kTile, inExtent, seg, A(buf ^ 1, 0), A(buf ^ 1, 1), tid);
+         // Fetch the next segment into registers now; it is written to shared memory after
+         // this tile's drain, so the load latency hides behind the MMAs and the drain.
+         constexpr int kPre = SPLIT ? 5 : 3; // 16-byte vectors per thread: (2048 + 2080) * sizeof(T) / 16 / 128
+         int4 pre[kPre];
+         const long long jn = j0 + kTile;
+         const bool preVec = t + 1 < t1 && jn + seg <= inExtent && ((((uintptr_t) (x + jn)) & 15) == 0);
+         const int nvec = seg * (int) sizeof(T) / 16;
+         if (preVec) {
+#pragma unroll
+            for (int i = 0; i < kPre; i++) {
+               const int k = tid + i * kThreads;
+               if (k < nvec) pre[i] = ((const int4 *) (x + jn))[k];
+            }
+         }
          const bool done = tc::mbarWait(mbar, iter & 1);
          if (!done && tid == 0) atomicExch(&g_firTcError, 1);
          failed = __syncthreads_or(!done) != 0;
@@ -312,6 +325,32 @@ __global__ void __launch_bounds__(kThreads) fir_int_tc_kernel(FirLaunch a, int t
          __syncthreads(); // the output tile is complete in shared memory
          storeTile<T>(y + j0, (int) min((long long) kTile, (long long) a.outSize - j0),
                       (const unsigned char *) ostage, [](int ci) { return ci * 16; }, tid, kThreads);
+         if (preVec) {
+            unsigned char *N0 = A(buf ^ 1, 0), *N1 = A(buf ^ 1, 1);
+#pragma unroll
+            for (int i = 0; i < kPre; i++) {
+               const int k = tid + i * kThreads;
+               if (k < nvec) {
+                  if (!SPLIT) {
+                     ((int4 *) N0)[k] = pre[i];
+                  }
+                  else {
+                     const int16_t *e = (const int16_t *) &pre[i];
+                     __align__(8) unsigned char hb[8], lb[8];
+#pragma unroll
+                     for (int q = 0; q < 8; q++) {
+                        hb[q] = (unsigned char) (e[q] >> 8);
+                        lb[q] = (unsigned char) (e[q] & 0xFF);
+                     }
+                     ((uint2 *) N0)[k] = *(uint2 *) hb;
+                     ((uint2 *) N1)[k] = *(uint2 *) lb;
+                  }
+               }
+            }
+         }
+         else if (t + 1 < t1) {
+            intStage<T>(x + jn, jn, inExtent, seg, A(buf ^ 1, 0), A(buf ^ 1, 1), tid); // row edge / unaligned
+         }
       }
       __syncthreads(); // before the next channel's taps overwrite the band
    }
@@ -378,14 +417,25 @@ __device__ __forceinline__ void bfStage(const float *x, long long q0, long long 
                                         unsigned char *Alo, int tid)
 {
    float f[kBfChunksPerThread][8];
+   // chunk starts are 8 floats apart, so all share one misalignment (in floats)
+   const int mis = (int) ((((uintptr_t) (x + q0)) >> 2) & 3);
 #pragma unroll
    for (int u = 0; u < kBfChunksPerThread; u++) {
       const int cidx = tid + u * kBfThreads;
       if (cidx < nb * 8) {
          const long long q = q0 + (long long) (cidx >> 3) * 64 + (cidx & 7) * 8;
-         if (q >= 0 && q + 8 <= inLen && ((((uintptr_t) (x + q)) & 15) == 0)) {
+         if (mis == 0 && q >= 0 && q + 8 <= inLen) {
             *(float4 *) &f[u][0] = *(const float4 *) (x + q);
             *(float4 *) &f[u][4] = *(const float4 *) (x + q + 4);
+         }
+         else if (mis != 0 && q - mis >= 0 && q - mis + 12 <= inLen) {
+            // three aligned vectors around the chunk, then pick its 8 samples
+            const float4 a = *(const float4 *) (x + q - mis);
+            const float4 b = *(const float4 *) (x + q - mis + 4);
+            const float4 cc = *(const float4 *) (x + q - mis + 8);
+            const float w[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, cc.x, cc.y, cc.z, cc.w};
+#pragma unroll
+            for (int e = 0; e < 8; e++) f[u][e] = mis == 1 ? w[1 + e] : (mis == 2 ? w[2 + e] : w[3 + e]);
          }
          else {
 #pragma unroll
