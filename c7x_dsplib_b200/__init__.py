@@ -64,6 +64,15 @@ class BiquadInitArgs(ctypes.Structure):
                 ("biquadForm", ctypes.c_uint32)]
 
 
+class BufParams1D(ctypes.Structure):
+    _fields_ = [("data_type", ctypes.c_uint32), ("dim_x", ctypes.c_uint32)]
+
+
+class ConvertInitArgs(ctypes.Structure):
+    """DSPLIB_fltoq15_InitArgs and DSPLIB_q15tofl_InitArgs (same layout)."""
+    _fields_ = [("funcStyle", ctypes.c_int8), ("dataSize", ctypes.c_uint32)]
+
+
 _lib = None
 _P = ctypes.POINTER
 _VP = ctypes.c_void_p
@@ -87,6 +96,16 @@ SIGNATURES = {
     "DSPLIB_cascadeBiquad_exec": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_cascadeBiquad_exec_checkParams": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_cascadeBiquad_perfEst": (None, [_VP, _BP, _BP, _BP, _BP, _P(ctypes.c_uint64), _P(ctypes.c_uint64)]),
+    "DSPLIB_fltoq15_getHandleSize": (ctypes.c_int32, [_P(ConvertInitArgs)]),
+    "DSPLIB_fltoq15_init_checkParams": (ctypes.c_int, [_VP, _P(BufParams1D), _P(BufParams1D), _P(ConvertInitArgs)]),
+    "DSPLIB_fltoq15_init": (ctypes.c_int, [_VP, _P(BufParams1D), _P(BufParams1D), _P(ConvertInitArgs)]),
+    "DSPLIB_fltoq15_exec_checkParams": (ctypes.c_int, [_VP, _VP, _VP]),
+    "DSPLIB_fltoq15_exec": (ctypes.c_int, [_VP, _VP, _VP]),
+    "DSPLIB_q15tofl_getHandleSize": (ctypes.c_int32, [_P(ConvertInitArgs)]),
+    "DSPLIB_q15tofl_init_checkParams": (ctypes.c_int, [_VP, _P(BufParams1D), _P(BufParams1D), _P(ConvertInitArgs)]),
+    "DSPLIB_q15tofl_init": (ctypes.c_int, [_VP, _P(BufParams1D), _P(BufParams1D), _P(ConvertInitArgs)]),
+    "DSPLIB_q15tofl_exec_checkParams": (ctypes.c_int, [_VP, _VP, _VP]),
+    "DSPLIB_q15tofl_exec": (ctypes.c_int, [_VP, _VP, _VP]),
     "DSPLIB_gpu_setStream": (ctypes.c_int, [_VP, _VP]),
     "DSPLIB_gpu_setAsync": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_lastError": (ctypes.c_char_p, [_VP]),
@@ -94,6 +113,11 @@ SIGNATURES = {
     "DSPLIB_gpu_firSetQMode": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_kernelLaunchCount": (ctypes.c_int64, []),
     "DSPLIB_gpu_releaseHandle": (ctypes.c_int, [_VP]),
+    "DSPLIB_gpu_firStreamCreate": (ctypes.c_int, [_P(_VP), _P(FirInitArgs), _BP, _BP, _BP]),
+    "DSPLIB_gpu_firStreamHandle": (_VP, [_VP]),
+    "DSPLIB_gpu_firStreamExec": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    "DSPLIB_gpu_firStreamReset": (ctypes.c_int, [_VP]),
+    "DSPLIB_gpu_firStreamDestroy": (ctypes.c_int, [_VP]),
     "DSPLIB_gpu_raggedPlanCreate": (ctypes.c_int, [_P(_VP), ctypes.c_int32, _P(ctypes.c_int32),
                                                    _P(ctypes.c_int32), _P(ctypes.c_int32)]),
     "DSPLIB_gpu_raggedPlanSize": (ctypes.c_int64, [_VP, ctypes.c_int32]),
@@ -221,6 +245,74 @@ class BiquadHandle(_Handle):
         return lib().DSPLIB_cascadeBiquad_exec(self.h, _ptr(x), _ptr(coef), _ptr(state), _ptr(y))
 
 
+class Fltoq15Handle(_Handle):
+    """Reference call sequence of test/DSPLIB_fltoq15/DSPLIB_fltoq15_d.c:100-221."""
+
+    size_fn = "DSPLIB_fltoq15_getHandleSize"
+    prefix = "DSPLIB_fltoq15"
+
+    def init(self, args: ConvertInitArgs, pin: BufParams1D, pout: BufParams1D) -> int:
+        return getattr(lib(), self.prefix + "_init")(self.h, ctypes.byref(pin), ctypes.byref(pout), ctypes.byref(args))
+
+    def init_check(self, args, pin, pout) -> int:
+        return getattr(lib(), self.prefix + "_init_checkParams")(self.h, ctypes.byref(pin), ctypes.byref(pout),
+                                                                 ctypes.byref(args))
+
+    def exec(self, x, y) -> int:
+        return getattr(lib(), self.prefix + "_exec")(self.h, _ptr(x), _ptr(y))
+
+
+class Q15toflHandle(Fltoq15Handle):
+    """Reference call sequence of test/DSPLIB_q15tofl/DSPLIB_q15tofl_d.c."""
+
+    size_fn = "DSPLIB_q15tofl_getHandleSize"
+    prefix = "DSPLIB_q15tofl"
+
+
+def _float_code(a):
+    dt = a.dtype if isinstance(a, np.ndarray) else str(a.dtype).replace("torch.", "")
+    return {"float32": FLOAT32, "float64": FLOAT64}[str(dt)]
+
+
+def fltoq15(x, *, func_style=OPTIMIZED, out=None, handle=None):
+    """Float32 / float64 array (numpy or torch, host or device) to Q.15 int16."""
+    n = int(x.size if isinstance(x, np.ndarray) else x.numel())
+    if out is None:
+        if isinstance(x, np.ndarray):
+            out = np.zeros(n, np.int16)
+        else:
+            import torch
+
+            out = torch.zeros(n, dtype=torch.int16, device=x.device)
+    hd = handle or Fltoq15Handle()
+    args = ConvertInitArgs(funcStyle=func_style, dataSize=n)
+    pin, pout = BufParams1D(_float_code(x), n), BufParams1D(INT16, n)
+    hd._check("DSPLIB_fltoq15_init_checkParams", hd.init_check(args, pin, pout))
+    hd._check("DSPLIB_fltoq15_init", hd.init(args, pin, pout))
+    hd._check("DSPLIB_fltoq15_exec", hd.exec(x, out))
+    return out
+
+
+def q15tofl(x, dtype=np.float32, *, func_style=OPTIMIZED, out=None, handle=None):
+    """Q.15 int16 array (numpy or torch, host or device) to float32 / float64."""
+    n = int(x.size if isinstance(x, np.ndarray) else x.numel())
+    code = {np.dtype(np.float32): FLOAT32, np.dtype(np.float64): FLOAT64}[np.dtype(dtype)]
+    if out is None:
+        if isinstance(x, np.ndarray):
+            out = np.zeros(n, dtype)
+        else:
+            import torch
+
+            out = torch.zeros(n, dtype=torch.float32 if code == FLOAT32 else torch.float64, device=x.device)
+    hd = handle or Q15toflHandle()
+    args = ConvertInitArgs(funcStyle=func_style, dataSize=n)
+    pin, pout = BufParams1D(INT16, n), BufParams1D(code, n)
+    hd._check("DSPLIB_q15tofl_init_checkParams", hd.init_check(args, pin, pout))
+    hd._check("DSPLIB_q15tofl_init", hd.init(args, pin, pout))
+    hd._check("DSPLIB_q15tofl_exec", hd.exec(x, out))
+    return out
+
+
 # ------------------------------------------------------------------ helpers
 
 
@@ -265,6 +357,50 @@ def fir(x, h, T=None, *, nch=None, func_style=OPTIMIZED, precision=FIR_SIMT, qmo
     hd.set_qmode(qmode)
     hd._check("DSPLIB_fir_exec", hd.exec(x, h, out))
     return out
+
+
+class FirStream:
+    """Streaming (overlap-save) FIR: each ``exec`` takes ``block`` new samples per
+    channel (rows of ``x``) and returns ``block`` outputs per channel; the last
+    ``T - 1`` samples of every channel are kept on the device for the next call
+    (``DSPLIB_gpu_firStream*``)."""
+
+    def __init__(self, dtype_code, channels, block, T, *, nch, func_style=OPTIMIZED, shift=0, precision=FIR_SIMT,
+                 qmode=False):
+        elt = _elt(dtype_code)
+        self.channels, self.block, self.T = channels, block, T
+        args = FirInitArgs(funcStyle=func_style, dataSize=block, batchSize=channels, filterSize=T, shift=shift,
+                           enableNchCoefs=int(nch), enableMMA=0, MMA_SIZE=MMA_SIZE[elt], enableQ=0, Q=0)
+        pin = bp(dtype_code, block, channels, block * elt)
+        pout = bp(dtype_code, block, channels, block * elt)
+        pfilt = bp(dtype_code, T, channels if nch else 1, T * elt)
+        self.s = ctypes.c_void_p()
+        st = lib().DSPLIB_gpu_firStreamCreate(ctypes.byref(self.s), ctypes.byref(args), ctypes.byref(pin),
+                                              ctypes.byref(pfilt), ctypes.byref(pout))
+        if st != SUCCESS:
+            raise DsplibError("DSPLIB_gpu_firStreamCreate", st)
+        h = lib().DSPLIB_gpu_firStreamHandle(self.s)
+        lib().DSPLIB_gpu_firSetPrecision(h, precision)
+        lib().DSPLIB_gpu_firSetQMode(h, int(bool(qmode)))
+        self.h = h
+
+    def exec(self, x, h, out):
+        st = lib().DSPLIB_gpu_firStreamExec(self.s, _ptr(x), _ptr(h), _ptr(out))
+        if st != SUCCESS:
+            msg = lib().DSPLIB_gpu_lastError(self.h)
+            raise DsplibError("DSPLIB_gpu_firStreamExec", st, msg.decode() if msg else "")
+        return out
+
+    def reset(self):
+        return lib().DSPLIB_gpu_firStreamReset(self.s)
+
+    def __del__(self):
+        if getattr(self, "s", None) is not None and self.s.value:
+            try:
+                lib().DSPLIB_gpu_firStreamDestroy(self.s)
+            except Exception:
+                pass
+            self.s = None
 
 
 def biquad_descs(C, N, S, form, nch, *, pitch=None, var_pitch=None, func_style=OPTIMIZED):

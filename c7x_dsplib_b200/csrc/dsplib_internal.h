@@ -14,6 +14,8 @@ namespace dsplib {
 
 constexpr uint32_t kMagicFir = 0xF1A0B200u;
 constexpr uint32_t kMagicBiquad = 0xB1A0B200u;
+constexpr uint32_t kMagicFltoq15 = 0xF15AB200u;
+constexpr uint32_t kMagicQ15tofl = 0x15F0B200u;
 
 // First member of every handle: GPU settings that survive re-init
 // (the reference test drivers re-run init on the same handle to switch
@@ -51,6 +53,16 @@ struct BiquadPriv {
    int32_t initialized;
 };
 
+// DSPLIB_fltoq15 / DSPLIB_q15tofl handle (DSPLIB_fltoq15_priv.h / DSPLIB_q15tofl_priv.h
+// of the reference keep blockSize = dataSize and the type-specific exec).
+struct Q15Priv {
+   HandleCommon common;
+   int32_t funcStyle;
+   uint32_t dataSize; // elements per exec
+   int32_t isDouble;  // float side is FLOAT64
+   int32_t initialized;
+};
+
 // ---------------------------------------------------------------- runtime
 
 void setError(HandleCommon *h, const char *fmt, ...);
@@ -84,6 +96,10 @@ cudaError_t regionIn(Region &r, int slot, bool copyIn, cudaStream_t s);
 // Copy a staged region back to the caller's host buffer (row by row, leaving
 // the bytes between rows untouched).
 cudaError_t regionOut(const Region &r, cudaStream_t s);
+
+// Device pointer through which kernels reach a page-locked host buffer (nullptr
+// when p is not page-locked host memory).
+void *mappedHostPtr(const void *p);
 
 // Copy `rows` rows of `width` bytes, `pitch` bytes apart, in one call.
 cudaError_t copyRows(void *dst, const void *src, size_t width, size_t rows, size_t pitch, cudaMemcpyKind kind,
@@ -130,6 +146,11 @@ enum FirKernelKind {
 };
 
 cudaError_t launchFir(const FirLaunch &a, FirKernelKind kind, cudaStream_t s);
+
+// Q.15 conversions over n elements (any alignment; 16-byte aligned pointers take the
+// vector kernels).  natc: the natural-C rounding steps, else round-half-to-even.
+cudaError_t launchFltoq15(const void *in, int16_t *out, long long n, bool isDouble, bool natc, cudaStream_t s);
+cudaError_t launchQ15tofl(const int16_t *in, void *out, long long n, bool isDouble, cudaStream_t s);
 bool firIntTcSupported(const FirLaunch &a);
 bool firBf16x3Supported(const FirLaunch &a);
 cudaError_t launchFirIntTc(const FirLaunch &a, bool qmode, cudaStream_t s);

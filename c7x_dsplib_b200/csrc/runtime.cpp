@@ -50,6 +50,8 @@ static void *pinnedDevicePtr(const void *p)
    return attr.type == cudaMemoryTypeHost ? attr.devicePointer : nullptr;
 }
 
+void *mappedHostPtr(const void *p) { return pinnedDevicePtr(p); }
+
 namespace {
 constexpr int kMaxDevices = 16;
 constexpr int kSlots = 6;
@@ -150,7 +152,8 @@ static HandleCommon *common(DSPLIB_kernelHandle h)
 {
    if (!h) return nullptr;
    HandleCommon *c = (HandleCommon *) h;
-   if (c->magic != kMagicFir && c->magic != kMagicBiquad) return nullptr;
+   if (c->magic != kMagicFir && c->magic != kMagicBiquad && c->magic != kMagicFltoq15 && c->magic != kMagicQ15tofl)
+      return nullptr;
    return c;
 }
 

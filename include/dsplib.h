@@ -1,4 +1,4 @@
-/* Umbrella header, as src/dsplib.h of the reference (:19 biquad, :28 FIR). */
+/* Umbrella header, as src/dsplib.h of the reference (:19 biquad, :28 FIR, :29 fltoq15, :53 q15tofl). */
 #ifndef DSPLIB_H_
 #define DSPLIB_H_
 
@@ -6,6 +6,8 @@
 #include "DSPLIB_bufParams.h"
 #include "DSPLIB_cascadeBiquad.h"
 #include "DSPLIB_fir.h"
+#include "DSPLIB_fltoq15.h"
+#include "DSPLIB_q15tofl.h"
 #include "dsplib_gpu.h"
 
 #endif

@@ -54,6 +54,36 @@ int64_t DSPLIB_gpu_kernelLaunchCount(void);
 DSPLIB_STATUS DSPLIB_gpu_releaseHandle(DSPLIB_kernelHandle handle);
 
 /* ---------------------------------------------------------------------------
+ * Streaming (overlap-save) FIR.  DSPLIB_fir computes "valid" outputs: N input
+ * samples give N - T + 1 outputs, and a caller filtering a continuous signal in
+ * blocks must carry each channel's last T - 1 input samples into the next call
+ * (the reference leaves this to the caller, test/DSPLIB_fir/DSPLIB_fir_d.c).  A
+ * stream keeps that history on the device: every call takes dataSize new samples
+ * per channel and returns dataSize outputs per channel, as if the whole signal,
+ * preceded by T - 1 zeros, had been filtered in one call.  No counterpart in the
+ * reference.
+ * ------------------------------------------------------------------------- */
+typedef struct DSPLIB_gpu_firStream_s *DSPLIB_gpu_firStream;
+
+/** args, bufParamsFilter as for DSPLIB_fir_init, with args->dataSize = new samples
+ *  per channel and block; bufParamsIn / bufParamsOut describe one block of input /
+ *  output (dim_x = dataSize, dim_y = channels, stride_y = row pitch in bytes).
+ *  Allocates the device history and window buffers (DSPLIB_gpu_firStreamDestroy
+ *  frees them); the history starts at zero. */
+DSPLIB_STATUS DSPLIB_gpu_firStreamCreate(DSPLIB_gpu_firStream *stream, const DSPLIB_fir_InitArgs *args,
+                                         const DSPLIB_bufParams2D_t *bufParamsIn,
+                                         const DSPLIB_bufParams2D_t *bufParamsFilter,
+                                         const DSPLIB_bufParams2D_t *bufParamsOut);
+/** The stream's internal DSPLIB_fir handle: DSPLIB_gpu_setStream / setAsync /
+ *  firSetPrecision / firSetQMode / lastError apply to the stream through it. */
+DSPLIB_kernelHandle DSPLIB_gpu_firStreamHandle(DSPLIB_gpu_firStream stream);
+/** Filter the next block (host or device buffers, as DSPLIB_fir_exec). */
+DSPLIB_STATUS DSPLIB_gpu_firStreamExec(DSPLIB_gpu_firStream stream, const void *pIn, void *pFilter, void *pOut);
+/** Zero the history (start a new signal). */
+DSPLIB_STATUS DSPLIB_gpu_firStreamReset(DSPLIB_gpu_firStream stream);
+DSPLIB_STATUS DSPLIB_gpu_firStreamDestroy(DSPLIB_gpu_firStream stream);
+
+/* ---------------------------------------------------------------------------
  * Batched filter bank over channels of uneven length, forward and adjoint.
  * Per channel c (length L_c, T_c taps, S_c second-order stages):
  *     u_c = DSPLIB_fir valid correlation of x_c with h_c      (L_c - T_c + 1 samples)

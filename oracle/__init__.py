@@ -4,8 +4,9 @@ Two checkers live here, both loaded through ctypes:
 
 * ``port``: this project's C restatement (``dsplib_oracle.c``), built into
   ``oracle/_build/liboracle_port.so`` by ``oracle/Makefile``.
-* ``ref``: the reference's own natural-C kernels (``DSPLIB_fir_cn.cpp`` and
-  ``DSPLIB_cascadeBiquad_cn.cpp``) compiled unmodified, with the stand-in TI
+* ``ref``: the reference's own natural-C kernels (``DSPLIB_fir_cn.cpp``,
+  ``DSPLIB_cascadeBiquad_cn.cpp``, ``DSPLIB_fltoq15_cn.cpp``, ``DSPLIB_q15tofl_cn.cpp``)
+  compiled unmodified, with the stand-in TI
   headers of ``oracle/shim``, into ``oracle/_ref/libdsplib_ref.so``.  Present
   whenever the library was built here (it travels with the repository
   snapshot) — it is optional; tests that need it skip when it is absent.
@@ -57,7 +58,8 @@ def port():
             build()
         _port = ctypes.CDLL(PORT_SO)
         for name in ("oracle_fir_cn", "oracle_fir_q", "oracle_fir_f64", "oracle_biquad_df",
-                     "oracle_biquad_df_f64", "oracle_biquad_tif", "oracle_tif_coefficients"):
+                     "oracle_biquad_df_f64", "oracle_biquad_tif", "oracle_tif_coefficients", "oracle_fltoq15",
+                     "oracle_q15tofl"):
             getattr(_port, name).restype = None
     return _port
 
@@ -196,3 +198,41 @@ def biquad_tif(x, tif_coef, gains, state, *, nch):
     port().oracle_biquad_tif(_ptr(x), _ptr(tif_coef), _ptr(gains), _ptr(state), _ptr(y), N, S, C, int(nch), C, C,
                              state.shape[1])
     return y
+
+
+# ------------------------------------------------------------------ Q.15 conversions
+
+_FT = {np.dtype(np.float32): 12, np.dtype(np.float64): 13}
+
+
+def fltoq15(x, *, style="natc", impl="port"):
+    """Float (float32 / float64, 1-D) to Q.15 int16.  ``style``: "natc" (the natural-C
+    steps, DSPLIB_fltoq15_cn.cpp:35-62) or "opt" (round half to even, saturate).
+    ``impl='ref'`` runs the reference _cn kernel itself (natc only; inputs whose
+    scaled value leaves the int32 range are undefined there)."""
+    x = np.ascontiguousarray(x)
+    out = np.zeros(x.size, np.int16)
+    dt = _FT[x.dtype]
+    if impl == "ref":
+        if style != "natc":
+            raise ValueError("the reference natural-C kernel has one style")
+        rc = ref().ref_fltoq15_cn(dt, _ptr(x), _ptr(out), ctypes.c_int(x.size))
+        if rc != 0:
+            raise RuntimeError(f"ref_fltoq15_cn: {rc}")
+    else:
+        port().oracle_fltoq15(dt, 0 if style == "natc" else 1, _ptr(x), _ptr(out), ctypes.c_longlong(x.size))
+    return out
+
+
+def q15tofl(x, dtype=np.float32, *, impl="port"):
+    """Q.15 int16 (1-D) to float32 / float64: x / 32768 (DSPLIB_q15tofl_cn.cpp:33-37)."""
+    x = np.ascontiguousarray(x, dtype=np.int16)
+    out = np.zeros(x.size, dtype)
+    dt = _FT[np.dtype(dtype)]
+    if impl == "ref":
+        rc = ref().ref_q15tofl_cn(dt, _ptr(x), _ptr(out), ctypes.c_int(x.size))
+        if rc != 0:
+            raise RuntimeError(f"ref_q15tofl_cn: {rc}")
+    else:
+        port().oracle_q15tofl(dt, _ptr(x), _ptr(out), ctypes.c_longlong(x.size))
+    return out

@@ -277,3 +277,77 @@ void oracle_tif_coefficients(const float *natural, int S, float *tifCoef, float 
       gains[g] = gain;
    }
 }
+
+/* ---------------------------------------------------------------- Q.15 conversions */
+
+/* float/double -> int32 truncation toward zero; saturating by sign outside the
+ * int32 range and 0 for NaN (where the reference's C cast is undefined). */
+static int32_t trunc_sat(double v)
+{
+   if (v != v) return 0;
+   if (v >= 2147483647.0) return INT32_MAX;
+   if (v <= -2147483648.0) return INT32_MIN;
+   return (int32_t) v;
+}
+
+static int16_t sat16(int32_t v) { return (int16_t) (v > 32767 ? 32767 : (v < -32768 ? -32768 : v)); }
+
+/* DSPLIB_fltoq15_cn.cpp:36-60, float arithmetic kept in float. */
+static int16_t q15_natc_f(float a)
+{
+   const float m = a * 32768.0f;
+   const int32_t ip = trunc_sat(m);
+   const float fp = m - (float) ip;
+   int32_t r;
+   if (ip % 2 == 0 && fabsf(fp) == 0.5f) r = ip;
+   else if (a < 0) r = trunc_sat((float) (m - 0.5f));
+   else r = trunc_sat((float) (m + 0.5f));
+   return sat16(r);
+}
+
+/* The same steps for double input (the 0.5f constant widens to 0.5). */
+static int16_t q15_natc_d(double a)
+{
+   const double m = a * 32768.0;
+   const int32_t ip = trunc_sat(m);
+   const double fp = m - (double) ip;
+   int32_t r;
+   if (ip % 2 == 0 && fabs(fp) == 0.5) r = ip;
+   else if (a < 0) r = trunc_sat(m - 0.5);
+   else r = trunc_sat(m + 0.5);
+   return sat16(r);
+}
+
+/* Round half to even with saturation (the C7x conversion instructions). */
+static int16_t q15_rne(double m)
+{
+   if (m != m) return 0;
+   if (m >= 32767.0) return 32767;
+   if (m <= -32768.0) return -32768;
+   double f = floor(m);
+   const double d = m - f;
+   if (d > 0.5 || (d == 0.5 && fmod(f, 2.0) != 0.0)) f += 1.0;
+   return (int16_t) f;
+}
+
+void oracle_fltoq15(int dtype, int style, const void *in, int16_t *out, long long n)
+{
+   for (long long i = 0; i < n; i++) {
+      if (dtype == DT_FLOAT32) {
+         const float a = ((const float *) in)[i];
+         out[i] = style ? q15_rne((double) (a * 32768.0f)) : q15_natc_f(a);
+      }
+      else {
+         const double a = ((const double *) in)[i];
+         out[i] = style ? q15_rne(a * 32768.0) : q15_natc_d(a);
+      }
+   }
+}
+
+void oracle_q15tofl(int dtype, const int16_t *in, void *out, long long n)
+{
+   for (long long i = 0; i < n; i++) {
+      if (dtype == DT_FLOAT32) ((float *) out)[i] = (float) in[i] / 32768.0f;
+      else ((double *) out)[i] = (double) in[i] / 32768.0;
+   }
+}

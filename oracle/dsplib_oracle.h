@@ -72,6 +72,20 @@ int oracle_tif_num_groups(int S);
  * The reciprocal is the correctly rounded 1/b0. */
 void oracle_tif_coefficients(const float *natural, int S, float *tifCoef, float *gains);
 
+/* ------------------------------------------------------------ Q.15 conversions */
+
+/* Float to Q.15, natural-C arithmetic of src/DSPLIB_fltoq15/DSPLIB_fltoq15_cn.cpp:35-62
+ * (style 0) or one round-half-to-even conversion with saturation, the reference
+ * C7x kernel's __float_to_int / __double_to_int + __int_to_short_sat
+ * (DSPLIB_fltoq15_ci.cpp; style 1).  dtype 12 = float input, 13 = double input.
+ * Where the reference C code converts a value outside the int32 range (undefined
+ * behaviour) this restatement saturates by sign and maps NaN to 0. */
+void oracle_fltoq15(int dtype, int style, const void *in, int16_t *out, long long n);
+
+/* Q.15 to float: out = in / 32768 (src/DSPLIB_q15tofl/DSPLIB_q15tofl_cn.cpp:33-37);
+ * dtype 12 = float output, 13 = double output. */
+void oracle_q15tofl(int dtype, const int16_t *in, void *out, long long n);
+
 #ifdef __cplusplus
 }
 #endif

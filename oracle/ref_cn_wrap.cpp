@@ -2,8 +2,8 @@
  * Thin C entry points around the reference's natural-C kernels.
  *
  * TEST INFRASTRUCTURE ONLY.  Compiled by oracle/Makefile together with the
- * reference's own DSPLIB_fir_cn.cpp and DSPLIB_cascadeBiquad_cn.cpp (taken
- * unmodified from the read-only reference checkout) into oracle/_ref/.
+ * reference's own DSPLIB_fir_cn.cpp, DSPLIB_cascadeBiquad_cn.cpp,
+ * DSPLIB_fltoq15_cn.cpp and DSPLIB_q15tofl_cn.cpp (taken unmodified from the read-only reference checkout) into oracle/_ref/.
  * Nothing in the product library links or loads this file; only tests/,
  * the smoke check and bench.py's CPU-baseline leg use it, as the checker.
  *
@@ -23,6 +23,8 @@
 
 #include "DSPLIB_fir_priv.h"
 #include "DSPLIB_cascadeBiquad_priv.h"
+#include "DSPLIB_fltoq15_priv.h"
+#include "DSPLIB_q15tofl_priv.h"
 
 namespace {
 
@@ -162,6 +164,34 @@ int ref_biquad_cn_mt(int form, const void *in, const void *coef, void *state, vo
       if (rc[t] != 0) r = rc[t];
    }
    return r;
+}
+
+
+/* Q.15 conversions: the reference init() stores dataSize as blockSize and
+ * picks the _cn template by the float type (DSPLIB_fltoq15.cpp:64-90,
+ * DSPLIB_q15tofl.cpp:64-90); the _cn code reads nothing else. */
+int ref_fltoq15_cn(int dtype, const void *in, void *out, int n)
+{
+   DSPLIB_fltoq15_PrivArgs priv;
+   std::memset(&priv, 0, sizeof(priv));
+   priv.blockSize = n;
+   if (dtype == DSPLIB_FLOAT32)
+      return (int) DSPLIB_fltoq15_exec_cn<float>((DSPLIB_kernelHandle) &priv, (void *) in, out);
+   if (dtype == DSPLIB_FLOAT64)
+      return (int) DSPLIB_fltoq15_exec_cn<double>((DSPLIB_kernelHandle) &priv, (void *) in, out);
+   return DSPLIB_ERR_INVALID_TYPE;
+}
+
+int ref_q15tofl_cn(int dtype, const void *in, void *out, int n)
+{
+   DSPLIB_q15tofl_PrivArgs priv;
+   std::memset(&priv, 0, sizeof(priv));
+   priv.blockSize = n;
+   if (dtype == DSPLIB_FLOAT32)
+      return (int) DSPLIB_q15tofl_exec_cn<float>((DSPLIB_kernelHandle) &priv, (void *) in, out);
+   if (dtype == DSPLIB_FLOAT64)
+      return (int) DSPLIB_q15tofl_exec_cn<double>((DSPLIB_kernelHandle) &priv, (void *) in, out);
+   return DSPLIB_ERR_INVALID_TYPE;
 }
 
 } /* extern "C" */

@@ -274,3 +274,42 @@ def test_reference_flow_golden(golden_biquad, key, style):
     elif form == D.TDF2:  # TDF2 states coincide with scipy's sosfilt zf
         zf = golden_biquad[key + "_zf64"].reshape(S * 2, C)
         assert np.max(np.abs(host(sd)[:, :C] - zf)) <= TOL_REF
+
+
+@pytest.mark.parametrize("C", [8, 64])
+def test_opt_blocks_replayed_from_cuda_graph(C):
+    """Block-by-block processing (the numExecReps pattern) captured once in a CUDA
+    graph: asynchronous exec calls on device buffers queue kernels only, so a
+    sequence of blocks replays as one graph and equals one call on the whole signal."""
+    rng = np.random.default_rng(40 + C)
+    N, blocks, S = 2048, 4, 4
+    x = rng.standard_normal((N * blocks, C)).astype(np.float32)
+    nat = stable_sections(rng, 1, S)
+    opt, _ = D.opt_coefficients(nat, D.DF2, 0, C)
+    xd, cd = dev(x), dev(opt)
+    yd = torch.zeros_like(xd)
+    sd = torch.zeros((2 * S, C), device="cuda")
+    args, pin, pout, pvar, pcn, popt = D.biquad_descs(C, N, S, D.DF2, 0)
+    h = D.BiquadHandle()
+    assert h.init(args, pin, popt, pvar, pout) == D.SUCCESS
+    h.set_async(True)
+    cs = torch.cuda.Stream()
+    h.set_stream(cs)
+    with torch.cuda.stream(cs):  # one eager pass sets up the launch attributes
+        for b in range(blocks):
+            assert h.exec(xd[b * N:(b + 1) * N], cd, sd, yd[b * N:(b + 1) * N]) == D.SUCCESS
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=cs):
+        for b in range(blocks):
+            assert h.exec(xd[b * N:(b + 1) * N], cd, sd, yd[b * N:(b + 1) * N]) == D.SUCCESS
+    sd.zero_()
+    yd.zero_()
+    torch.cuda.synchronize()
+    g.replay()
+    torch.cuda.synchronize()
+    st_whole = dev(np.zeros((2 * S, C), np.float32))
+    want = host(D.cascade_biquad(xd, cd, st_whole, form=D.DF2, nch=0))
+    scale = max(1.0, float(np.abs(want).max()))
+    assert np.max(np.abs(host(yd) - want)) <= 1e-4 * scale
+    assert np.max(np.abs(host(sd) - host(st_whole))) <= 1e-4 * max(1.0, float(np.abs(host(st_whole)).max()))

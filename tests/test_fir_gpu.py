@@ -283,3 +283,49 @@ def test_host_buffers_pipelined(dt, precision, qmode, B, N, T, pinned):
     else:
         got = D.fir(x, h, T, nch=1, precision=precision, qmode=qmode, shift=shift)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("dt,style,precision,qmode,C,T,N,blocks", [
+    (np.int16, D.NATC, D.FIR_SIMT, False, 5, 37, 100, 6),       # bit-exact natural C
+    (np.int8, D.OPTIMIZED, D.FIR_SIMT, True, 3, 64, 16, 9),     # block shorter than the history, tensor cores
+    (np.float32, D.OPTIMIZED, D.FIR_BF16X3, False, 4, 256, 4096, 3),
+])
+@pytest.mark.parametrize("on_device", [False, True])
+def test_fir_stream_matches_one_call(dt, style, precision, qmode, C, T, N, blocks, on_device):
+    """Streaming FIR: blocks filtered one call at a time equal one call over the
+    whole signal preceded by T - 1 zeros."""
+    rng = np.random.default_rng(C * T + N)
+    x = rand(dt, (C, N * blocks), rng)
+    h = rand(dt, (C, T), rng) if dt != np.float32 else (rng.standard_normal((C, T)) / T).astype(np.float32)
+    shift = 7 if qmode else 0
+    code = {np.int8: D.INT8, np.int16: D.INT16, np.float32: D.FLOAT32}[dt]
+    st = D.FirStream(code, C, N, T, nch=1, func_style=style, shift=shift, precision=precision, qmode=qmode)
+    padded = np.concatenate([np.zeros((C, T - 1), dt), x], axis=1)
+    if dt == np.float32:
+        want64 = oracle.fir_f64(padded, h, T, nch=1)
+    elif qmode:
+        want = oracle.fir_q(padded, h, T, shift, nch=1)
+    else:
+        want = oracle.fir(padded, h, T, nch=1)
+    hd = dev(h) if on_device else h
+    got = []
+    for b in range(blocks):
+        xb = np.ascontiguousarray(x[:, b * N:(b + 1) * N])
+        if on_device:
+            out = torch.zeros((C, N), dtype=dev(xb).dtype, device="cuda")
+            got.append(host(st.exec(dev(xb), hd, out)))
+        else:
+            out = np.zeros((C, N), dt)
+            got.append(st.exec(xb, hd, out))
+    got = np.concatenate(got, axis=1)
+    if dt == np.float32:
+        peak = np.abs(want64).max(axis=1, keepdims=True)
+        assert np.max(np.abs(got - want64) / peak) <= 1e-5
+    else:
+        assert np.array_equal(got, want)
+    # reset starts a new signal: the first block again
+    st.reset()
+    xb = np.ascontiguousarray(x[:, :N])
+    out = np.zeros((C, N), dt)
+    again = st.exec(xb, h, out)
+    assert np.array_equal(again, got[:, :N])
