@@ -397,6 +397,150 @@ class FilterBankWorkload(Workload):
                                      f"adjoint composed of the reference's FIR and biquad natural-C kernels"
 
 
+def stream_name(kind, n, channels, inputs):
+    return {"fltoq15": f"fltoq15_f32_{n >> 20}M", "q15tofl": f"q15tofl_f32_{n >> 20}M",
+            "interleave": f"interleave_{channels}ch_f32_{n >> 20}M",
+            "deinterleave": f"deinterleave_{channels}ch_f32_{n >> 20}M",
+            "addnch": f"addNCh_f32_{inputs}in_{channels}ch_{n >> 20}M"}[kind]
+
+
+def _ref_chunks(fn, n, threads):
+    """Run fn(lo, hi) over [0, n) split into `threads` contiguous ranges on host threads
+    (ctypes releases the GIL during the foreign call, so the ranges run in parallel)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    threads = max(1, min(threads, n))
+    bounds = [(n * k // threads, n * (k + 1) // threads) for k in range(threads)]
+    if threads == 1:
+        fn(0, n)
+        return
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda b: fn(*b), bounds))
+
+
+class StreamWorkload(Workload):
+    """The Q.15 conversions and layout kernels next to the filters (DSPLIB_fltoq15,
+    DSPLIB_q15tofl, DSPLIB_interleave, DSPLIB_deinterleave, DSPLIB_addNCh): one exec over
+    arrays far larger than L2 per step, metric = elements (output samples) per second."""
+
+    bound = "hbm"
+    metric = "Gsamples/s"
+
+    def __init__(self, kind, n, *, channels=2, inputs=12, seed=6):
+        import c7x_dsplib_b200 as D
+
+        self.D, self.kind, self.n = D, kind, n
+        rng = np.random.default_rng(seed)
+        self.C, self.L = channels, inputs
+        if kind == "fltoq15":
+            self.x = rng.uniform(-1, 1, n).astype(np.float32)
+            self.out_dtype, self.samples, self.alg_bytes = np.int16, n, 6 * n
+            self.kernel, self.dtype = "fltoq15_vec_kernel", "f32"
+        elif kind == "q15tofl":
+            self.x = rng.integers(-32768, 32767, n, endpoint=True).astype(np.int16)
+            self.out_dtype, self.samples, self.alg_bytes = np.float32, n, 6 * n
+            self.kernel, self.dtype = "q15tofl_vec_kernel", "i16"
+        elif kind in ("interleave", "deinterleave"):
+            # interleave: C channel rows of n samples -> n rows of C; deinterleave the reverse
+            self.x = rng.standard_normal(n * channels).astype(np.float32)
+            self.out_dtype, self.samples, self.alg_bytes = np.float32, n * channels, 8 * n * channels
+            self.W, self.H = (n, channels) if kind == "interleave" else (channels, n)
+            self.kernel, self.dtype = ("interleave_k_kernel" if kind == "interleave" else "deinterleave_k_kernel"), "f32"
+        else:  # addNCh: `inputs` stacked inputs of `channels` rows of n samples
+            self.x = rng.uniform(-10, 10, n * channels * inputs).astype(np.float32)
+            self.out_dtype, self.samples = np.float32, n * channels
+            self.alg_bytes = 4 * n * channels * (inputs + 1)
+            self.kernel, self.dtype = "addnch_kernel", "f32"
+        self.name = stream_name(kind, n, channels, inputs)
+
+    def config(self):
+        c = {"workload": self.name, "elements_out": self.samples, "funcStyle": "OPTIMIZED"}
+        if self.kind in ("interleave", "deinterleave", "addnch"):
+            c["channels"] = self.C
+        if self.kind == "addnch":
+            c["inputs"] = self.L
+        return c
+
+    def _call(self, x, y, h):
+        D = self.D
+        if self.kind == "fltoq15":
+            D.fltoq15(x, out=y, handle=h)
+        elif self.kind == "q15tofl":
+            D.q15tofl(x, np.float32, out=y, handle=h)
+        elif self.kind in ("interleave", "deinterleave"):
+            D.transpose(x, y, self.W, self.H, self.W * 4, self.H * 4, kind=self.kind, handle=h)
+        else:
+            D.add_nch(x, y, self.n, self.C, self.L, self.n, self.n * self.C, self.n, handle=h)
+
+    def _handle(self):
+        D = self.D
+        if self.kind == "fltoq15":
+            return D.Fltoq15Handle()
+        if self.kind == "q15tofl":
+            return D.Q15toflHandle()
+        return D.LayoutHandle({"interleave": "DSPLIB_interleave", "deinterleave": "DSPLIB_deinterleave",
+                               "addnch": "DSPLIB_addNCh"}[self.kind])
+
+    def setup_device(self, torch, func_style=None):
+        self.h = self._handle()
+        self.xd = torch.from_numpy(self.x).cuda()
+        self.yd = torch.zeros(self.samples, dtype=getattr(torch, np.dtype(self.out_dtype).name), device="cuda")
+        self.h.set_async(True)
+        self._call(self.xd, self.yd, self.h)
+
+    def step(self):
+        self._call(self.xd, self.yd, self.h)
+
+    def e2e_setup(self, torch):
+        self.hx = torch.from_numpy(self.x).pin_memory()
+        self.hy = torch.zeros(self.samples, dtype=self.yd.dtype).pin_memory()
+        self.h2d = self.x.nbytes
+        self.d2h = self.samples * np.dtype(self.out_dtype).itemsize
+        self.he = self._handle()
+
+    def e2e_step(self):
+        self._call(self.hx, self.hy, self.he)
+
+    def cpu_reference(self, threads, budget_s):
+        import ctypes
+
+        import oracle
+
+        R = oracle.ref()
+        m = min(self.n, 1 << 22)  # bounded sample: the first 4 Mi samples per channel
+        y = np.zeros(self.samples, self.out_dtype)
+        vp = ctypes.c_void_p
+        e = self.x.itemsize
+        if self.kind == "fltoq15":
+            fn = lambda lo, hi: R.ref_fltoq15_cn(12, vp(self.x.ctypes.data + lo * 4), vp(y.ctypes.data + lo * 2),
+                                                 hi - lo)
+            units, per = m, 1
+        elif self.kind == "q15tofl":
+            fn = lambda lo, hi: R.ref_q15tofl_cn(12, vp(self.x.ctypes.data + lo * 2), vp(y.ctypes.data + lo * 4),
+                                                 hi - lo)
+            units, per = m, 1
+        elif self.kind == "interleave":  # column ranges of the C x n matrix
+            fn = lambda lo, hi: R.ref_transpose_cn(12, vp(self.x.ctypes.data + lo * e), vp(y.ctypes.data + lo * e * self.C),
+                                                   hi - lo, self.C, self.n * e, self.C * e)
+            units, per = m, self.C
+        elif self.kind == "deinterleave":  # row ranges of the n x C matrix
+            fn = lambda lo, hi: R.ref_transpose_cn(12, vp(self.x.ctypes.data + lo * e * self.C), vp(y.ctypes.data + lo * e),
+                                                   self.C, hi - lo, self.C * e, self.n * e)
+            units, per = m, self.C
+        else:  # addNCh: one channel row per task
+            fn = lambda lo, hi: R.ref_addnch_cn(12, vp(self.x.ctypes.data + lo * self.n * e), vp(y.ctypes.data + lo * self.n * e),
+                                                m, hi - lo, self.L, self.n, self.n * self.C, self.n)
+            units, per = self.C, m
+        reps, t_total = 0, 0.0
+        while t_total < budget_s or reps < 1:
+            t0 = time.perf_counter()
+            _ref_chunks(fn, units, threads)
+            t_total += time.perf_counter() - t0
+            reps += 1
+        done = reps * units * per
+        return done / t_total / 1e9, f"{reps} passes over the first {m} samples per channel (of {self.n})"
+
+
 WORKLOADS = {
     "fir_biquad_bank_2048ch_ragged": lambda: FilterBankWorkload(),
     "fir_biquad_bank_256ch_ragged": lambda: FilterBankWorkload(C=256),
@@ -413,6 +557,9 @@ WORKLOADS = {
     "fir_int16_4096ch_16384_128taps": lambda: FirWorkload("fir_int16_4096ch_16384_128taps", np.int16, 4096, 16384,
                                                           128, nch=0, qmode=True, shift=15, seed=4),
 }
+for _k, _n, _c in (("fltoq15", 64 << 20, 2), ("q15tofl", 64 << 20, 2), ("interleave", 16 << 20, 2),
+                   ("deinterleave", 16 << 20, 2), ("addnch", 1 << 20, 16)):
+    WORKLOADS[stream_name(_k, _n, _c, 12)] = (lambda k=_k, n=_n, c=_c: StreamWorkload(k, n, channels=c))
 DEFAULT = "biquad_32x8192x4"
 
 

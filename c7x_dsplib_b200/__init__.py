@@ -68,6 +68,16 @@ class BufParams1D(ctypes.Structure):
     _fields_ = [("data_type", ctypes.c_uint32), ("dim_x", ctypes.c_uint32)]
 
 
+class BufParams3D(ctypes.Structure):
+    _fields_ = [("data_type", ctypes.c_uint32), ("dim_x", ctypes.c_uint32), ("dim_y", ctypes.c_uint32),
+                ("stride_y", ctypes.c_int32), ("dim_z", ctypes.c_uint32), ("stride_z", ctypes.c_int32)]
+
+
+class StyleInitArgs(ctypes.Structure):
+    """DSPLIB_interleaveInitArgs, DSPLIB_deinterleaveInitArgs, DSPLIB_addNCh_InitArgs."""
+    _fields_ = [("funcStyle", ctypes.c_int8)]
+
+
 class ConvertInitArgs(ctypes.Structure):
     """DSPLIB_fltoq15_InitArgs and DSPLIB_q15tofl_InitArgs (same layout)."""
     _fields_ = [("funcStyle", ctypes.c_int8), ("dataSize", ctypes.c_uint32)]
@@ -106,6 +116,24 @@ SIGNATURES = {
     "DSPLIB_q15tofl_init": (ctypes.c_int, [_VP, _P(BufParams1D), _P(BufParams1D), _P(ConvertInitArgs)]),
     "DSPLIB_q15tofl_exec_checkParams": (ctypes.c_int, [_VP, _VP, _VP]),
     "DSPLIB_q15tofl_exec": (ctypes.c_int, [_VP, _VP, _VP]),
+    "DSPLIB_interleave_getHandleSize": (ctypes.c_int32, [_P(StyleInitArgs)]),
+    "DSPLIB_interleave_init_checkParams": (ctypes.c_int, [_VP, _BP, _BP, _P(StyleInitArgs)]),
+    "DSPLIB_interleave_init": (ctypes.c_int, [_VP, _BP, _BP, _P(StyleInitArgs)]),
+    "DSPLIB_interleave_exec_checkParams": (ctypes.c_int, [_VP, _VP, _VP]),
+    "DSPLIB_interleave_exec": (ctypes.c_int, [_VP, _VP, _VP]),
+    "DSPLIB_interleave_perfEst": (None, [_VP, _P(ctypes.c_uint64), _P(ctypes.c_uint64)]),
+    "DSPLIB_deinterleave_getHandleSize": (ctypes.c_int32, [_P(StyleInitArgs)]),
+    "DSPLIB_deinterleave_init_checkParams": (ctypes.c_int, [_VP, _BP, _BP, _P(StyleInitArgs)]),
+    "DSPLIB_deinterleave_init": (ctypes.c_int, [_VP, _BP, _BP, _P(StyleInitArgs)]),
+    "DSPLIB_deinterleave_exec_checkParams": (ctypes.c_int, [_VP, _VP, _VP]),
+    "DSPLIB_deinterleave_exec": (ctypes.c_int, [_VP, _VP, _VP]),
+    "DSPLIB_deinterleave_perfEst": (None, [_VP, _P(ctypes.c_uint64), _P(ctypes.c_uint64), ctypes.c_uint64]),
+    "DSPLIB_addNCh_getHandleSize": (ctypes.c_int32, [_P(StyleInitArgs)]),
+    "DSPLIB_addNCh_init_checkParams": (ctypes.c_int, [_VP, _P(BufParams3D), _BP, _P(StyleInitArgs)]),
+    "DSPLIB_addNCh_init": (ctypes.c_int, [_VP, _P(BufParams3D), _BP, _P(StyleInitArgs)]),
+    "DSPLIB_addNCh_exec_checkParams": (ctypes.c_int, [_VP, _VP, _VP]),
+    "DSPLIB_addNCh_exec": (ctypes.c_int, [_VP, _VP, _VP]),
+    "DSPLIB_addNCh_perfEst": (None, [_VP, _P(ctypes.c_uint64), _P(ctypes.c_uint64), ctypes.c_uint32]),
     "DSPLIB_gpu_setStream": (ctypes.c_int, [_VP, _VP]),
     "DSPLIB_gpu_setAsync": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_lastError": (ctypes.c_char_p, [_VP]),
@@ -267,6 +295,62 @@ class Q15toflHandle(Fltoq15Handle):
 
     size_fn = "DSPLIB_q15tofl_getHandleSize"
     prefix = "DSPLIB_q15tofl"
+
+
+class LayoutHandle(_Handle):
+    """DSPLIB_interleave / DSPLIB_deinterleave / DSPLIB_addNCh handle (``prefix`` picks the kernel);
+    reference call sequence of test/DSPLIB_interleave/DSPLIB_interleave_d.c."""
+
+    def __init__(self, prefix="DSPLIB_interleave"):
+        self.prefix = prefix
+        self.size_fn = prefix + "_getHandleSize"
+        super().__init__()
+
+    def init(self, args, pin, pout) -> int:
+        return getattr(lib(), self.prefix + "_init")(self.h, ctypes.byref(pin), ctypes.byref(pout), ctypes.byref(args))
+
+    def init_check(self, args, pin, pout) -> int:
+        return getattr(lib(), self.prefix + "_init_checkParams")(self.h, ctypes.byref(pin), ctypes.byref(pout),
+                                                                 ctypes.byref(args))
+
+    def exec(self, x, y) -> int:
+        return getattr(lib(), self.prefix + "_exec")(self.h, _ptr(x), _ptr(y))
+
+
+_LAYOUT_CODES = {"int8": INT8, "uint8": UINT8, "int16": INT16, "uint16": UINT16, "int32": INT32, "uint32": UINT32,
+                 "int64": INT64, "uint64": UINT64, "float32": FLOAT32, "float64": FLOAT64}
+
+
+def _type_code(a):
+    return _LAYOUT_CODES[str(a.dtype).replace("torch.", "")]
+
+
+def transpose(x, out, W, H, stride_in, stride_out, *, kind="interleave", func_style=OPTIMIZED, handle=None):
+    """DSPLIB_interleave / DSPLIB_deinterleave on flat buffers (numpy or torch, host or device):
+    ``x`` holds H rows of W elements ``stride_in`` bytes apart, ``out`` receives W rows of H
+    elements ``stride_out`` bytes apart.  ``kind`` picks the entry points (same transpose)."""
+    prefix = "DSPLIB_" + kind
+    hd = handle or LayoutHandle(prefix)
+    code = _type_code(x)
+    args = StyleInitArgs(funcStyle=func_style)
+    pin, pout = bp(code, W, H, stride_in), bp(code, H, W, stride_out)
+    hd._check(prefix + "_init", hd.init(args, pin, pout))
+    hd._check(prefix + "_exec", hd.exec(x, out))
+    return out
+
+
+def add_nch(x, out, samples, channels, inputs, sY, sZ, sO, *, func_style=OPTIMIZED, handle=None):
+    """DSPLIB_addNCh on flat float32 / float64 buffers; strides in elements."""
+    hd = handle or LayoutHandle("DSPLIB_addNCh")
+    code = _type_code(x)
+    e = 4 if code == FLOAT32 else 8
+    args = StyleInitArgs(funcStyle=func_style)
+    pin = BufParams3D(code, samples, channels, sY * e, inputs, sZ * e)
+    pout = bp(code, samples, channels, sO * e)
+    hd._check("DSPLIB_addNCh_init_checkParams", hd.init_check(args, pin, pout))
+    hd._check("DSPLIB_addNCh_init", hd.init(args, pin, pout))
+    hd._check("DSPLIB_addNCh_exec", hd.exec(x, out))
+    return out
 
 
 def _float_code(a):

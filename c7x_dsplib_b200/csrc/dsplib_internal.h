@@ -16,6 +16,9 @@ constexpr uint32_t kMagicFir = 0xF1A0B200u;
 constexpr uint32_t kMagicBiquad = 0xB1A0B200u;
 constexpr uint32_t kMagicFltoq15 = 0xF15AB200u;
 constexpr uint32_t kMagicQ15tofl = 0x15F0B200u;
+constexpr uint32_t kMagicInterleave = 0x1E7EB200u;
+constexpr uint32_t kMagicDeinterleave = 0xDE1EB200u;
+constexpr uint32_t kMagicAddNCh = 0xADDCB200u;
 
 // First member of every handle: GPU settings that survive re-init
 // (the reference test drivers re-run init on the same handle to switch
@@ -60,6 +63,25 @@ struct Q15Priv {
    int32_t funcStyle;
    uint32_t dataSize; // elements per exec
    int32_t isDouble;  // float side is FLOAT64
+   int32_t initialized;
+};
+
+// DSPLIB_interleave / DSPLIB_deinterleave handle: the fields the reference keeps in
+// DSPLIB_matTrans_PrivArgs (widthIn, heightIn, strideIn, strideOut) plus the type.
+struct LayoutPriv {
+   HandleCommon common;
+   uint32_t widthIn, heightIn;
+   int32_t strideIn, strideOut; // bytes
+   int32_t dataType;
+   int32_t initialized;
+};
+
+// DSPLIB_addNCh handle: the fields of DSPLIB_addNCh_PrivArgs.
+struct AddNChPriv {
+   HandleCommon common;
+   uint32_t inputs, samples, channels;
+   int32_t strideInElementsY, strideInElementsZ, strideOutElements;
+   int32_t dataType;
    int32_t initialized;
 };
 
@@ -151,6 +173,29 @@ cudaError_t launchFir(const FirLaunch &a, FirKernelKind kind, cudaStream_t s);
 // vector kernels).  natc: the natural-C rounding steps, else round-half-to-even.
 cudaError_t launchFltoq15(const void *in, int16_t *out, long long n, bool isDouble, bool natc, cudaStream_t s);
 cudaError_t launchQ15tofl(const int16_t *in, void *out, long long n, bool isDouble, cudaStream_t s);
+
+// Strided transpose of DSPLIB_interleave / DSPLIB_deinterleave:
+// out[(i * sOutB) / elt + j] = in[i + sInE * j], i < W, j < H.
+struct TransposeLaunch {
+   const void *in;
+   void *out;
+   long long W, H;
+   long long sInE; // input row stride, elements
+   long long sOutB; // output row stride, bytes
+   int elt;         // 1, 2, 4 or 8
+};
+cudaError_t launchTranspose(const TransposeLaunch &a, cudaStream_t s);
+
+// DSPLIB_addNCh: out[row * sO + col] = sum over l of in[row * sY + col + l * sZ] (element strides).
+struct AddNChLaunch {
+   const void *in;
+   void *out;
+   long long samples, channels;
+   int inputs;
+   long long sY, sZ, sO;
+   bool isDouble;
+};
+cudaError_t launchAddNCh(const AddNChLaunch &a, cudaStream_t s);
 bool firIntTcSupported(const FirLaunch &a);
 bool firBf16x3Supported(const FirLaunch &a);
 cudaError_t launchFirIntTc(const FirLaunch &a, bool qmode, cudaStream_t s);

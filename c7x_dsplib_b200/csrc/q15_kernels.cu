@@ -2,10 +2,10 @@
 //
 // Both are pure streams: 6 bytes per element for FLOAT32 <-> Q.15 and 10 for
 // FLOAT64 <-> Q.15, so they are bound by memory bandwidth.  Each thread moves
-// eight elements per iteration with 16-byte vector accesses (the int16 side is
-// one 16-byte word), loads marked streaming (read once, not kept in L1) and
-// stores marked evict-first; the grid is a whole number of waves over the 148
-// SMs and strides over the array.  When a pointer is not 16-byte aligned the
+// 16-byte groups of the float side (and the matching 8 / 4 bytes of int16), warp
+// instructions cover contiguous spans, loads are marked streaming (read once, not
+// kept in L1) and stores evict-first; the grid is one wave over the 148 SMs and
+// strides over the array.  When a pointer is not 16-byte aligned the
 // scalar kernel runs instead (same arithmetic, coalesced 4/8-byte loads).
 //
 // The same kernels also run on mapped pinned host memory (the API's zero-copy
@@ -23,7 +23,6 @@ namespace dsplib {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kPerThread = 8;
 
 __device__ __forceinline__ int16_t sat16(int v) { return (int16_t) min(max(v, -32768), 32767); }
 
@@ -72,35 +71,68 @@ template <bool NATC, typename F> __device__ __forceinline__ int16_t toQ15(F a)
 __device__ __forceinline__ float fromQ15f(int16_t v) { return __fmul_rn((float) v, 3.0517578125e-05f); }
 __device__ __forceinline__ double fromQ15d(int16_t v) { return __dmul_rn((double) v, 3.0517578125e-05); }
 
-__device__ __forceinline__ void load8(const float *p, float (&v)[8])
-{
-   const float4 a = __ldcs((const float4 *) p), b = __ldcs((const float4 *) p + 1);
-   v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
-}
+// Vector kernels: one "group" is 16 bytes of the wide (float) side, G = 16 / sizeof(F)
+// elements, and 2G bytes of the narrow (int16) side.  Consecutive threads take
+// consecutive groups, so every load and store instruction of a warp covers one
+// contiguous span (512 bytes wide side, 128 or 256 bytes narrow side): full lines in
+// HBM and full-line PCIe transactions on mapped host memory.  kUnroll independent
+// groups per thread are loaded before any is converted.
+constexpr int kUnroll = 4;
 
-__device__ __forceinline__ void load8(const double *p, double (&v)[8])
+template <typename F> struct Wide;
+template <> struct Wide<float> { using T = float4; };
+template <> struct Wide<double> { using T = double2; };
+template <int G> struct Narrow;
+template <> struct Narrow<4> { using T = uint2; };
+template <> struct Narrow<2> { using T = unsigned int; };
+
+__device__ __forceinline__ void packQ15(uint2 &w, const int16_t (&q)[4])
 {
-#pragma unroll
-   for (int k = 0; k < 4; k++) {
-      const double2 a = __ldcs((const double2 *) p + k);
-      v[2 * k] = a.x;
-      v[2 * k + 1] = a.y;
-   }
+   w.x = (uint32_t) (uint16_t) q[0] | ((uint32_t) (uint16_t) q[1] << 16);
+   w.y = (uint32_t) (uint16_t) q[2] | ((uint32_t) (uint16_t) q[3] << 16);
+}
+__device__ __forceinline__ void packQ15(unsigned int &w, const int16_t (&q)[2])
+{
+   w = (uint32_t) (uint16_t) q[0] | ((uint32_t) (uint16_t) q[1] << 16);
+}
+__device__ __forceinline__ void unpackQ15(const uint2 &w, int16_t (&q)[4])
+{
+   q[0] = (int16_t) (w.x & 0xffffu), q[1] = (int16_t) (w.x >> 16);
+   q[2] = (int16_t) (w.y & 0xffffu), q[3] = (int16_t) (w.y >> 16);
+}
+__device__ __forceinline__ void unpackQ15(const unsigned int &w, int16_t (&q)[2])
+{
+   q[0] = (int16_t) (w & 0xffffu), q[1] = (int16_t) (w >> 16);
 }
 
 template <bool NATC, typename F>
 __global__ void __launch_bounds__(kThreads) fltoq15_vec_kernel(const F *__restrict__ in, int16_t *__restrict__ out,
                                                                long long groups)
 {
+   constexpr int G = 16 / (int) sizeof(F);
+   using W = typename Wide<F>::T;
+   using N = typename Narrow<G>::T;
    const long long stride = (long long) gridDim.x * kThreads;
-   for (long long g = (long long) blockIdx.x * kThreads + threadIdx.x; g < groups; g += stride) {
-      F v[8];
-      load8(in + g * kPerThread, v);
-      uint32_t w[4];
+   for (long long g0 = (long long) blockIdx.x * kThreads + threadIdx.x; g0 < groups; g0 += stride * kUnroll) {
+      W v[kUnroll];
 #pragma unroll
-      for (int k = 0; k < 4; k++)
-         w[k] = (uint32_t) (uint16_t) toQ15<NATC>(v[2 * k]) | ((uint32_t) (uint16_t) toQ15<NATC>(v[2 * k + 1]) << 16);
-      __stcs((int4 *) (out + g * kPerThread), make_int4((int) w[0], (int) w[1], (int) w[2], (int) w[3]));
+      for (int u = 0; u < kUnroll; u++) {
+         const long long g = g0 + u * stride;
+         if (g < groups) v[u] = __ldcs((const W *) in + g);
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; u++) {
+         const long long g = g0 + u * stride;
+         if (g < groups) {
+            const F *e = reinterpret_cast<const F *>(&v[u]);
+            int16_t q[G];
+#pragma unroll
+            for (int k = 0; k < G; k++) q[k] = toQ15<NATC>(e[k]);
+            N w;
+            packQ15(w, q);
+            __stcs((N *) out + g, w);
+         }
+      }
    }
 }
 
@@ -113,36 +145,34 @@ __global__ void __launch_bounds__(kThreads) fltoq15_scalar_kernel(const F *__res
       out[i] = toQ15<NATC>(__ldcs(in + i));
 }
 
-__global__ void __launch_bounds__(kThreads) q15tofl_vec_kernel(const int16_t *__restrict__ in, float *__restrict__ out,
+template <typename F>
+__global__ void __launch_bounds__(kThreads) q15tofl_vec_kernel(const int16_t *__restrict__ in, F *__restrict__ out,
                                                                long long groups)
 {
+   constexpr int G = 16 / (int) sizeof(F);
+   using W = typename Wide<F>::T;
+   using N = typename Narrow<G>::T;
    const long long stride = (long long) gridDim.x * kThreads;
-   for (long long g = (long long) blockIdx.x * kThreads + threadIdx.x; g < groups; g += stride) {
-      const int4 w = __ldcs((const int4 *) (in + g * kPerThread));
-      const uint32_t u[4] = {(uint32_t) w.x, (uint32_t) w.y, (uint32_t) w.z, (uint32_t) w.w};
-      float v[8];
+   for (long long g0 = (long long) blockIdx.x * kThreads + threadIdx.x; g0 < groups; g0 += stride * kUnroll) {
+      N w[kUnroll];
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-         v[2 * k] = fromQ15f((int16_t) (u[k] & 0xffffu));
-         v[2 * k + 1] = fromQ15f((int16_t) (u[k] >> 16));
+      for (int u = 0; u < kUnroll; u++) {
+         const long long g = g0 + u * stride;
+         if (g < groups) w[u] = __ldcs((const N *) in + g);
       }
-      float4 *o = (float4 *) (out + g * kPerThread);
-      __stcs(o, make_float4(v[0], v[1], v[2], v[3]));
-      __stcs(o + 1, make_float4(v[4], v[5], v[6], v[7]));
-   }
-}
-
-__global__ void __launch_bounds__(kThreads) q15tofl_vec_kernel(const int16_t *__restrict__ in,
-                                                               double *__restrict__ out, long long groups)
-{
-   const long long stride = (long long) gridDim.x * kThreads;
-   for (long long g = (long long) blockIdx.x * kThreads + threadIdx.x; g < groups; g += stride) {
-      const int4 w = __ldcs((const int4 *) (in + g * kPerThread));
-      const uint32_t u[4] = {(uint32_t) w.x, (uint32_t) w.y, (uint32_t) w.z, (uint32_t) w.w};
-      double2 *o = (double2 *) (out + g * kPerThread);
 #pragma unroll
-      for (int k = 0; k < 4; k++)
-         __stcs(o + k, make_double2(fromQ15d((int16_t) (u[k] & 0xffffu)), fromQ15d((int16_t) (u[k] >> 16))));
+      for (int u = 0; u < kUnroll; u++) {
+         const long long g = g0 + u * stride;
+         if (g < groups) {
+            int16_t q[G];
+            unpackQ15(w[u], q);
+            W v;
+            F *e = reinterpret_cast<F *>(&v);
+#pragma unroll
+            for (int k = 0; k < G; k++) e[k] = sizeof(F) == 4 ? (F) fromQ15f(q[k]) : (F) fromQ15d(q[k]);
+            __stcs((W *) out + g, v);
+         }
+      }
    }
 }
 
@@ -178,14 +208,15 @@ bool aligned16(const void *p) { return ((uintptr_t) p & 15u) == 0; }
 
 template <bool NATC, typename F> cudaError_t fltoq15Typed(const F *in, int16_t *out, long long n, cudaStream_t s)
 {
+   constexpr int G = 16 / (int) sizeof(F);
    long long done = 0;
    if (aligned16(in) && aligned16(out)) {
-      const long long groups = n / kPerThread;
+      const long long groups = n / G;
       if (groups > 0) {
-         fltoq15_vec_kernel<NATC, F><<<gridFor(groups), kThreads, 0, s>>>(in, out, groups);
+         fltoq15_vec_kernel<NATC, F><<<gridFor((groups + kUnroll - 1) / kUnroll), kThreads, 0, s>>>(in, out, groups);
          countLaunch();
       }
-      done = groups * kPerThread;
+      done = groups * G;
    }
    if (done < n) {
       fltoq15_scalar_kernel<NATC, F><<<gridFor(n - done), kThreads, 0, s>>>(in, out, done, n);
@@ -196,14 +227,15 @@ template <bool NATC, typename F> cudaError_t fltoq15Typed(const F *in, int16_t *
 
 template <typename F> cudaError_t q15toflTyped(const int16_t *in, F *out, long long n, cudaStream_t s)
 {
+   constexpr int G = 16 / (int) sizeof(F);
    long long done = 0;
    if (aligned16(in) && aligned16(out)) {
-      const long long groups = n / kPerThread;
+      const long long groups = n / G;
       if (groups > 0) {
-         q15tofl_vec_kernel<<<gridFor(groups), kThreads, 0, s>>>(in, out, groups);
+         q15tofl_vec_kernel<F><<<gridFor((groups + kUnroll - 1) / kUnroll), kThreads, 0, s>>>(in, out, groups);
          countLaunch();
       }
-      done = groups * kPerThread;
+      done = groups * G;
    }
    if (done < n) {
       q15tofl_scalar_kernel<F><<<gridFor(n - done), kThreads, 0, s>>>(in, out, done, n);

@@ -152,8 +152,16 @@ static HandleCommon *common(DSPLIB_kernelHandle h)
 {
    if (!h) return nullptr;
    HandleCommon *c = (HandleCommon *) h;
-   if (c->magic != kMagicFir && c->magic != kMagicBiquad && c->magic != kMagicFltoq15 && c->magic != kMagicQ15tofl)
-      return nullptr;
+   switch (c->magic) {
+   case kMagicFir:
+   case kMagicBiquad:
+   case kMagicFltoq15:
+   case kMagicQ15tofl:
+   case kMagicInterleave:
+   case kMagicDeinterleave:
+   case kMagicAddNCh: break;
+   default: return nullptr;
+   }
    return c;
 }
 

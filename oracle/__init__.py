@@ -5,7 +5,8 @@ Two checkers live here, both loaded through ctypes:
 * ``port``: this project's C restatement (``dsplib_oracle.c``), built into
   ``oracle/_build/liboracle_port.so`` by ``oracle/Makefile``.
 * ``ref``: the reference's own natural-C kernels (``DSPLIB_fir_cn.cpp``,
-  ``DSPLIB_cascadeBiquad_cn.cpp``, ``DSPLIB_fltoq15_cn.cpp``, ``DSPLIB_q15tofl_cn.cpp``)
+  ``DSPLIB_cascadeBiquad_cn.cpp``, ``DSPLIB_fltoq15_cn.cpp``, ``DSPLIB_q15tofl_cn.cpp``,
+  ``DSPLIB_matTrans_cn.cpp``, ``DSPLIB_addNCh_cn.cpp``)
   compiled unmodified, with the stand-in TI
   headers of ``oracle/shim``, into ``oracle/_ref/libdsplib_ref.so``.  Present
   whenever the library was built here (it travels with the repository
@@ -59,7 +60,7 @@ def port():
         _port = ctypes.CDLL(PORT_SO)
         for name in ("oracle_fir_cn", "oracle_fir_q", "oracle_fir_f64", "oracle_biquad_df",
                      "oracle_biquad_df_f64", "oracle_biquad_tif", "oracle_tif_coefficients", "oracle_fltoq15",
-                     "oracle_q15tofl"):
+                     "oracle_q15tofl", "oracle_transpose", "oracle_addnch"):
             getattr(_port, name).restype = None
     return _port
 
@@ -235,4 +236,41 @@ def q15tofl(x, dtype=np.float32, *, impl="port"):
             raise RuntimeError(f"ref_q15tofl_cn: {rc}")
     else:
         port().oracle_q15tofl(dt, _ptr(x), _ptr(out), ctypes.c_longlong(x.size))
+    return out
+
+
+# ------------------------------------------------------------------ layout kernels
+
+_LAYOUT_DT = {np.dtype(np.int8): 0, np.dtype(np.int16): 1, np.dtype(np.int32): 2, np.dtype(np.int64): 3,
+              np.dtype(np.uint8): 5, np.dtype(np.uint16): 6, np.dtype(np.uint32): 8, np.dtype(np.uint64): 9,
+              np.dtype(np.float32): 12, np.dtype(np.float64): 13}
+
+
+def transpose(x, W, H, stride_in, stride_out, out, *, impl="port"):
+    """The interleave / deinterleave transpose (DSPLIB_matTrans_cn.cpp:41-45) on flat
+    buffers: ``x`` holds H rows of W elements ``stride_in`` bytes apart; ``out`` (updated in
+    place, other bytes untouched) receives W rows of H elements at ``(i*stride_out)/size``."""
+    x = np.ascontiguousarray(x)
+    assert out.dtype == x.dtype and out.flags.c_contiguous
+    if impl == "ref":
+        rc = ref().ref_transpose_cn(_LAYOUT_DT[x.dtype], _ptr(x), _ptr(out), W, H, stride_in, stride_out)
+        if rc != 0:
+            raise RuntimeError(f"ref_transpose_cn: {rc}")
+    else:
+        port().oracle_transpose(x.itemsize, _ptr(x), _ptr(out), ctypes.c_longlong(W), ctypes.c_longlong(H),
+                                ctypes.c_longlong(stride_in), ctypes.c_longlong(stride_out))
+    return out
+
+
+def addnch(x, samples, channels, inputs, sY, sZ, sO, out, *, impl="port"):
+    """DSPLIB_addNCh on flat buffers (strides in elements); ``out`` updated in place."""
+    x = np.ascontiguousarray(x)
+    dt = _FT[x.dtype]
+    if impl == "ref":
+        rc = ref().ref_addnch_cn(dt, _ptr(x), _ptr(out), samples, channels, inputs, sY, sZ, sO)
+        if rc != 0:
+            raise RuntimeError(f"ref_addnch_cn: {rc}")
+    else:
+        L = ctypes.c_longlong
+        port().oracle_addnch(dt, _ptr(x), _ptr(out), L(samples), L(channels), L(inputs), L(sY), L(sZ), L(sO))
     return out

@@ -351,3 +351,36 @@ void oracle_q15tofl(int dtype, const int16_t *in, void *out, long long n)
       else ((double *) out)[i] = (double) in[i] / 32768.0;
    }
 }
+
+/* ---------------------------------------------------------------- layout kernels */
+
+void oracle_transpose(int elt, const void *in, void *out, long long W, long long H, long long strideIn,
+                      long long strideOut)
+{
+   const unsigned char *src = (const unsigned char *) in;
+   unsigned char *dst = (unsigned char *) out;
+   const long long sInE = strideIn / elt;
+   for (long long i = 0; i < W; i++)
+      for (long long j = 0; j < H; j++)
+         memcpy(dst + ((i * strideOut) / elt + j) * elt, src + (i + sInE * j) * elt, (size_t) elt);
+}
+
+void oracle_addnch(int dtype, const void *in, void *out, long long samples, long long channels, long long inputs,
+                   long long sY, long long sZ, long long sO)
+{
+   for (long long row = 0; row < channels; row++)
+      for (long long col = 0; col < samples; col++) {
+         if (dtype == DT_FLOAT32) {
+            const float *x = (const float *) in;
+            float acc = 0.0f;
+            for (long long l = 0; l < inputs; l++) acc = acc + x[row * sY + col + sZ * l];
+            ((float *) out)[row * sO + col] = acc;
+         }
+         else {
+            const double *x = (const double *) in;
+            double acc = 0.0;
+            for (long long l = 0; l < inputs; l++) acc = acc + x[row * sY + col + sZ * l];
+            ((double *) out)[row * sO + col] = acc;
+         }
+      }
+}

@@ -86,6 +86,20 @@ void oracle_fltoq15(int dtype, int style, const void *in, int16_t *out, long lon
  * dtype 12 = float output, 13 = double output. */
 void oracle_q15tofl(int dtype, const int16_t *in, void *out, long long n);
 
+/* ------------------------------------------------------------ layout kernels */
+
+/* Strided matrix transpose of DSPLIB_interleave / DSPLIB_deinterleave
+ * (src/DSPLIB_matTrans/DSPLIB_matTrans_cn.cpp:41-45): for i < W, j < H
+ *   out[(i * strideOut) / elt + j] = in[i + (strideIn / elt) * j]   (strides in bytes). */
+void oracle_transpose(int elt, const void *in, void *out, long long W, long long H, long long strideIn,
+                      long long strideOut);
+
+/* DSPLIB_addNCh (src/DSPLIB_addNCh/DSPLIB_addNCh_cn.cpp:30-39): out[row*sO + col] is the sum over
+ * the inputs in order, starting from zero, in the data type (dtype 12 float, 13 double);
+ * strides in elements. */
+void oracle_addnch(int dtype, const void *in, void *out, long long samples, long long channels, long long inputs,
+                   long long sY, long long sZ, long long sO);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,7 +3,8 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Compiled by oracle/Makefile together with the
  * reference's own DSPLIB_fir_cn.cpp, DSPLIB_cascadeBiquad_cn.cpp,
- * DSPLIB_fltoq15_cn.cpp and DSPLIB_q15tofl_cn.cpp (taken unmodified from the read-only reference checkout) into oracle/_ref/.
+ * DSPLIB_fltoq15_cn.cpp, DSPLIB_q15tofl_cn.cpp, DSPLIB_matTrans_cn.cpp and
+ * DSPLIB_addNCh_cn.cpp (taken unmodified from the read-only reference checkout) into oracle/_ref/.
  * Nothing in the product library links or loads this file; only tests/,
  * the smoke check and bench.py's CPU-baseline leg use it, as the checker.
  *
@@ -25,6 +26,8 @@
 #include "DSPLIB_cascadeBiquad_priv.h"
 #include "DSPLIB_fltoq15_priv.h"
 #include "DSPLIB_q15tofl_priv.h"
+#include "DSPLIB_matTrans_priv.h"
+#include "DSPLIB_addNCh_priv.h"
 
 namespace {
 
@@ -191,6 +194,52 @@ int ref_q15tofl_cn(int dtype, const void *in, void *out, int n)
       return (int) DSPLIB_q15tofl_exec_cn<float>((DSPLIB_kernelHandle) &priv, (void *) in, out);
    if (dtype == DSPLIB_FLOAT64)
       return (int) DSPLIB_q15tofl_exec_cn<double>((DSPLIB_kernelHandle) &priv, (void *) in, out);
+   return DSPLIB_ERR_INVALID_TYPE;
+}
+
+/* Interleave / deinterleave: the reference init() records widthIn, heightIn and the
+ * two byte strides in DSPLIB_matTrans_PrivArgs and selects DSPLIB_matTrans_exec_cn
+ * by type (DSPLIB_interleave.cpp:89-253, DSPLIB_deinterleave.cpp:89-251). */
+int ref_transpose_cn(int dtype, const void *in, void *out, int W, int H, int strideIn, int strideOut)
+{
+   DSPLIB_matTrans_PrivArgs priv;
+   std::memset(&priv, 0, sizeof(priv));
+   priv.widthIn = (uint32_t) W;
+   priv.heightIn = (uint32_t) H;
+   priv.strideIn = strideIn;
+   priv.strideOut = strideOut;
+   DSPLIB_kernelHandle h = (DSPLIB_kernelHandle) &priv;
+   void *i = (void *) in;
+   switch (dtype) {
+   case DSPLIB_INT8: return (int) DSPLIB_matTrans_exec_cn<int8_t>(h, i, out);
+   case DSPLIB_UINT8: return (int) DSPLIB_matTrans_exec_cn<uint8_t>(h, i, out);
+   case DSPLIB_INT16: return (int) DSPLIB_matTrans_exec_cn<int16_t>(h, i, out);
+   case DSPLIB_UINT16: return (int) DSPLIB_matTrans_exec_cn<uint16_t>(h, i, out);
+   case DSPLIB_INT32: return (int) DSPLIB_matTrans_exec_cn<int32_t>(h, i, out);
+   case DSPLIB_UINT32: return (int) DSPLIB_matTrans_exec_cn<uint32_t>(h, i, out);
+   case DSPLIB_FLOAT32: return (int) DSPLIB_matTrans_exec_cn<float>(h, i, out);
+   case DSPLIB_INT64: return (int) DSPLIB_matTrans_exec_cn<int64_t>(h, i, out);
+   case DSPLIB_UINT64: return (int) DSPLIB_matTrans_exec_cn<uint64_t>(h, i, out);
+   case DSPLIB_FLOAT64: return (int) DSPLIB_matTrans_exec_cn<double>(h, i, out);
+   default: return DSPLIB_ERR_INVALID_TYPE;
+   }
+}
+
+/* addNCh: the fields DSPLIB_addNCh.cpp:67-72 fills (strides in elements). */
+int ref_addnch_cn(int dtype, const void *in, void *out, int samples, int channels, int inputs, int sY, int sZ,
+                  int sO)
+{
+   DSPLIB_addNCh_PrivArgs priv;
+   std::memset(&priv, 0, sizeof(priv));
+   priv.samples = (uint32_t) samples;
+   priv.channels = (uint32_t) channels;
+   priv.inputs = (uint32_t) inputs;
+   priv.strideInElementsY = sY;
+   priv.strideInElementsZ = sZ;
+   priv.strideOutElements = sO;
+   DSPLIB_kernelHandle h = (DSPLIB_kernelHandle) &priv;
+   if (dtype == DSPLIB_FLOAT32) return (int) DSPLIB_addNCh_exec_cn<float>(h, (void *) in, out);
+   if (dtype == DSPLIB_FLOAT64) return (int) DSPLIB_addNCh_exec_cn<double>(h, (void *) in, out);
    return DSPLIB_ERR_INVALID_TYPE;
 }
 

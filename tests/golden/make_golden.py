@@ -7,6 +7,9 @@ Outputs (committed; the GPU box never needs the reference tree):
   fir_golden.npz     FIR cases drawn from test/DSPLIB_idat_gen/DSPLIB_fir/test_cases_list.csv
   biquad_golden.npz  cascade-biquad cases drawn from
                      test/DSPLIB_idat_gen/DSPLIB_cascadeBiquad/test_cases_list.csv
+  layout_golden.npz  interleave / deinterleave / addNCh cases drawn from
+                     test/DSPLIB_idat_gen/DSPLIB_{interleave,deinterleave,addNCh}/test_cases_list.csv
+                     (``--what layout`` writes only this file)
 
 FIR goldens follow the reference generator step for step
 (test/DSPLIB_idat_gen/DSPLIB_fir/gen_data.py:218-311): uniform data, taps
@@ -135,12 +138,87 @@ def biquad_cases(ref):
     return out
 
 
+LAYOUT_DT = {"int8_t": np.int8, "uint8_t": np.uint8, "int16_t": np.int16, "uint16_t": np.uint16,
+             "int32_t": np.int32, "uint32_t": np.uint32, "int64_t": np.int64, "uint64_t": np.uint64,
+             "float": np.float32, "double": np.float64}
+
+
+def calc_stride(nbytes):
+    """DSPLIB_CALC_STRIDE(bytes, DSPLIB_ALIGN_SHIFT_64BYTES) (src/common/DSPLIB_types.h:316)."""
+    return ((nbytes - 1) >> 6) + 1 << 6
+
+
+def _layout_input(rng, dt, count):
+    if np.dtype(dt).kind == "f":
+        return rng.uniform(-1, 1, count).astype(dt)
+    info = np.iinfo(dt)
+    return rng.integers(info.min, info.max, count, dtype=dt, endpoint=True)
+
+
+def layout_cases(ref, max_elems=4096, max_sum_elems=16000):
+    """Transposes (interleave, deinterleave) and channel sums (addNCh) at the shapes of the
+    reference's test tables, outputs from the reference natural-C kernels (oracle/_ref).
+    Strides are the drivers' DSPLIB_CALC_STRIDE(stride * size, 64-byte) bytes
+    (DSPLIB_interleave_d.c:98-106, DSPLIB_deinterleave_d.c:99-107); addNCh follows
+    DSPLIB_addNCh_d.c:93-103 and its generator (DSPLIB_idat_gen/DSPLIB_addNCh/gen_data.py:
+    uniform(-10, 10) inputs, golden = float64 sum over the inputs)."""
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    import oracle
+
+    out = {}
+    for kind in ("interleave", "deinterleave"):
+        path = os.path.join(ref, f"test/DSPLIB_idat_gen/DSPLIB_{kind}/test_cases_list.csv")
+        for r in csv.DictReader(open(path, encoding="utf-8-sig")):
+            cid, dt = int(r["ID"]), LAYOUT_DT[r["dType"]]
+            W, H = int(r["widthIn"]), int(r["heightIn"])
+            if W * H > max_elems:
+                continue
+            e = np.dtype(dt).itemsize
+            s_in, s_out = calc_stride(int(r["strideIn"]) * e), calc_stride(int(r["strideOut"]) * e)
+            s_in, s_out = max(s_in, calc_stride(W * e)), max(s_out, calc_stride(H * e))
+            if H * s_in > (16 << 10) or W * s_out > (16 << 10):
+                continue
+            rng = np.random.default_rng(cid + (0 if kind == "interleave" else 1000))
+            x = _layout_input(rng, dt, H * s_in // e)
+            y = np.zeros(((W - 1) * s_out) // e + H, dt)
+            oracle.transpose(x, W, H, s_in, s_out, y, impl="ref")
+            key = f"{kind[0]}{cid}"
+            out[key + "_meta"] = np.array([cid, W, H, s_in, s_out], dtype=np.int64)
+            out[key + "_x"] = x
+            out[key + "_y"] = y
+    path = os.path.join(ref, "test/DSPLIB_idat_gen/DSPLIB_addNCh/test_cases_list.csv")
+    for r in csv.DictReader(open(path, encoding="utf-8-sig")):
+        cid, dt = int(r["ID"]), LAYOUT_DT[r["dType"]]
+        L, C, S = int(r["inInputs"]), int(r["inChannels"]), int(r["inSamples"])
+        e = np.dtype(dt).itemsize
+        sY = calc_stride(int(r["strideInElements"]) * e) // e
+        sZ = sY * C
+        if L * sZ > max_sum_elems:
+            continue
+        np.random.seed(cid)
+        x64 = np.random.uniform(low=-10, high=10, size=(L, C, S))
+        x = np.zeros((L, C, sY), dt)
+        x[:, :, :S] = x64.astype(dt)
+        golden = np.sum(x64, axis=0).astype(dt)  # the generator's static reference
+        y = np.zeros(C * sY, dt)
+        oracle.addnch(x.reshape(-1), S, C, L, sY, sZ, sY, y, impl="ref")
+        key = f"a{cid}"
+        out[key + "_meta"] = np.array([cid, S, C, L, sY, sZ, sY], dtype=np.int64)
+        out[key + "_x"] = x.reshape(-1)
+        out[key + "_y"] = y
+        out[key + "_golden"] = golden
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--what", default="all", choices=["all", "layout"])
     a = ap.parse_args()
-    np.savez_compressed(os.path.join(HERE, "fir_golden.npz"), **fir_cases(a.ref))
-    np.savez_compressed(os.path.join(HERE, "biquad_golden.npz"), **biquad_cases(a.ref))
+    if a.what == "all":
+        np.savez_compressed(os.path.join(HERE, "fir_golden.npz"), **fir_cases(a.ref))
+        np.savez_compressed(os.path.join(HERE, "biquad_golden.npz"), **biquad_cases(a.ref))
+    np.savez_compressed(os.path.join(HERE, "layout_golden.npz"), **layout_cases(a.ref))
 
 
 if __name__ == "__main__":
