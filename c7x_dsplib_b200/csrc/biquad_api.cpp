@@ -302,6 +302,15 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_exec(DSPLIB_kernelHandle handle,
    cudaStream_t s = hc->stream;
    Region rin{pIn, nullptr, (size_t) C * 4, (size_t) N, (size_t) p->inPitch * 4, false};
    Region rout{pOut, nullptr, (size_t) C * 4, (size_t) N, (size_t) p->outPitch * 4, false};
+   // Page-locked signal buffers are read and written in place by the lane-per-channel scan
+   // kernel, which reads each input sample once and writes each output sample once, one
+   // coalesced row of 32 channels or more at a time; the sequential kernel (NATC, deep
+   // cascades) revisits the output once per stage and narrower rows are scattered, so those
+   // are staged.
+   if (!natc && S <= biquadScanMaxStages() && C >= 32 && pOut != pIn) {
+      rin.zeroCopy = rin.streamed = true;
+      rout.zeroCopy = rout.streamed = true;
+   }
    // states and coefficients are read (states also written) about once per channel and stage
    Region rst{pFilterVar, nullptr, (size_t) C * 4, (size_t) S * nv, (size_t) p->varPitch * 4, false, true};
    Region rc{pFilterCoeff, nullptr, cw, ch, cp, false, true};
@@ -335,7 +344,7 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_exec(DSPLIB_kernelHandle handle,
    if (e != cudaSuccess) return cudaFail(hc, e, "biquad kernel launch");
    if ((e = regionOut(rout, s)) != cudaSuccess) return cudaFail(hc, e, "copy output");
    if ((e = regionOut(rst, s)) != cudaSuccess) return cudaFail(hc, e, "copy state");
-   if (!hc->async || rin.staged || rout.staged || rst.staged || rc.staged) {
+   if (!hc->async || rin.onHost || rout.onHost || rst.onHost || rc.onHost) {
       if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, "biquad execution");
    }
    return DSPLIB_SUCCESS;

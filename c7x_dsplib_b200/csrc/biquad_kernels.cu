@@ -859,11 +859,11 @@ cudaError_t launchBiquadSequential(const BiquadLaunch &a, cudaStream_t s)
 // Deepest cascade whose coefficient and carry tables fit the scan kernel's
 // shared memory budget (36 B per stage and channel); deeper cascades use
 // the sequential kernel.
-static int scanMaxStages() { return 160; }
+int biquadScanMaxStages() { return 160; }
 
 cudaError_t launchBiquadScan(const BiquadLaunch &a, cudaStream_t s)
 {
-   if (a.S > scanMaxStages()) return launchBiquadSequential(a, s);
+   if (a.S > biquadScanMaxStages()) return launchBiquadSequential(a, s);
    switch (a.form) {
    case DSPLIB_BIQUAD_DF1: return launchScanForm<DSPLIB_BIQUAD_DF1>(a, s);
    case DSPLIB_BIQUAD_DF2: return launchScanForm<DSPLIB_BIQUAD_DF2>(a, s);

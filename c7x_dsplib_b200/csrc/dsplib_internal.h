@@ -107,11 +107,14 @@ struct Region {
    size_t pitch;      // bytes between rows
    bool staged;       // host buffer copied through a staging buffer
    bool zeroCopy;     // the kernel touches each element about once: a small pinned buffer may be used in place
+   bool streamed = false; // ... and in whole coalesced rows: a pinned buffer of any size may be used in place
+   bool onHost = false;   // set by regionIn: the caller's buffer is host memory (staged or mapped)
    size_t bytes() const { return height ? (height - 1) * pitch + width : 0; }
 };
 
 // Prepare a region: device pointers, and (zeroCopy regions) pinned host buffers
-// of at most kZeroCopyMaxBytes, are used in place; other host pointers are
+// of at most kZeroCopyMaxBytes (of any size for streamed regions), are used in
+// place through their mapped addresses; other host pointers are
 // staged (copied in when copyIn).  Returns cudaSuccess or the failure.
 constexpr size_t kZeroCopyMaxBytes = 64 * 1024;
 cudaError_t regionIn(Region &r, int slot, bool copyIn, cudaStream_t s);
@@ -235,6 +238,8 @@ struct BiquadLaunch {
 // NATC: sequential recursion per channel, bit-exact to the reference _cn kernels.
 cudaError_t launchBiquadSequential(const BiquadLaunch &a, cudaStream_t s);
 // OPTIMIZED: chunked parallel-in-time scan.
+// Stages up to which launchBiquadScan runs the scan kernels (beyond: the sequential kernel).
+int biquadScanMaxStages();
 cudaError_t launchBiquadScan(const BiquadLaunch &a, cudaStream_t s);
 
 } // namespace dsplib

@@ -87,12 +87,17 @@ void *stagingBuffer(int slot, size_t bytes)
 cudaError_t regionIn(Region &r, int slot, bool copyIn, cudaStream_t s)
 {
    r.staged = false;
+   r.onHost = false;
    r.dev = r.host;
    if (r.height == 0 || r.width == 0) return cudaSuccess;
    if (isDevicePtr(r.host)) return cudaSuccess;
+   r.onHost = true;
    // Small pinned buffers (coefficients, states, taps) are read and written in place by
-   // the kernels: a staging copy each way would cost more than the few accesses.
-   if (r.zeroCopy && r.bytes() <= kZeroCopyMaxBytes) {
+   // the kernels: a staging copy each way would cost more than the few accesses.  So are
+   // pinned buffers of any size that a kernel streams through once in whole rows: its
+   // loads and stores cross PCIe as the copy engines' would, in both directions at once,
+   // and overlap the kernel's own work.
+   if (r.zeroCopy && (r.streamed || r.bytes() <= kZeroCopyMaxBytes)) {
       if (void *d = pinnedDevicePtr(r.host)) {
          r.dev = d;
          return cudaSuccess;
