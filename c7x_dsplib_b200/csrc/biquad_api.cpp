@@ -340,6 +340,7 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_exec(DSPLIB_kernelHandle handle,
    a.outPitch = p->outPitch;
    a.varPitch = p->varPitch;
    a.coefPitch = coefPitch;
+   a.prefetch = (!rin.onHost || rin.staged) ? 1 : 0; // not for mapped host memory
    e = natc ? launchBiquadSequential(a, s) : launchBiquadScan(a, s);
    if (e != cudaSuccess) return cudaFail(hc, e, "biquad kernel launch");
    if ((e = regionOut(rout, s)) != cudaSuccess) return cudaFail(hc, e, "copy output");

@@ -269,6 +269,19 @@ constexpr int kPowTableBytes = 64 * 1024;
 
 __host__ __device__ constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x / 2); }
 
+// FP32 2x2 matrices and affine maps of the lane scan kernel.  Its matrix powers are
+// formed in FP64 and rounded once; the scans themselves run in FP32: chunk transitions
+// of stable sections contract, so their rounding stays at the level of the sequential
+// FP32 recursion while the dependent chains are several times shorter than in FP64.
+struct M2f {
+   float a, b, c, d;
+};
+
+__device__ __forceinline__ float2 affinef(const M2f &m, float2 v, float2 e)
+{
+   return make_float2(fmaf(m.a, v.x, fmaf(m.b, v.y, e.x)), fmaf(m.c, v.x, fmaf(m.d, v.y, e.y)));
+}
+
 // Matrix powers kept per stage and channel: M^(2^k), M = A^L, for
 // k = 0 .. log2(W) + 4 (the last five cover the CTA span A^(W*L) and its
 // powers up to 16 CTAs).
@@ -279,7 +292,7 @@ template <int W> struct ScanShape {
 };
 
 struct ScanSmem {
-   size_t E, P, Agg, Win, Pow, Cf, total;
+   size_t E, P, Agg, Win, Pow, Cf, Next, total;
    bool powTable;
 };
 
@@ -288,21 +301,37 @@ template <int W> __host__ __device__ inline ScanSmem scanLayout(int S)
    ScanSmem o;
    size_t off = 0;
    o.E = off;
-   off += (size_t) W * kPad * sizeof(double2);
+   off += (size_t) W * kPad * sizeof(float2);
    o.P = off;
-   off += (size_t) W * kPad * sizeof(double2);
+   off += (size_t) W * kPad * sizeof(float2);
    o.Agg = off;
-   off += (size_t) 2 * 32 * sizeof(double2);
+   off += (size_t) 2 * 32 * sizeof(float2);
    o.Win = off;
-   off += (size_t) S * 32 * sizeof(double2);
-   const size_t pow = (size_t) S * 32 * ScanShape<W>::NP * sizeof(M2);
+   off += (size_t) S * 32 * sizeof(float2);
+   const size_t pow = (size_t) S * 32 * ScanShape<W>::NP * sizeof(M2f);
    o.powTable = pow <= (size_t) kPowTableBytes;
    o.Pow = off; // all stages' powers, or one stage's (recomputed per stage) when that is too large
-   off += o.powTable ? pow : (size_t) 32 * ScanShape<W>::NP * sizeof(M2);
+   off += o.powTable ? pow : (size_t) 32 * ScanShape<W>::NP * sizeof(M2f);
    o.Cf = off;
    off += (size_t) S * 32 * 5 * sizeof(float);
-   o.total = off;
+   o.Next = (off + 15) / 16 * 16; // next window's input, fetched during this one (prefetch launches)
+   o.total = o.Next;
    return o;
+}
+
+// Shared memory of a scan launch: the tables, plus the next-window buffer when the
+// input is device memory and spans more than one window.
+template <int W> inline size_t scanSmemBytes(const BiquadLaunch &a, int K)
+{
+   const ScanSmem lay = scanLayout<W>(a.S);
+   const bool next = a.prefetch && (long long) a.N > (long long) K * W * kScanL;
+   return lay.total + (next ? (size_t) kScanL * W * 32 * sizeof(float) : 0);
+}
+
+__device__ __forceinline__ void cpAsync4(float *dst, const float *src)
+{
+   const unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
 }
 
 // Writes M^(2^k), k = 0 .. NP-1, of M = A^L to out[] (two matrices live at a time).
@@ -344,6 +373,40 @@ __device__ __forceinline__ double2 powApply(const M2 *P, int n, int nb, double2 
    return v;
 }
 
+template <int FORM, int W> __device__ __forceinline__ void stagePowersF(const Coef &c, M2f *out)
+{
+   M2 P = transition<FORM>(c);
+#pragma unroll
+   for (int r = 1; r < kScanL; r <<= 1) P = mmul(P, P);
+   out[0] = {(float) P.a, (float) P.b, (float) P.c, (float) P.d};
+#pragma unroll
+   for (int k = 1; k < ScanShape<W>::NP; k++) {
+      P = mmul(P, P);
+      out[k] = {(float) P.a, (float) P.b, (float) P.c, (float) P.d};
+   }
+}
+
+template <int W> __device__ __forceinline__ float2 segmentScanF(float2 val, int j, const M2f *P, int count)
+{
+#pragma unroll
+   for (int k = 0; (1 << k) < W; k++) {
+      float2 o;
+      o.x = __shfl_up_sync(0xffffffffu, val.x, 1 << k, W);
+      o.y = __shfl_up_sync(0xffffffffu, val.y, 1 << k, W);
+      if ((1 << k) < count && j >= (1 << k)) val = affinef(P[k], o, val);
+   }
+   return val;
+}
+
+__device__ __forceinline__ float2 powApplyF(const M2f *P, int n, int nb, float2 v)
+{
+   const float2 z = make_float2(0.0f, 0.0f);
+#pragma unroll
+   for (int k = 0; k < 5; k++)
+      if (k < nb && ((n >> k) & 1)) v = affinef(P[k], v, z);
+   return v;
+}
+
 template <int FORM, int W, bool CLUSTER>
 __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunch a)
 {
@@ -354,12 +417,13 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
    constexpr int CPW = ScanShape<W>::CPW;
    extern __shared__ __align__(16) unsigned char smem[];
    const ScanSmem lay = scanLayout<W>(a.S);
-   double2 *sE = (double2 *) (smem + lay.E);
-   double2 *sP = (double2 *) (smem + lay.P);
-   double2 *sAgg = (double2 *) (smem + lay.Agg);
-   double2 *sWin = (double2 *) (smem + lay.Win);
-   M2 *sPow = (M2 *) (smem + lay.Pow);
+   float2 *sE = (float2 *) (smem + lay.E);
+   float2 *sP = (float2 *) (smem + lay.P);
+   float2 *sAgg = (float2 *) (smem + lay.Agg);
+   float2 *sWin = (float2 *) (smem + lay.Win);
+   M2f *sPow = (M2f *) (smem + lay.Pow);
    float *sCf = (float *) (smem + lay.Cf);
+   float *sNext = (float *) (smem + lay.Next);
 
    const int lane = threadIdx.x & 31;
    const int w = threadIdx.x >> 5;
@@ -400,8 +464,8 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
       else
          for (int k = 0; k < 5; k++) c.k[k] = 0.0f;
       for (int k = 0; k < 5; k++) sCf[(s * 32 + lane) * 5 + k] = c.k[k];
-      if (lay.powTable) stagePowers<FORM, W>(c, sPow + (s * 32 + lane) * NP);
-      double2 st0 = make_double2(0.0, 0.0);
+      if (lay.powTable) stagePowersF<FORM, W>(c, sPow + (s * 32 + lane) * NP);
+      float2 st0 = make_float2(0.0, 0.0);
       if (active) {
          const float *sp = a.state + (long long) (s * nv) * a.varPitch + ch;
          if (FORM == DSPLIB_BIQUAD_DF1) { // DF1 (xd1, xd2, yd1, yd2) -> transposed-form state
@@ -410,7 +474,7 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
             st0.y = c.k[2] * xd1 - c.k[4] * yd1;
          }
          else {
-            st0 = make_double2(sp[0], sp[a.varPitch]);
+            st0 = make_float2(sp[0], sp[a.varPitch]);
          }
       }
       sWin[s * 32 + lane] = st0;
@@ -419,19 +483,39 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
    else __syncthreads();
 
    int phase = 0;
+   bool arrived = false; // uniform across the cluster
+   // Device-memory input over several windows: the next window's samples are copied into
+   // shared memory (each thread its own slots) while this one is filtered.
+   const bool usePrefetch = a.prefetch && a.N > windowLen;
    for (long long win0 = 0; win0 < a.N; win0 += windowLen) {
       if (win0 > 0) {
          t0 = win0 + ((long long) rank * W + w) * L;
          len = (active && t0 < a.N) ? (int) ((a.N - t0) < L ? (a.N - t0) : L) : 0;
-         const float *xp = a.x + t0 * a.inPitch + ch;
-         if (len == L) {
+         if (usePrefetch) {
+            asm volatile("cp.async.wait_all;" ::: "memory");
 #pragma unroll
-            for (int i = 0; i < L; i++) v[i] = xp[i * a.inPitch];
+            for (int i = 0; i < L; i++) v[i] = i < len ? sNext[i * (W * 32) + threadIdx.x] : 0.0f;
          }
          else {
+            const float *xp = a.x + t0 * a.inPitch + ch;
+            if (len == L) {
 #pragma unroll
-            for (int i = 0; i < L; i++) v[i] = i < len ? xp[i * a.inPitch] : 0.0f;
+               for (int i = 0; i < L; i++) v[i] = xp[i * a.inPitch];
+            }
+            else {
+#pragma unroll
+               for (int i = 0; i < L; i++) v[i] = i < len ? xp[i * a.inPitch] : 0.0f;
+            }
          }
+      }
+      if (usePrefetch && win0 + windowLen < a.N) {
+         const long long tn = win0 + windowLen + ((long long) rank * W + w) * L;
+         const int ln = (active && tn < a.N) ? (int) ((a.N - tn) < L ? (a.N - tn) : L) : 0;
+         const float *xp = a.x + tn * a.inPitch + ch;
+#pragma unroll
+         for (int i = 0; i < L; i++)
+            if (i < ln) cpAsync4(&sNext[i * (W * 32) + threadIdx.x], xp + i * a.inPitch);
+         asm volatile("cp.async.commit_group;" ::: "memory");
       }
       for (int s = 0; s < a.S; s++) {
          Coef c;
@@ -440,11 +524,11 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
          // 1. zero-state end state of this chunk
          float2 e = make_float2(0.f, 0.f);
          runChunkAny<FORM, L, false>(v, len, c, e, nullptr);
-         sE[w * kPad + lane] = make_double2(e.x, e.y);
+         sE[w * kPad + lane] = make_float2(e.x, e.y);
          __syncthreads();
 
-         // 2. scan over the CTA's W chunks (FP64)
-         const M2 *P;
+         // 2. scan over the CTA's W chunks
+         const M2f *P;
          if (lay.powTable) {
             P = sPow + (s * 32 + cc) * NP;
          }
@@ -454,54 +538,60 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
                Coef cs;
 #pragma unroll
                for (int k = 0; k < 5; k++) cs.k[k] = sCf[(s * 32 + cc) * 5 + k];
-               stagePowers<FORM, W>(cs, sPow + cc * NP);
+               stagePowersF<FORM, W>(cs, sPow + cc * NP);
             }
             __syncwarp();
          }
-         double2 val = segmentScan<W>(sE[j * kPad + cc], j, P, W);
-         double2 ex;
+         float2 val = segmentScanF<W>(sE[j * kPad + cc], j, P, W);
+         float2 ex;
          ex.x = __shfl_up_sync(0xffffffffu, val.x, 1, W);
          ex.y = __shfl_up_sync(0xffffffffu, val.y, 1, W);
-         if (j == 0) ex = make_double2(0.0, 0.0);
+         if (j == 0) ex = make_float2(0.0, 0.0);
 
          // 3. entry state of this CTA, and the state at the end of the window
-         const double2 win = sWin[s * 32 + cc];
-         double2 mine = win, wend;
+         const float2 win = sWin[s * 32 + cc];
+         float2 mine = win, wend;
          if (CLUSTER && K > 1) {
-            double2 *agg = sAgg + (phase & 1) * 32;
+            float2 *agg = sAgg + (phase & 1) * 32;
             if (j == W - 1) agg[cc] = val; // end of this CTA's span from a zero entry state
             cg::this_cluster().sync();
             // lane j holds CTA j's aggregate; scan them with Mc = A^(W*L) powers
-            double2 ej = make_double2(0.0, 0.0);
+            float2 ej = make_float2(0.0, 0.0);
             if (j < K) ej = (j == rank) ? agg[cc] : cg::this_cluster().map_shared_rank(agg, j)[cc];
-            const double2 incl = segmentScan<W>(ej, j, P + LOGW, K);
+            const float2 incl = segmentScanF<W>(ej, j, P + LOGW, K);
+            if (s == a.S - 1 && win0 + windowLen >= a.N) {
+               // last remote read of this CTA: let the others finish (and release their
+               // shared memory) without a second full barrier at the end
+               asm volatile("barrier.cluster.arrive.aligned;" ::: "memory");
+               arrived = true;
+            }
             const int seg = lane - j;
-            double2 before;
+            float2 before;
             before.x = __shfl_sync(0xffffffffu, incl.x, seg + (rank > 0 ? rank - 1 : 0));
             before.y = __shfl_sync(0xffffffffu, incl.y, seg + (rank > 0 ? rank - 1 : 0));
-            double2 last;
+            float2 last;
             last.x = __shfl_sync(0xffffffffu, incl.x, seg + K - 1);
             last.y = __shfl_sync(0xffffffffu, incl.y, seg + K - 1);
-            mine = powApply(P + LOGW, rank, logK, win);
-            if (rank > 0) mine = make_double2(mine.x + before.x, mine.y + before.y);
-            wend = affine(P[LOGW + logK], win, last);
+            mine = powApplyF(P + LOGW, rank, logK, win);
+            if (rank > 0) mine = make_float2(mine.x + before.x, mine.y + before.y);
+            wend = affinef(P[LOGW + logK], win, last);
          }
          else {
-            wend = affine(P[LOGW], win, make_double2(0.0, 0.0));
-            double2 lastv;
+            wend = affinef(P[LOGW], win, make_float2(0.0, 0.0));
+            float2 lastv;
             lastv.x = __shfl_sync(0xffffffffu, val.x, lane - j + W - 1);
             lastv.y = __shfl_sync(0xffffffffu, val.y, lane - j + W - 1);
-            wend = make_double2(wend.x + lastv.x, wend.y + lastv.y);
+            wend = make_float2(wend.x + lastv.x, wend.y + lastv.y);
          }
          // true initial state of chunk j: M^j * entry + exclusive prefix
-         const double2 tv = powApply(P, j, LOGW, mine);
-         sP[j * kPad + cc] = make_double2(tv.x + ex.x, tv.y + ex.y);
+         const float2 tv = powApplyF(P, j, LOGW, mine);
+         sP[j * kPad + cc] = make_float2(tv.x + ex.x, tv.y + ex.y);
          __syncwarp();
          if (j == 0) sWin[s * 32 + cc] = wend;
          __syncthreads();
 
          // 4. rerun from the true state, producing the stage output in place
-         const double2 p = sP[w * kPad + lane];
+         const float2 p = sP[w * kPad + lane];
          float2 st = make_float2((float) p.x, (float) p.y);
          float4 tail = make_float4(0.f, 0.f, 0.f, 0.f);
          runChunkAny<FORM, L, true>(v, len, c, st, &tail);
@@ -552,7 +642,10 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
       }
    }
    // Keep every CTA's shared memory alive until the cluster's last remote read.
-   if (CLUSTER) cg::this_cluster().sync();
+   if (CLUSTER) {
+      if (arrived) asm volatile("barrier.cluster.wait.aligned;" ::: "memory");
+      else cg::this_cluster().sync();
+   }
 }
 
 // ------------------------------------------------------------ per-channel scan
@@ -767,26 +860,29 @@ template <int FORM, int W> cudaError_t launchScanShape(const BiquadLaunch &a, in
    cudaError_t e;
    auto fn1 = biquad_scan_kernel<FORM, W, false>;
    auto fnK = biquad_scan_kernel<FORM, W, true>;
+   // the largest footprint this launch can take (tables + next-window buffer)
+   const size_t maxBytes = lay.total + (a.prefetch ? (size_t) kScanL * W * 32 * sizeof(float) : 0);
    static bool attrSet = false;
    static size_t attrBytes = 0;
-   if (!attrSet || attrBytes < lay.total) {
-      if ((e = cudaFuncSetAttribute(fn1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) lay.total)) != cudaSuccess)
+   if (!attrSet || attrBytes < maxBytes) {
+      if ((e = cudaFuncSetAttribute(fn1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) maxBytes)) != cudaSuccess)
          return e;
-      if ((e = cudaFuncSetAttribute(fnK, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) lay.total)) != cudaSuccess)
+      if ((e = cudaFuncSetAttribute(fnK, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) maxBytes)) != cudaSuccess)
          return e;
       attrSet = true;
-      attrBytes = lay.total;
+      attrBytes = maxBytes;
    }
-   const int K = want > 1 ? pickCluster<FORM, W>(want, lay.total) : 1;
+   const int K = want > 1 ? pickCluster<FORM, W>(want, maxBytes) : 1;
+   const size_t bytes = scanSmemBytes<W>(a, K);
    dim3 grid(K, groups);
    if (K == 1) {
-      fn1<<<grid, block, lay.total, s>>>(a);
+      fn1<<<grid, block, bytes, s>>>(a);
    }
    else {
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = grid;
       cfg.blockDim = block;
-      cfg.dynamicSmemBytes = lay.total;
+      cfg.dynamicSmemBytes = bytes;
       cfg.stream = s;
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributeClusterDimension;

@@ -233,6 +233,7 @@ struct BiquadLaunch {
    int optLayout; // 1: coefficients in the get_coefficients layout
    int N, C, S;
    long long inPitch, outPitch, varPitch, coefPitch; // elements
+   int prefetch = 0; // x is device memory: the scan kernel may fetch the next window early (cp.async)
 };
 
 // NATC: sequential recursion per channel, bit-exact to the reference _cn kernels.
