@@ -353,12 +353,19 @@ def add_nch(x, out, samples, channels, inputs, sY, sZ, sO, *, func_style=OPTIMIZ
     return out
 
 
+def _queue_on(hd, stream):
+    """After init (which sets the handle up): launch on ``stream`` and return once queued."""
+    if stream is not None:
+        hd._check("DSPLIB_gpu_setStream", hd.set_stream(stream))
+        hd._check("DSPLIB_gpu_setAsync", hd.set_async(True))
+
+
 def _float_code(a):
     dt = a.dtype if isinstance(a, np.ndarray) else str(a.dtype).replace("torch.", "")
     return {"float32": FLOAT32, "float64": FLOAT64}[str(dt)]
 
 
-def fltoq15(x, *, func_style=OPTIMIZED, out=None, handle=None):
+def fltoq15(x, *, func_style=OPTIMIZED, out=None, handle=None, stream=None):
     """Float32 / float64 array (numpy or torch, host or device) to Q.15 int16."""
     n = int(x.size if isinstance(x, np.ndarray) else x.numel())
     if out is None:
@@ -373,11 +380,12 @@ def fltoq15(x, *, func_style=OPTIMIZED, out=None, handle=None):
     pin, pout = BufParams1D(_float_code(x), n), BufParams1D(INT16, n)
     hd._check("DSPLIB_fltoq15_init_checkParams", hd.init_check(args, pin, pout))
     hd._check("DSPLIB_fltoq15_init", hd.init(args, pin, pout))
+    _queue_on(hd, stream)
     hd._check("DSPLIB_fltoq15_exec", hd.exec(x, out))
     return out
 
 
-def q15tofl(x, dtype=np.float32, *, func_style=OPTIMIZED, out=None, handle=None):
+def q15tofl(x, dtype=np.float32, *, func_style=OPTIMIZED, out=None, handle=None, stream=None):
     """Q.15 int16 array (numpy or torch, host or device) to float32 / float64."""
     n = int(x.size if isinstance(x, np.ndarray) else x.numel())
     code = {np.dtype(np.float32): FLOAT32, np.dtype(np.float64): FLOAT64}[np.dtype(dtype)]
@@ -393,6 +401,7 @@ def q15tofl(x, dtype=np.float32, *, func_style=OPTIMIZED, out=None, handle=None)
     pin, pout = BufParams1D(INT16, n), BufParams1D(code, n)
     hd._check("DSPLIB_q15tofl_init_checkParams", hd.init_check(args, pin, pout))
     hd._check("DSPLIB_q15tofl_init", hd.init(args, pin, pout))
+    _queue_on(hd, stream)
     hd._check("DSPLIB_q15tofl_exec", hd.exec(x, out))
     return out
 
@@ -417,10 +426,11 @@ def fir_setup(dtype_code, batch, N, T, *, nch, func_style=OPTIMIZED, mma=False, 
 
 
 def fir(x, h, T=None, *, nch=None, func_style=OPTIMIZED, precision=FIR_SIMT, qmode=False, shift=0, out=None,
-        handle=None):
+        handle=None, stream=None):
     """y = FIR(x, h) over channel-major rows of ``x`` [batch, N] with stored
     taps ``h`` [1 or batch, T] (reference tap order).  numpy in -> numpy out
-    (host staging inside the library); torch CUDA in -> torch CUDA out."""
+    (host staging inside the library); torch CUDA in -> torch CUDA out.
+    ``stream``: queue the work on that CUDA stream and return without waiting."""
     batch, N = x.shape
     T = T or h.shape[1]
     if nch is None:
@@ -439,6 +449,7 @@ def fir(x, h, T=None, *, nch=None, func_style=OPTIMIZED, precision=FIR_SIMT, qmo
     hd._check("DSPLIB_fir_init", hd.init(args, pin, pfilt, pout))
     hd.set_precision(precision)
     hd.set_qmode(qmode)
+    _queue_on(hd, stream)
     hd._check("DSPLIB_fir_exec", hd.exec(x, h, out))
     return out
 
@@ -519,7 +530,7 @@ def opt_coefficients(natural, form, nch, C):
     return opt, popt
 
 
-def cascade_biquad(x, coef, state, *, form, nch, func_style=OPTIMIZED, out=None, handle=None):
+def cascade_biquad(x, coef, state, *, form, nch, func_style=OPTIMIZED, out=None, handle=None, stream=None):
     """One exec over time-major ``x`` [N, C].  ``coef`` is the natural buffer
     for NATC and the optimized buffer (``opt_coefficients``) for OPTIMIZED;
     ``state`` [S*nv, C] is updated in place."""
@@ -537,6 +548,7 @@ def cascade_biquad(x, coef, state, *, form, nch, func_style=OPTIMIZED, out=None,
             out = torch.zeros_like(x)
     hd = handle or BiquadHandle()
     hd._check("DSPLIB_cascadeBiquad_init", hd.init(args, pin, pcn if func_style == NATC else popt, pvar, pout))
+    _queue_on(hd, stream)
     hd._check("DSPLIB_cascadeBiquad_exec", hd.exec(x, coef, state, out))
     return out
 

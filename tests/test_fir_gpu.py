@@ -329,3 +329,45 @@ def test_fir_stream_matches_one_call(dt, style, precision, qmode, C, T, N, block
     out = np.zeros((C, N), dt)
     again = st.exec(xb, h, out)
     assert np.array_equal(again, got[:, :N])
+
+
+def test_handles_on_concurrent_host_threads():
+    """Handles are independent: host threads filtering pageable host buffers at the same
+    time (per-thread staging buffers and copy pipelines) give the oracle's results."""
+    import threading
+
+    rng = np.random.default_rng(21)
+    jobs = []
+    for k in range(4):
+        x = rng.integers(-1000, 1000, (64, 40000)).astype(np.int16)
+        h = rng.integers(-1000, 1000, (64, 33)).astype(np.int16)
+        jobs.append((x, h))
+    results, errors = [None] * len(jobs), []
+
+    def work(k):
+        try:
+            x, h = jobs[k]
+            hd = D.FirHandle()
+            s = torch.cuda.Stream()
+            ys = []
+            for _ in range(3):
+                args, pin, pf, po = D.fir_setup(D.INT16, 64, 40000, 33, nch=True)
+                assert hd.init(args, pin, pf, po) == D.SUCCESS
+                hd.set_stream(s)
+                y = np.zeros((64, 40000 - 32), np.int16)
+                assert hd.exec(x, h, y) == D.SUCCESS, hd.last_error()
+                ys.append(y)
+            results[k] = ys
+        except Exception as e:  # reported below
+            errors.append(repr(e))
+
+    threads = [threading.Thread(target=work, args=(k,)) for k in range(len(jobs))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for (x, h), ys in zip(jobs, results):
+        want = oracle.fir(x, h, 33, nch=True)
+        for y in ys:
+            assert np.array_equal(y, want)
