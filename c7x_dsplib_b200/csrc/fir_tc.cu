@@ -30,7 +30,10 @@
 // Each CTA owns consecutive tiles of one channel: the taps are staged into
 // shared memory once and the band built from there; the next tile's signal is
 // staged into the second buffer while the tensor core works on the current
-// one.  All waits on the tensor core are bounded; on expiry the kernel raises
+// one.  The integer kernel is persistent: one wave of CTAs strides over the
+// (channel, tile range) work items, keeps a band of shared taps for all of them
+// and fetches each item's first segment during the previous item's last tile.
+// All waits on the tensor core are bounded; on expiry the kernel raises
 // g_firTcError, frees its TMEM and exits.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -77,37 +80,56 @@ __device__ __forceinline__ T outStage(long long acc, int shift)
    return (T) acc;
 }
 
-// Stage seg samples of xs into the byte plane(s): int8 -> A0; int16 -> A0 = high
-// (signed) bytes, A1 = low (unsigned) bytes.  16-byte vectors when aligned.
+// One 16-byte vector (16 / sizeof(T) samples) of the segment starting at xs, the
+// samples at or beyond `avail` read as zero: whole vectors load as one access, the one
+// vector that straddles the row end element by element.
+template <typename T> __device__ __forceinline__ int4 loadSegVec(const T *xs, long long k, long long avail)
+{
+   constexpr int per = 16 / sizeof(T);
+   const long long s0 = k * per;
+   if (s0 + per <= avail) return ((const int4 *) xs)[k];
+   __align__(16) T tmp[per];
+#pragma unroll
+   for (int e = 0; e < per; e++) tmp[e] = (s0 + e < avail) ? xs[s0 + e] : (T) 0;
+   return *(const int4 *) tmp;
+}
+
+// Write one 16-byte vector of samples into the byte plane(s): int8 -> A0; int16 ->
+// A0 = high (signed) bytes, A1 = low (unsigned) bytes.
+template <typename T>
+__device__ __forceinline__ void putSegVec(const int4 &v, int k, unsigned char *A0, unsigned char *A1)
+{
+   if (sizeof(T) == 1) {
+      ((int4 *) A0)[k] = v;
+   }
+   else {
+      const int16_t *e = (const int16_t *) &v;
+      __align__(8) unsigned char hb[8], lb[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+         hb[i] = (unsigned char) (e[i] >> 8);
+         lb[i] = (unsigned char) (e[i] & 0xFF);
+      }
+      ((uint2 *) A0)[k] = *(uint2 *) hb;
+      ((uint2 *) A1)[k] = *(uint2 *) lb;
+   }
+}
+
+// Stage seg samples of xs (row positions j0 .. j0 + seg - 1, zero from inExtent on) into
+// the byte plane(s).  16-byte vectors when xs is aligned, samples otherwise.
 template <typename T>
 __device__ __forceinline__ void intStage(const T *xs, long long j0, long long inExtent, int seg, unsigned char *A0,
                                          unsigned char *A1, int tid)
 {
    constexpr bool SPLIT = sizeof(T) == 2;
    constexpr int per = 16 / sizeof(T); // samples per 16-byte vector
-   const bool full = j0 + seg <= inExtent;
-   if (full && (((uintptr_t) xs) & 15) == 0) {
-      for (int k = tid; k < seg / per; k += kThreads) {
-         const int4 v = ((const int4 *) xs)[k];
-         if (!SPLIT) {
-            ((int4 *) A0)[k] = v;
-         }
-         else {
-            const int16_t *e = (const int16_t *) &v;
-            __align__(8) unsigned char hb[8], lb[8];
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-               hb[i] = (unsigned char) (e[i] >> 8);
-               lb[i] = (unsigned char) (e[i] & 0xFF);
-            }
-            ((uint2 *) A0)[k] = *(uint2 *) hb;
-            ((uint2 *) A1)[k] = *(uint2 *) lb;
-         }
-      }
+   const long long avail = inExtent - j0;
+   if ((((uintptr_t) xs) & 15) == 0) {
+      for (int k = tid; k < seg / per; k += kThreads) putSegVec<T>(loadSegVec<T>(xs, k, avail), k, A0, A1);
    }
    else {
       for (int k = tid; k < seg; k += kThreads) {
-         const int v = (j0 + k < inExtent) ? (int) xs[k] : 0;
+         const int v = (k < avail) ? (int) xs[k] : 0;
          if (SPLIT) {
             A0[k] = (unsigned char) (v >> 8);
             A1[k] = (unsigned char) (v & 0xFF);
@@ -165,7 +187,7 @@ __device__ __forceinline__ void storeTile(T *dst, int n, const unsigned char *st
 }
 
 template <typename T, int QMODE>
-__global__ void __launch_bounds__(kThreads, 8) fir_int_tc_kernel(FirLaunch a, int tilesPerCta)
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 2 ? 6 : 8) fir_int_tc_kernel(FirLaunch a, int tilesPerCta)
 {
    constexpr bool SPLIT = sizeof(T) == 2;
    constexpr uint32_t kCols = SPLIT ? 64 : 32; // TMEM columns (accumulators of 16 columns each)
@@ -198,53 +220,69 @@ __global__ void __launch_bounds__(kThreads, 8) fir_int_tc_kernel(FirLaunch a, in
 
    const int nt = (a.outSize + kTile - 1) / kTile;
    const long long inExtent = (long long) a.outSize + T_ - 1;
+   // Work item = tiles [part * tilesPerCta, ...) of one channel; CTAs stride over the items
+   // (persistent: the taps band of shared taps is built once per CTA, and each item's first
+   // segment is fetched during the previous item's last tile).
+   const int nParts = (nt + tilesPerCta - 1) / tilesPerCta;
+   const long long nItems = (long long) a.batch * nParts;
    uint32_t iter = 0;
    bool failed = false;
-   for (int l = blockIdx.y; l < a.batch && !failed; l += gridDim.y) {
-      const T *x = (const T *) a.x + (long long) l * a.inPitch;
-      const T *h = (const T *) a.h + (long long) l * a.filtPitch;
-      T *y = (T *) a.y + (long long) l * a.outPitch;
-      for (int wd = tid; wd < gbWords; wd += kThreads) {
-         uint32_t w0 = 0, w1 = 0;
-#pragma unroll
-         for (int j = 0; j < 4; j++) {
-            const int c = 4 * wd + j - 16;
-            const int g = (c >= 0 && c < T_) ? (int) h[T_ - 1 - c] : 0;
-            if (SPLIT) {
-               w0 |= (uint32_t) ((g >> 8) & 0xFF) << (8 * j);
-               w1 |= (uint32_t) (g & 0xFF) << (8 * j);
-            }
-            else {
-               w0 |= (uint32_t) (g & 0xFF) << (8 * j);
-            }
-         }
-         gb0[wd] = w0;
-         if (SPLIT) gb1[wd] = w1;
-      }
-      __syncthreads();
-      // Taps band, K-major no-swizzle: 16-byte chunk ch = 16q + 8i + r (byte 16 ch) holds
-      // B[m = 16q + e][b = 8i + r] = g[16q + e - 8i - r], e < 16: bytes gb[16 + 16q - 8i - r + e],
-      // gathered from five words with funnel shifts.
-      for (int ch = tid; ch < Kt; ch += kThreads) {
-         const int base = 16 + 16 * (ch >> 4) - 8 * ((ch >> 3) & 1) - (ch & 7);
-         const int w = base >> 2, sh = (base & 3) * 8;
-#pragma unroll
-         for (int pl = 0; pl < (SPLIT ? 2 : 1); pl++) {
-            const uint32_t *gb = pl ? gb1 : gb0;
-            const uint32_t v0 = gb[w], v1 = gb[w + 1], v2 = gb[w + 2], v3 = gb[w + 3], v4 = gb[w + 4];
-            uint4 o;
-            o.x = __funnelshift_r(v0, v1, sh);
-            o.y = __funnelshift_r(v1, v2, sh);
-            o.z = __funnelshift_r(v2, v3, sh);
-            o.w = __funnelshift_r(v3, v4, sh);
-            *(uint4 *) ((pl ? B1 : B0) + 16 * ch) = o;
-         }
-      }
-      const int t0 = blockIdx.x * tilesPerCta;
+   int bandOf = -1; // channel whose taps the band holds
+   int buf = 0;
+   long long item = blockIdx.x;
+   if (item < nItems) {
+      const int l = (int) (item / nParts), t0 = (int) (item % nParts) * tilesPerCta;
+      intStage<T>((const T *) a.x + (long long) l * a.inPitch + (long long) t0 * kTile, (long long) t0 * kTile,
+                  inExtent, seg, A(0, 0), A(0, 1), tid);
+   }
+   for (; item < nItems && !failed; item += gridDim.x) {
+      const int l = (int) (item / nParts);
+      const int t0 = (int) (item % nParts) * tilesPerCta;
       const int t1 = min(nt, t0 + tilesPerCta);
-      if (t0 < t1) intStage<T>(x + (long long) t0 * kTile, (long long) t0 * kTile, inExtent, seg, A(0, 0), A(0, 1), tid);
+      const T *x = (const T *) a.x + (long long) l * a.inPitch;
+      T *y = (T *) a.y + (long long) l * a.outPitch;
+      if (bandOf < 0 || (a.filtPitch != 0 && bandOf != l)) {
+         const T *h = (const T *) a.h + (long long) l * a.filtPitch;
+         __syncthreads(); // the previous band's last MMAs are complete (waited) before it changes
+         for (int wd = tid; wd < gbWords; wd += kThreads) {
+            uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+               const int c = 4 * wd + j - 16;
+               const int g = (c >= 0 && c < T_) ? (int) h[T_ - 1 - c] : 0;
+               if (SPLIT) {
+                  w0 |= (uint32_t) ((g >> 8) & 0xFF) << (8 * j);
+                  w1 |= (uint32_t) (g & 0xFF) << (8 * j);
+               }
+               else {
+                  w0 |= (uint32_t) (g & 0xFF) << (8 * j);
+               }
+            }
+            gb0[wd] = w0;
+            if (SPLIT) gb1[wd] = w1;
+         }
+         __syncthreads();
+         // Taps band, K-major no-swizzle: 16-byte chunk ch = 16q + 8i + r (byte 16 ch) holds
+         // B[m = 16q + e][b = 8i + r] = g[16q + e - 8i - r], e < 16: bytes gb[16 + 16q - 8i - r + e],
+         // gathered from five words with funnel shifts.
+         for (int ch = tid; ch < Kt; ch += kThreads) {
+            const int base = 16 + 16 * (ch >> 4) - 8 * ((ch >> 3) & 1) - (ch & 7);
+            const int w = base >> 2, sh = (base & 3) * 8;
+#pragma unroll
+            for (int pl = 0; pl < (SPLIT ? 2 : 1); pl++) {
+               const uint32_t *gb = pl ? gb1 : gb0;
+               const uint32_t v0 = gb[w], v1 = gb[w + 1], v2 = gb[w + 2], v3 = gb[w + 3], v4 = gb[w + 4];
+               uint4 o;
+               o.x = __funnelshift_r(v0, v1, sh);
+               o.y = __funnelshift_r(v1, v2, sh);
+               o.z = __funnelshift_r(v2, v3, sh);
+               o.w = __funnelshift_r(v3, v4, sh);
+               *(uint4 *) ((pl ? B1 : B0) + 16 * ch) = o;
+            }
+         }
+         bandOf = l;
+      }
       for (int t = t0; t < t1; t++) {
-         const int buf = (t - t0) & 1;
          const long long j0 = (long long) t * kTile;
          tc::fenceProxyAsync();
          __syncthreads(); // segment[buf] and band written; previous accumulators drained
@@ -269,18 +307,29 @@ __global__ void __launch_bounds__(kThreads, 8) fir_int_tc_kernel(FirLaunch a, in
             }
             tc::commit(mbar);
          }
-         // Fetch the next segment into registers now; it is written to shared memory after
-         // this tile's drain, so the load latency hides behind the MMAs and the drain.
+         // Fetch the next segment (this item's next tile, or the next item's first) into
+         // registers now; it is written to shared memory after this tile's drain, so the
+         // load latency hides behind the MMAs and the drain.
          constexpr int kPre = SPLIT ? 5 : 3; // 16-byte vectors per thread: (2048 + 2080) * sizeof(T) / 16 / 128
          int4 pre[kPre];
-         const long long jn = j0 + kTile;
-         const bool preVec = t + 1 < t1 && jn + seg <= inExtent && ((((uintptr_t) (x + jn)) & 15) == 0);
+         const T *xn = nullptr;
+         long long jn = 0;
+         if (t + 1 < t1) {
+            xn = x;
+            jn = j0 + kTile;
+         }
+         else if (item + gridDim.x < nItems) {
+            const long long ni = item + gridDim.x;
+            xn = (const T *) a.x + (long long) (ni / nParts) * a.inPitch;
+            jn = (long long) (ni % nParts) * tilesPerCta * kTile;
+         }
+         const bool preVec = xn != nullptr && ((((uintptr_t) (xn + jn)) & 15) == 0);
          const int nvec = seg * (int) sizeof(T) / 16;
          if (preVec) {
 #pragma unroll
             for (int i = 0; i < kPre; i++) {
                const int k = tid + i * kThreads;
-               if (k < nvec) pre[i] = ((const int4 *) (x + jn))[k];
+               if (k < nvec) pre[i] = loadSegVec<T>(xn + jn, k, inExtent - jn);
             }
          }
          const bool done = tc::mbarWait(mbar, iter & 1);
@@ -330,29 +379,14 @@ __global__ void __launch_bounds__(kThreads, 8) fir_int_tc_kernel(FirLaunch a, in
 #pragma unroll
             for (int i = 0; i < kPre; i++) {
                const int k = tid + i * kThreads;
-               if (k < nvec) {
-                  if (!SPLIT) {
-                     ((int4 *) N0)[k] = pre[i];
-                  }
-                  else {
-                     const int16_t *e = (const int16_t *) &pre[i];
-                     __align__(8) unsigned char hb[8], lb[8];
-#pragma unroll
-                     for (int q = 0; q < 8; q++) {
-                        hb[q] = (unsigned char) (e[q] >> 8);
-                        lb[q] = (unsigned char) (e[q] & 0xFF);
-                     }
-                     ((uint2 *) N0)[k] = *(uint2 *) hb;
-                     ((uint2 *) N1)[k] = *(uint2 *) lb;
-                  }
-               }
+               if (k < nvec) putSegVec<T>(pre[i], k, N0, N1);
             }
          }
-         else if (t + 1 < t1) {
-            intStage<T>(x + jn, jn, inExtent, seg, A(buf ^ 1, 0), A(buf ^ 1, 1), tid); // row edge / unaligned
+         else if (xn != nullptr) {
+            intStage<T>(xn + jn, jn, inExtent, seg, A(buf ^ 1, 0), A(buf ^ 1, 1), tid); // unaligned row
          }
+         buf ^= 1;
       }
-      __syncthreads(); // before the next channel's taps overwrite the band
    }
    __syncthreads();
    if (warp == 0) tc::tmemFree(tmem, kCols);
@@ -380,7 +414,18 @@ template <typename T, int QMODE> cudaError_t launchIntTc(const FirLaunch &a, cud
    if (e != cudaSuccess) return e;
    const int nt = (a.outSize + kTile - 1) / kTile;
    const int tpc = tilesPerCtaFor(nt, a.batch, 8);
-   dim3 grid((nt + tpc - 1) / tpc, a.batch < 65535 ? a.batch : 65535);
+   const long long items = (long long) a.batch * ((nt + tpc - 1) / tpc);
+   // persistent: one wave of resident CTAs striding over the work items (CTAs per SM: the
+   // launch bound, or fewer when shared memory runs out first)
+   const int bySmem = (int) ((228u * 1024u) / (smem + 1024u));
+   const int perSm = (SPLIT ? 6 : 8) < bySmem ? (SPLIT ? 6 : 8) : bySmem;
+   int sms = 148;
+   {
+      int dev = 0;
+      if (cudaGetDevice(&dev) == cudaSuccess) (void) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+   }
+   const long long wave = (long long) (perSm > 0 ? perSm : 1) * sms;
+   const int grid = (int) (items < wave ? items : wave);
    fn<<<grid, kThreads, smem, s>>>(a, tpc);
    countLaunch();
    return cudaGetLastError();
