@@ -61,6 +61,7 @@ struct RaggedPlan {
 namespace {
 
 using scan::M2;
+using scan::M2f;
 
 
 constexpr int kRTile = 2048; // samples per item of the adjoint reductions and the loss
@@ -77,7 +78,7 @@ constexpr int kBPowers = 6 + kBLogWarps; // M^(2^k), M = A^16: lanes (k < 5), wa
 constexpr int kRaggedMaxStages = 64;
 // Dynamic shared memory of biquad_ragged_kernel: per-stage carry, powers, coefficients and
 // (adjoint) FP64 coefficient-gradient sums; the adjoint adds each thread's u / y chunk.
-constexpr size_t kBDynCommon = kRaggedMaxStages * sizeof(double2) + kRaggedMaxStages * kBPowers * sizeof(M2) +
+constexpr size_t kBDynCommon = kRaggedMaxStages * sizeof(float2) + kRaggedMaxStages * kBPowers * sizeof(M2f) +
                                (kRaggedMaxStages * 5 + 4) * sizeof(float) + kRaggedMaxStages * 5 * sizeof(double);
 constexpr size_t kBDynPlanes = (size_t) kBThreads * 40 * sizeof(float);
 
@@ -106,54 +107,54 @@ __device__ __forceinline__ int padIdx(int k) { return (k >> 4) * kBPad + (k & 15
 // is filtered from the stage's carried state, the carry is advanced.  P: the
 // stage's M^(2^k); tot: a kBWarps-entry shared buffer not in use by the previous stage.
 template <bool KEEP_W0>
-__device__ __forceinline__ void scanStage(float (&v)[kBL], const float *cf, const M2 *P, double2 *carry,
-                                          double2 *tot, float *w0s, int lane, int warp)
+__device__ __forceinline__ void scanStage(float (&v)[kBL], const float *cf, const M2f *P, float2 *carry,
+                                          float2 *tot, float *w0s, int lane, int warp)
 {
-   const double2 zero = make_double2(0.0, 0.0);
+   const float2 zero = make_float2(0.0f, 0.0f);
    // 1. zero-state end state of this chunk
    float w1 = 0.f, w2 = 0.f;
    df2Chunk<false>(v, cf, w1, w2, nullptr);
    // 2. warp-level inclusive scan over 32 chunks
-   double2 val = make_double2(w1, w2);
+   float2 val = make_float2(w1, w2);
 #pragma unroll
    for (int k = 0; k < 5; k++) {
-      const double2 o = scan::shflUp(val, 1 << k, 32);
+      const float2 o = scan::shflUp(val, 1 << k, 32);
       if (lane >= (1 << k)) val = scan::affine(P[k], o, val);
    }
    if (lane == 31) tot[warp] = val;
    __syncthreads();
    // 3. warp 0: scan over the warp totals (powers M^(32 * 2^k)), entry states, window carry
    if (warp == 0) {
-      double2 tv = lane < kBWarps ? tot[lane] : zero;
+      float2 tv = lane < kBWarps ? tot[lane] : zero;
 #pragma unroll
       for (int k = 0; k < kBLogWarps; k++) {
-         const double2 o = scan::shflUp(tv, 1 << k, 32);
+         const float2 o = scan::shflUp(tv, 1 << k, 32);
          if (lane >= (1 << k) && lane < kBWarps) tv = scan::affine(P[5 + k], o, tv);
       }
-      const double2 win = *carry;
-      const double2 before = scan::shflUp(tv, 1, 32);
-      const double2 last = scan::shflIdx(tv, kBWarps - 1);
+      const float2 win = *carry;
+      const float2 before = scan::shflUp(tv, 1, 32);
+      const float2 last = scan::shflIdx(tv, kBWarps - 1);
       if (lane < kBWarps) {
          // entry of warp `lane`: M^(32*lane) win + inclusive total of warps < lane
-         double2 e = win;
+         float2 e = win;
 #pragma unroll
          for (int k = 0; k < kBLogWarps; k++)
             if ((lane >> k) & 1) e = scan::affine(P[5 + k], e, zero);
-         if (lane > 0) e = make_double2(e.x + before.x, e.y + before.y);
+         if (lane > 0) e = make_float2(e.x + before.x, e.y + before.y);
          tot[lane] = e;
       }
       if (lane == 0) *carry = scan::affine(P[5 + kBLogWarps], win, last);
    }
    __syncthreads();
    // 4. this chunk's initial state: M^lane * entry(warp) + exclusive warp prefix
-   double2 ex = scan::shflUp(val, 1, 32);
+   float2 ex = scan::shflUp(val, 1, 32);
    if (lane == 0) ex = zero;
-   double2 st = tot[warp];
+   float2 st = tot[warp];
 #pragma unroll
    for (int k = 0; k < 5; k++)
       if ((lane >> k) & 1) st = scan::affine(P[k], st, zero);
-   w1 = (float) (st.x + ex.x);
-   w2 = (float) (st.y + ex.y);
+   w1 = st.x + ex.x;
+   w2 = st.y + ex.y;
    df2Chunk<true>(v, cf, w1, w2, KEEP_W0 ? w0s : nullptr);
 }
 
@@ -184,11 +185,11 @@ __global__ void __launch_bounds__(kBThreads, 1)
                          float *planes, long long planeStride, float *yout, float *gout, float *gcoefs)
 {
    __shared__ float sbuf[kBThreads * kBPad];
-   __shared__ double2 sTot[2][kBWarps];
+   __shared__ float2 sTot[2][kBWarps];
    __shared__ float sRed[kBWarps][5];
    extern __shared__ __align__(16) unsigned char dyn[];
-   double2 *sWin = (double2 *) dyn;                     // carry per stage
-   M2 *sPow = (M2 *) (sWin + kRaggedMaxStages);         // M^(2^k) per stage
+   float2 *sWin = (float2 *) dyn;                       // carry per stage
+   M2f *sPow = (M2f *) (sWin + kRaggedMaxStages);       // M^(2^k) per stage (formed in FP64)
    float *sCf = (float *) (sPow + kRaggedMaxStages * kBPowers); // coefficients per stage
    double *sAcc = (double *) (sCf + kRaggedMaxStages * 5 + 4);  // BWD: coefficient gradients per stage
    float *sUY = (float *) (sAcc + kRaggedMaxStages * 5);  // BWD: per thread, u and y of its chunk (20 + 20 floats)
@@ -200,7 +201,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
    const int LuP = (Lu + 15) & ~15;
    const float *cbase = coefs + c.cOff;
    for (int s = tid; s < S; s += kBThreads) {
-      sWin[s] = make_double2(0.0, 0.0);
+      sWin[s] = make_float2(0.0f, 0.0f);
       float cf[5];
 #pragma unroll
       for (int k = 0; k < 5; k++) {
@@ -211,10 +212,10 @@ __global__ void __launch_bounds__(kBThreads, 1)
       M2 A = {-(double) cf[3], -(double) cf[4], 1.0, 0.0};
 #pragma unroll
       for (int r = 1; r < kBL; r <<= 1) A = scan::mmul(A, A);
-      sPow[s * kBPowers] = A;
+      sPow[s * kBPowers] = scan::toF(A);
       for (int k = 1; k < kBPowers; k++) {
          A = scan::mmul(A, A);
-         sPow[s * kBPowers + k] = A;
+         sPow[s * kBPowers + k] = scan::toF(A);
       }
    }
    float *plane0 = planes + c.pOff;
