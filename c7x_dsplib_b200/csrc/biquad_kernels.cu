@@ -18,8 +18,11 @@
 //                       2. chunk-boundary states are combined with
 //                          M = A^L (A: the stage's one-sample state-transition
 //                          matrix) inside the CTA and with Mc = A^(W*L) across
-//                          the CTAs of the cluster through distributed shared
-//                          memory; A^L and the combination run in FP64;
+//                          the CTAs of the cluster: each CTA pushes its span
+//                          aggregates into every CTA's shared memory
+//                          (distributed shared memory), then one cluster
+//                          barrier; the matrix powers are formed in FP64 and
+//                          rounded once, the combination runs in FP32;
 //                       3. every chunk reruns the recursion from its true
 //                          initial state and its outputs become the next
 //                          stage's input, kept in registers.
@@ -305,7 +308,7 @@ template <int W> __host__ __device__ inline ScanSmem scanLayout(int S)
    o.P = off;
    off += (size_t) W * kPad * sizeof(float2);
    o.Agg = off;
-   off += (size_t) 2 * 32 * sizeof(float2);
+   off += (size_t) 32 * sizeof(float2);
    o.Win = off;
    off += (size_t) S * 32 * sizeof(float2);
    const size_t pow = (size_t) S * 32 * ScanShape<W>::NP * sizeof(M2f);
@@ -320,12 +323,14 @@ template <int W> __host__ __device__ inline ScanSmem scanLayout(int S)
 }
 
 // Shared memory of a scan launch: the tables, plus the next-window buffer when the
-// input is device memory and spans more than one window.
+// input is device memory and spans more than one window, plus (clusters) the
+// exchange buffer: two phases of every CTA's 32 chunk-span aggregates.
 template <int W> inline size_t scanSmemBytes(const BiquadLaunch &a, int K)
 {
    const ScanSmem lay = scanLayout<W>(a.S);
    const bool next = a.prefetch && (long long) a.N > (long long) K * W * kScanL;
-   return lay.total + (next ? (size_t) kScanL * W * 32 * sizeof(float) : 0);
+   return lay.total + (next ? (size_t) kScanL * W * 32 * sizeof(float) : 0) +
+          (K > 1 ? (size_t) 2 * K * 32 * sizeof(float2) : 0);
 }
 
 __device__ __forceinline__ void cpAsync4(float *dst, const float *src)
@@ -334,45 +339,7 @@ __device__ __forceinline__ void cpAsync4(float *dst, const float *src)
    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
 }
 
-// Writes M^(2^k), k = 0 .. NP-1, of M = A^L to out[] (two matrices live at a time).
-template <int FORM, int W> __device__ __forceinline__ void stagePowers(const Coef &c, M2 *out)
-{
-   M2 P = transition<FORM>(c);
-#pragma unroll
-   for (int r = 1; r < kScanL; r <<= 1) P = mmul(P, P);
-   out[0] = P;
-#pragma unroll
-   for (int k = 1; k < ScanShape<W>::NP; k++) {
-      P = mmul(P, P);
-      out[k] = P;
-   }
-}
-
-// Inclusive Kogge-Stone scan of x_j over the W lanes of a segment:
-// x_j <- sum_{i <= j} M^(j - i) x_i, with P[k] = M^(2^k) (shared memory).
-template <int W>
-__device__ __forceinline__ double2 segmentScan(double2 val, int j, const M2 *P, int count)
-{
-#pragma unroll
-   for (int k = 0; (1 << k) < W; k++) {
-      double2 o;
-      o.x = __shfl_up_sync(0xffffffffu, val.x, 1 << k, W);
-      o.y = __shfl_up_sync(0xffffffffu, val.y, 1 << k, W);
-      if ((1 << k) < count && j >= (1 << k)) val = affine(P[k], o, val);
-   }
-   return val;
-}
-
-// M^n v for 0 <= n < 2^nb, with P[k] = M^(2^k).
-__device__ __forceinline__ double2 powApply(const M2 *P, int n, int nb, double2 v)
-{
-   const double2 z = make_double2(0.0, 0.0);
-#pragma unroll
-   for (int k = 0; k < 5; k++)
-      if (k < nb && ((n >> k) & 1)) v = affine(P[k], v, z);
-   return v;
-}
-
+// Writes M^(2^k), k = 0 .. NP-1, of M = A^L to out[] (formed in FP64, rounded once).
 template <int FORM, int W> __device__ __forceinline__ void stagePowersF(const Coef &c, M2f *out)
 {
    M2 P = transition<FORM>(c);
@@ -386,6 +353,8 @@ template <int FORM, int W> __device__ __forceinline__ void stagePowersF(const Co
    }
 }
 
+// Inclusive Kogge-Stone scan of x_j over the W lanes of a segment:
+// x_j <- sum_{i <= j} M^(j - i) x_i, with P[k] = M^(2^k) (shared memory).
 template <int W> __device__ __forceinline__ float2 segmentScanF(float2 val, int j, const M2f *P, int count)
 {
 #pragma unroll
@@ -398,6 +367,7 @@ template <int W> __device__ __forceinline__ float2 segmentScanF(float2 val, int 
    return val;
 }
 
+// M^n v for 0 <= n < 2^nb, with P[k] = M^(2^k).
 __device__ __forceinline__ float2 powApplyF(const M2f *P, int n, int nb, float2 v)
 {
    const float2 z = make_float2(0.0f, 0.0f);
@@ -440,6 +410,11 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
    }
    const int logK = ilog2c(K);
    const long long windowLen = (long long) K * W * L;
+   // Device-memory input over several windows: the next window's samples are copied into
+   // shared memory (each thread its own slots) while this one is filtered.
+   const bool usePrefetch = a.prefetch && a.N > windowLen;
+   // [2][K][32]: the aggregates every CTA of the cluster pushed for this phase
+   float2 *sAggIn = (float2 *) (smem + lay.Next + (usePrefetch ? (size_t) L * W * 32 * sizeof(float) : 0));
 
    // First window's input, issued before the table set-up so the loads overlap it.
    long long t0 = ((long long) rank * W + w) * L;
@@ -483,10 +458,6 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
    else __syncthreads();
 
    int phase = 0;
-   bool arrived = false; // uniform across the cluster
-   // Device-memory input over several windows: the next window's samples are copied into
-   // shared memory (each thread its own slots) while this one is filtered.
-   const bool usePrefetch = a.prefetch && a.N > windowLen;
    for (long long win0 = 0; win0 < a.N; win0 += windowLen) {
       if (win0 > 0) {
          t0 = win0 + ((long long) rank * W + w) * L;
@@ -552,19 +523,20 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
          const float2 win = sWin[s * 32 + cc];
          float2 mine = win, wend;
          if (CLUSTER && K > 1) {
-            float2 *agg = sAgg + (phase & 1) * 32;
-            if (j == W - 1) agg[cc] = val; // end of this CTA's span from a zero entry state
+            // Push: warp d stores this CTA's 32 aggregates (the ends of its span from a zero
+            // entry state) into CTA d's exchange buffer, one coalesced 256-byte row; after
+            // the cluster barrier every CTA reads all K rows from its own shared memory.
+            // Writes of phase p + 2 into a row cannot overtake its reads of phase p: those
+            // precede this CTA's arrival at the barrier of phase p + 1.
+            float2 *in = sAggIn + (phase & 1) * (K * 32);
+            if (j == W - 1) sAgg[cc] = val;
+            __syncthreads();
+            if (w < K) cg::this_cluster().map_shared_rank(in, w)[rank * 32 + lane] = sAgg[lane];
             cg::this_cluster().sync();
             // lane j holds CTA j's aggregate; scan them with Mc = A^(W*L) powers
             float2 ej = make_float2(0.0, 0.0);
-            if (j < K) ej = (j == rank) ? agg[cc] : cg::this_cluster().map_shared_rank(agg, j)[cc];
+            if (j < K) ej = in[j * 32 + cc];
             const float2 incl = segmentScanF<W>(ej, j, P + LOGW, K);
-            if (s == a.S - 1 && win0 + windowLen >= a.N) {
-               // last remote read of this CTA: let the others finish (and release their
-               // shared memory) without a second full barrier at the end
-               asm volatile("barrier.cluster.arrive.aligned;" ::: "memory");
-               arrived = true;
-            }
             const int seg = lane - j;
             float2 before;
             before.x = __shfl_sync(0xffffffffu, incl.x, seg + (rank > 0 ? rank - 1 : 0));
@@ -641,11 +613,8 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
          }
       }
    }
-   // Keep every CTA's shared memory alive until the cluster's last remote read.
-   if (CLUSTER) {
-      if (arrived) asm volatile("barrier.cluster.wait.aligned;" ::: "memory");
-      else cg::this_cluster().sync();
-   }
+   // No remote access follows the last cluster barrier (pushes precede it), so CTAs
+   // exit without another one.
 }
 
 // ------------------------------------------------------------ per-channel scan
@@ -861,7 +830,8 @@ template <int FORM, int W> cudaError_t launchScanShape(const BiquadLaunch &a, in
    auto fn1 = biquad_scan_kernel<FORM, W, false>;
    auto fnK = biquad_scan_kernel<FORM, W, true>;
    // the largest footprint this launch can take (tables + next-window buffer)
-   const size_t maxBytes = lay.total + (a.prefetch ? (size_t) kScanL * W * 32 * sizeof(float) : 0);
+   const size_t maxBytes = lay.total + (a.prefetch ? (size_t) kScanL * W * 32 * sizeof(float) : 0) +
+                           (size_t) 2 * kMaxCluster * 32 * sizeof(float2);
    static bool attrSet = false;
    static size_t attrBytes = 0;
    if (!attrSet || attrBytes < maxBytes) {

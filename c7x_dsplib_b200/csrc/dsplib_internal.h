@@ -137,6 +137,8 @@ cudaError_t copyRows(void *dst, const void *src, size_t width, size_t rows, size
 constexpr int kPipeMaxBlocks = 8;
 constexpr size_t kFirPipeMinBytes = 8u << 20;    // host in + out bytes from which FIR exec pipelines
 constexpr size_t kFirPipeBlockBytes = 16u << 20; // in + out bytes per block (2 .. kPipeMaxBlocks blocks)
+constexpr size_t kBqPipeMinBytes = 4u << 20;      // page-locked input bytes from which cascade-biquad exec pipelines
+constexpr size_t kBqPipeBlockBytes = 2u << 20;    // input bytes per time block (2 .. kPipeMaxBlocks blocks)
 struct PipeContext {
    bool ready = false;
    cudaStream_t in = nullptr, comp = nullptr, out = nullptr;

@@ -335,3 +335,52 @@ def test_opt_pinned_host_buffers_read_in_place(form):
     D.cascade_biquad(hx, hc, hs, form=form, nch=0, out=hy, handle=h)
     assert np.array_equal(hy.numpy(), want)
     assert np.array_equal(hs.numpy(), host(sd))
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("C,pinned,in_place", [(40, True, False), (16, True, False), (40, True, True),
+                                               (40, False, False)])
+def test_opt_large_host_signals(form, C, pinned, in_place):
+    """Page-locked host signals of 4 MB or more are copied in, filtered and copied out in
+    blocks of rows on three streams, each block starting from the state the previous one
+    left (lane kernel, per-channel kernel, in place); pageable ones are staged whole.
+    Outputs and final state equal the FP64 oracle to the scan's accuracy, and the call
+    returns complete in asynchronous mode."""
+    rng = np.random.default_rng(60 + form + C)
+    N, S = (30001 if C == 40 else 70001), 3  # 4.5 - 4.8 MB of input, the last block ragged
+    x = rng.standard_normal((N, C)).astype(np.float32)
+    nat = stable_sections(rng, 1, S)
+    opt, _ = D.opt_coefficients(nat, form, 0, C)
+    st0 = (rng.standard_normal((S * nv(form), C)) * 0.1).astype(np.float32)
+    hx, hs, hc = torch.from_numpy(x.copy()), torch.from_numpy(st0.copy()), torch.from_numpy(opt)
+    if pinned:
+        hx, hs, hc = hx.pin_memory(), hs.pin_memory(), hc.pin_memory()
+    hy = hx if in_place else (torch.zeros(N, C).pin_memory() if pinned else torch.zeros(N, C))
+    h = D.BiquadHandle()
+    h.set_async(True)
+    D.cascade_biquad(hx, hc, hs, form=form, nch=0, out=hy, handle=h)
+    y32, st32, y64, _ = oracle_run(form, x, nat, st0, 0)
+    if form != D.TIF:
+        check_accuracy(hy.numpy(), y32, y64, (form, C))
+    else:  # the FP64 truth of TIF runs from a zero state: compare with the FP32 restatement
+        assert np.max(np.abs(hy.numpy() - y32)) <= TOL_REF * max(1.0, float(np.max(np.abs(y32))))
+    assert np.max(np.abs(hs.numpy() - st32)) <= 1e-3 * max(1.0, float(np.max(np.abs(st32))))
+
+
+@pytest.mark.parametrize("form", [D.DF1, D.DF2, D.TDF2])
+def test_natc_host_signals_pipelined_bitexact(form):
+    """NATC on page-locked host signals through the block pipeline (sequential kernel per
+    block, state chained) stays bit-exact to the natural-C restatement, outputs and final
+    state."""
+    rng = np.random.default_rng(70 + form)
+    N, C, S = 22001, 48, 4  # 4.2 MB of input: two blocks
+    x = rng.uniform(-1, 1, size=(N, C)).astype(np.float32)
+    nat = stable_sections(rng, C, S)
+    st = (rng.standard_normal((S * nv(form), C)) * 0.1).astype(np.float32)
+    s_ref = st.copy()
+    want = oracle.biquad(form, x, nat, s_ref, nch=1)
+    hx, hn = torch.from_numpy(x).pin_memory(), torch.from_numpy(nat).pin_memory()
+    hs, hy = torch.from_numpy(st.copy()).pin_memory(), torch.zeros(N, C).pin_memory()
+    D.cascade_biquad(hx, hn, hs, form=form, nch=1, func_style=D.NATC, out=hy)
+    assert np.array_equal(hy.numpy(), want)
+    assert np.array_equal(hs.numpy(), s_ref)
