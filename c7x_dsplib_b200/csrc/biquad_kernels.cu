@@ -867,9 +867,7 @@ template <int FORM, int W> cudaError_t launchScanShape(const BiquadLaunch &a, in
    return cudaGetLastError();
 }
 
-// Launch shape: few channel groups -> 16-warp CTAs and clusters of up to 16
-// CTAs along time (latency); many groups -> 8-warp CTAs (two per SM) with
-// clusters sized to fill one wave of the 148 SMs (throughput).
+// Per-channel kernel: one CTA per channel, shared memory for the stage tables.
 template <int FORM> cudaError_t launchChanForm(const BiquadLaunch &a, cudaStream_t s)
 {
    const size_t smem = chanSmemBytes(a.S);
