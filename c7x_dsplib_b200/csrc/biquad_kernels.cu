@@ -286,16 +286,14 @@ __device__ __forceinline__ float2 affinef(const M2f &m, float2 v, float2 e)
 }
 
 // Matrix powers kept per stage and channel: M^(2^k), M = A^L, for
-// k = 0 .. log2(W) + 4 (the last five cover the CTA span A^(W*L) and its
-// powers up to 16 CTAs).
+// k = 0 .. log2(W) (the last one is the CTA span A^(W*L)).
 template <int W> struct ScanShape {
    static constexpr int LOGW = ilog2c(W);
-   static constexpr int NP = LOGW + 5;
-   static constexpr int CPW = 32 / W; // channels scanned by one warp
+   static constexpr int NP = LOGW + 1;
 };
 
 struct ScanSmem {
-   size_t E, P, Agg, Win, Pow, Cf, Next, total;
+   size_t E, Win, Pow, Cf, Next, total;
    bool powTable;
 };
 
@@ -305,16 +303,12 @@ template <int W> __host__ __device__ inline ScanSmem scanLayout(int S)
    size_t off = 0;
    o.E = off;
    off += (size_t) W * kPad * sizeof(float2);
-   o.P = off;
-   off += (size_t) W * kPad * sizeof(float2);
-   o.Agg = off;
-   off += (size_t) 32 * sizeof(float2);
    o.Win = off;
    off += (size_t) S * 32 * sizeof(float2);
    const size_t pow = (size_t) S * 32 * ScanShape<W>::NP * sizeof(M2f);
    o.powTable = pow <= (size_t) kPowTableBytes;
-   o.Pow = off; // all stages' powers, or one stage's (recomputed per stage) when that is too large
-   off += o.powTable ? pow : (size_t) 32 * ScanShape<W>::NP * sizeof(M2f);
+   o.Pow = off; // all stages' powers, or two buffers of one stage's (recomputed per stage) when too large
+   off += o.powTable ? pow : (size_t) 2 * 32 * ScanShape<W>::NP * sizeof(M2f);
    o.Cf = off;
    off += (size_t) S * 32 * 5 * sizeof(float);
    o.Next = (off + 15) / 16 * 16; // next window's input, fetched during this one (prefetch launches)
@@ -353,20 +347,6 @@ template <int FORM, int W> __device__ __forceinline__ void stagePowersF(const Co
    }
 }
 
-// Inclusive Kogge-Stone scan of x_j over the W lanes of a segment:
-// x_j <- sum_{i <= j} M^(j - i) x_i, with P[k] = M^(2^k) (shared memory).
-template <int W> __device__ __forceinline__ float2 segmentScanF(float2 val, int j, const M2f *P, int count)
-{
-#pragma unroll
-   for (int k = 0; (1 << k) < W; k++) {
-      float2 o;
-      o.x = __shfl_up_sync(0xffffffffu, val.x, 1 << k, W);
-      o.y = __shfl_up_sync(0xffffffffu, val.y, 1 << k, W);
-      if ((1 << k) < count && j >= (1 << k)) val = affinef(P[k], o, val);
-   }
-   return val;
-}
-
 // M^n v for 0 <= n < 2^nb, with P[k] = M^(2^k).
 __device__ __forceinline__ float2 powApplyF(const M2f *P, int n, int nb, float2 v)
 {
@@ -384,12 +364,9 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
    constexpr int nv = FORM == DSPLIB_BIQUAD_DF1 ? 4 : 2;
    constexpr int LOGW = ScanShape<W>::LOGW;
    constexpr int NP = ScanShape<W>::NP;
-   constexpr int CPW = ScanShape<W>::CPW;
    extern __shared__ __align__(16) unsigned char smem[];
    const ScanSmem lay = scanLayout<W>(a.S);
    float2 *sE = (float2 *) (smem + lay.E);
-   float2 *sP = (float2 *) (smem + lay.P);
-   float2 *sAgg = (float2 *) (smem + lay.Agg);
    float2 *sWin = (float2 *) (smem + lay.Win);
    M2f *sPow = (M2f *) (smem + lay.Pow);
    float *sCf = (float *) (smem + lay.Cf);
@@ -399,16 +376,12 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
    const int w = threadIdx.x >> 5;
    const int ch = blockIdx.y * 32 + lane;
    const bool active = ch < a.C;
-   // scan role: warp w scans the W chunks of channels CPW*w .. CPW*w+CPW-1
-   const int j = lane % W;
-   const int cc = w * CPW + lane / W;
    int K = 1, rank = 0;
    if (CLUSTER) {
       cg::cluster_group cl = cg::this_cluster();
       K = (int) cl.num_blocks();
       rank = (int) cl.block_rank();
    }
-   const int logK = ilog2c(K);
    const long long windowLen = (long long) K * W * L;
    // Device-memory input over several windows: the next window's samples are copied into
    // shared memory (each thread its own slots) while this one is filtered.
@@ -492,79 +465,65 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
          Coef c;
 #pragma unroll
          for (int k = 0; k < 5; k++) c.k[k] = sCf[(s * 32 + lane) * 5 + k];
-         // 1. zero-state end state of this chunk
-         float2 e = make_float2(0.f, 0.f);
-         runChunkAny<FORM, L, false>(v, len, c, e, nullptr);
-         sE[w * kPad + lane] = make_float2(e.x, e.y);
-         __syncthreads();
-
-         // 2. scan over the CTA's W chunks
+         // Matrix powers of this stage for channel `lane`: the table, or (deep cascades) this
+         // stage's powers formed by warp 0 into the buffer of this iteration's parity.  A buffer
+         // is rewritten two iterations later, once every warp has passed the barrier between.
          const M2f *P;
          if (lay.powTable) {
-            P = sPow + (s * 32 + cc) * NP;
+            P = sPow + (s * 32 + lane) * NP;
          }
          else {
-            P = sPow + cc * NP;
-            if (j == 0) {
-               Coef cs;
-#pragma unroll
-               for (int k = 0; k < 5; k++) cs.k[k] = sCf[(s * 32 + cc) * 5 + k];
-               stagePowersF<FORM, W>(cs, sPow + cc * NP);
-            }
-            __syncwarp();
+            P = sPow + ((phase & 1) * 32 + lane) * NP;
+            if (w == 0) stagePowersF<FORM, W>(c, (M2f *) P);
          }
-         float2 val = segmentScanF<W>(sE[j * kPad + cc], j, P, W);
-         float2 ex;
-         ex.x = __shfl_up_sync(0xffffffffu, val.x, 1, W);
-         ex.y = __shfl_up_sync(0xffffffffu, val.y, 1, W);
-         if (j == 0) ex = make_float2(0.0, 0.0);
-
-         // 3. entry state of this CTA, and the state at the end of the window
-         const float2 win = sWin[s * 32 + cc];
-         float2 mine = win, wend;
-         if (CLUSTER && K > 1) {
-            // Push: warp d stores this CTA's 32 aggregates (the ends of its span from a zero
-            // entry state) into CTA d's exchange buffer, one coalesced 256-byte row; after
-            // the cluster barrier every CTA reads all K rows from its own shared memory.
-            // Writes of phase p + 2 into a row cannot overtake its reads of phase p: those
-            // precede this CTA's arrival at the barrier of phase p + 1.
-            float2 *in = sAggIn + (phase & 1) * (K * 32);
-            if (j == W - 1) sAgg[cc] = val;
-            __syncthreads();
-            if (w < K) cg::this_cluster().map_shared_rank(in, w)[rank * 32 + lane] = sAgg[lane];
-            cg::this_cluster().sync();
-            // lane j holds CTA j's aggregate; scan them with Mc = A^(W*L) powers
-            float2 ej = make_float2(0.0, 0.0);
-            if (j < K) ej = in[j * 32 + cc];
-            const float2 incl = segmentScanF<W>(ej, j, P + LOGW, K);
-            const int seg = lane - j;
-            float2 before;
-            before.x = __shfl_sync(0xffffffffu, incl.x, seg + (rank > 0 ? rank - 1 : 0));
-            before.y = __shfl_sync(0xffffffffu, incl.y, seg + (rank > 0 ? rank - 1 : 0));
-            float2 last;
-            last.x = __shfl_sync(0xffffffffu, incl.x, seg + K - 1);
-            last.y = __shfl_sync(0xffffffffu, incl.y, seg + K - 1);
-            mine = powApplyF(P + LOGW, rank, logK, win);
-            if (rank > 0) mine = make_float2(mine.x + before.x, mine.y + before.y);
-            wend = affinef(P[LOGW + logK], win, last);
-         }
-         else {
-            wend = affinef(P[LOGW], win, make_float2(0.0, 0.0));
-            float2 lastv;
-            lastv.x = __shfl_sync(0xffffffffu, val.x, lane - j + W - 1);
-            lastv.y = __shfl_sync(0xffffffffu, val.y, lane - j + W - 1);
-            wend = make_float2(wend.x + lastv.x, wend.y + lastv.y);
-         }
-         // true initial state of chunk j: M^j * entry + exclusive prefix
-         const float2 tv = powApplyF(P, j, LOGW, mine);
-         sP[j * kPad + cc] = make_float2(tv.x + ex.x, tv.y + ex.y);
-         __syncwarp();
-         if (j == 0) sWin[s * 32 + cc] = wend;
+         // 1. zero-state end state of this chunk.  The window's entry state for this stage
+         //    is read before the barrier: it is replaced after it.
+         float2 e = make_float2(0.f, 0.f);
+         runChunkAny<FORM, L, false>(v, len, c, e, nullptr);
+         const float2 win = sWin[s * 32 + lane];
+         sE[w * kPad + lane] = e;
          __syncthreads();
 
+         // 2. chunk-boundary states, lane = channel, by Horner's rule over the chunks before
+         //    this warp's with M = A^L: each warp needs only its own, so warps leave the scan
+         //    (and start their reruns) at staggered times.
+         const M2f M = P[0];
+         float2 st;
+         if (CLUSTER && K > 1) {
+            float2 pre = make_float2(0.f, 0.f); // from a zero state at the CTA's start
+            for (int i = 0; i < w; i++) pre = affinef(M, pre, sE[i * kPad + lane]);
+            // Push: the last warp holds this CTA's aggregates (the end of its span from a
+            // zero entry state) and stores them as one coalesced 256-byte row into every
+            // CTA's exchange buffer; after the cluster barrier each CTA reads all K rows from
+            // its own shared memory.  Writes of phase p + 2 into a row cannot overtake its
+            // reads of phase p: those precede this CTA's arrival at the barrier of phase p + 1.
+            float2 *in = sAggIn + (phase & 1) * (K * 32);
+            if (w == W - 1) {
+               const float2 agg = affinef(M, pre, e);
+               for (int d = 0; d < K; d++) cg::this_cluster().map_shared_rank(in, d)[rank * 32 + lane] = agg;
+            }
+            cg::this_cluster().sync();
+            // 3. entry state of this CTA: the window entry carried over the aggregates of the
+            //    CTAs before it with Mc = A^(W*L); over all K, the state at the window's end
+            const M2f Mc = P[LOGW];
+            float2 acc = win, mine = win;
+            for (int r = 0; r < K; r++) {
+               if (r == rank) mine = acc;
+               acc = affinef(Mc, acc, in[r * 32 + lane]);
+            }
+            if (w == 0) sWin[s * 32 + lane] = acc;
+            // true initial state of this chunk: M^w * entry + prefix
+            const float2 tv = powApplyF(P, w, LOGW, mine);
+            st = make_float2(tv.x + pre.x, tv.y + pre.y);
+         }
+         else {
+            float2 acc = win;
+            for (int i = 0; i < w; i++) acc = affinef(M, acc, sE[i * kPad + lane]);
+            st = acc;
+            if (w == W - 1) sWin[s * 32 + lane] = affinef(M, acc, e); // state at the window's end
+         }
+
          // 4. rerun from the true state, producing the stage output in place
-         const float2 p = sP[w * kPad + lane];
-         float2 st = make_float2((float) p.x, (float) p.y);
          float4 tail = make_float4(0.f, 0.f, 0.f, 0.f);
          runChunkAny<FORM, L, true>(v, len, c, st, &tail);
          if (FORM == DSPLIB_BIQUAD_TIF && c.k[4] != 1.0f) {
