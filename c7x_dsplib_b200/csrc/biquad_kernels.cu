@@ -15,14 +15,17 @@
 //                     samples.  For each stage:
 //                       1. every chunk runs the stage recursion from a zero
 //                          state, giving its end state e (FP32);
-//                       2. chunk-boundary states are combined with
-//                          M = A^L (A: the stage's one-sample state-transition
-//                          matrix) inside the CTA and with Mc = A^(W*L) across
-//                          the CTAs of the cluster: each CTA pushes its span
-//                          aggregates into every CTA's shared memory
-//                          (distributed shared memory), then one cluster
-//                          barrier; the matrix powers are formed in FP64 and
-//                          rounded once, the combination runs in FP32;
+//                       2. each warp forms its chunk's true initial state
+//                          from the end states of the chunks before it, by
+//                          Horner's rule with M = A^L (A: the stage's
+//                          one-sample state-transition matrix), lane =
+//                          channel; across the CTAs of the cluster the last
+//                          warp pushes the CTA's span aggregates into every
+//                          CTA's shared memory (distributed shared memory),
+//                          one cluster barrier, and each warp carries the
+//                          window entry over the earlier CTAs' aggregates
+//                          with Mc = A^(W*L); the matrix powers are formed in
+//                          FP64 and rounded once, the combination runs in FP32;
 //                       3. every chunk reruns the recursion from its true
 //                          initial state and its outputs become the next
 //                          stage's input, kept in registers.
