@@ -437,12 +437,13 @@ constexpr int kBfPhases = 64;
 constexpr int kBfTile = kRows * kBfPhases;
 constexpr int kBfMaxTaps = kFirBfMaxTaps;
 static_assert(kBfTile == kFirBfTile, "ragged run tiles and kernel tiles must agree");
-constexpr int kBfThreads = 256;
-constexpr int kBfChunksPerThread = 5; // 16-byte plane chunks staged per thread: bfBlocks(512) * 8 / 256
-constexpr int kBfPadLeft = 64;        // zero taps ahead of the reversed taps (phase offsets)
+constexpr int kBfThreads = 512;
+constexpr int kBfPadLeft = 64; // zero taps ahead of the reversed taps (phase offsets)
 
-__host__ __device__ inline int bfK(int T) { return ((63 + T + 15) / 16) * 16; }
-__host__ __device__ inline int bfBlocks(int T) { return kRows + (bfK(T) + 63) / 64; }
+__host__ __device__ constexpr int bfK(int T) { return ((63 + T + 15) / 16) * 16; }
+__host__ __device__ constexpr int bfBlocks(int T) { return kRows + (bfK(T) + 63) / 64; }
+// 16-byte plane chunks staged per thread by bfStage
+constexpr int kBfChunksPerThread = (bfBlocks(kBfMaxTaps) * 8 + kBfThreads - 1) / kBfThreads;
 __host__ __device__ inline int bfTapSlots(int T) { return kBfPadLeft + bfK(T) + 8; }
 
 __device__ __forceinline__ void splitBf16(float v, uint16_t &hi, uint16_t &lo)
@@ -603,26 +604,27 @@ __device__ __forceinline__ bool bfDrain(const BfRun &r, const BfSmem &L, uint32_
    tc::fenceAfterSync();
    const long long j0 = (long long) t * kBfTile;
    {
-      // Warp w drains TMEM lane quadrant w % 4 (rows a) and output half w / 4:
-      // y[j0 + 64a + 32*half + b] = D[a][32*half + b] + D[a][64 + 32*half + b].
-      const int quad = warp & 3, half = warp >> 2;
+      // Warp w drains TMEM lane quadrant w % 4 (rows a) and output quarter qt = w / 4
+      // (16 phases): y[j0 + 64a + 16*qt + b] = D[a][16*qt + b] + D[a][64 + 16*qt + b].
+      const int quad = warp & 3, qt = warp >> 2, half = qt >> 1;
       const uint32_t acc = tmem + ((uint32_t) (quad * 32) << 16);
       const int row = quad * 32 + lane;
-      uint32_t a[32], b[32];
-      tc::tmemLoad32(acc + half * 32, a);
-      tc::tmemLoad32(acc + 64 + half * 32, b);
+      uint32_t a[16], b[16];
+      tc::tmemLoad16(acc + qt * 16, a);
+      tc::tmemLoad16(acc + 64 + qt * 16, b);
       tc::tmemWaitLoad();
       // The planes are free once the MMAs completed: they hold the output tile,
       // 16-byte chunk v4 of row half (row, half) rotated to slot (v4 + row) & 7 so
       // that eight consecutive rows store to distinct banks.
       float *os = (float *) L.hi + row * kBfPhases + half * 32;
 #pragma unroll
-      for (int v4 = 0; v4 < 8; v4++) {
+      for (int v = 0; v < 4; v++) {
+         const int v4 = (qt & 1) * 4 + v;
          float4 o;
-         o.x = __uint_as_float(a[4 * v4 + 0]) + __uint_as_float(b[4 * v4 + 0]);
-         o.y = __uint_as_float(a[4 * v4 + 1]) + __uint_as_float(b[4 * v4 + 1]);
-         o.z = __uint_as_float(a[4 * v4 + 2]) + __uint_as_float(b[4 * v4 + 2]);
-         o.w = __uint_as_float(a[4 * v4 + 3]) + __uint_as_float(b[4 * v4 + 3]);
+         o.x = __uint_as_float(a[4 * v + 0]) + __uint_as_float(b[4 * v + 0]);
+         o.y = __uint_as_float(a[4 * v + 1]) + __uint_as_float(b[4 * v + 1]);
+         o.z = __uint_as_float(a[4 * v + 2]) + __uint_as_float(b[4 * v + 2]);
+         o.w = __uint_as_float(a[4 * v + 3]) + __uint_as_float(b[4 * v + 3]);
          *(float4 *) (os + (((v4 + row) & 7) << 2)) = o;
       }
    }
