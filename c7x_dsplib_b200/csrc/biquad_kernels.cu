@@ -296,7 +296,7 @@ template <int W> struct ScanShape {
 };
 
 struct ScanSmem {
-   size_t E, Win, Pow, Cf, Next, total;
+   size_t E, Mine, Win, Pow, Cf, Next, total;
    bool powTable;
 };
 
@@ -306,6 +306,8 @@ template <int W> __host__ __device__ inline ScanSmem scanLayout(int S)
    size_t off = 0;
    o.E = off;
    off += (size_t) W * kPad * sizeof(float2);
+   o.Mine = off;
+   off += (size_t) 32 * sizeof(float2);
    o.Win = off;
    off += (size_t) S * 32 * sizeof(float2);
    const size_t pow = (size_t) S * 32 * ScanShape<W>::NP * sizeof(M2f);
@@ -350,6 +352,25 @@ template <int FORM, int W> __device__ __forceinline__ void stagePowersF(const Co
    }
 }
 
+// Horner's rule acc <- M acc + e_i over i = 0 .. n-1 (n <= MAXN), e_i = src[i * stride].
+// The loads are issued eight at a time ahead of the dependent multiply-adds, so the chain
+// costs about one FMA latency pair per step rather than a shared-memory round trip.
+template <int MAXN>
+__device__ __forceinline__ float2 hornerF(const M2f &M, float2 acc, const float2 *src, int stride, int n)
+{
+#pragma unroll
+   for (int g = 0; g < MAXN; g += 8) {
+      if (g >= n) break;
+      float2 e[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) e[i] = (g + i < n) ? src[(g + i) * stride] : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+         if (g + i < n) acc = affinef(M, acc, e[i]);
+   }
+   return acc;
+}
+
 // M^n v for 0 <= n < 2^nb, with P[k] = M^(2^k).
 __device__ __forceinline__ float2 powApplyF(const M2f *P, int n, int nb, float2 v)
 {
@@ -370,6 +391,7 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
    extern __shared__ __align__(16) unsigned char smem[];
    const ScanSmem lay = scanLayout<W>(a.S);
    float2 *sE = (float2 *) (smem + lay.E);
+   float2 *sMine = (float2 *) (smem + lay.Mine);
    float2 *sWin = (float2 *) (smem + lay.Win);
    M2f *sPow = (M2f *) (smem + lay.Pow);
    float *sCf = (float *) (smem + lay.Cf);
@@ -493,35 +515,46 @@ __global__ void __launch_bounds__(W * 32, 16 / W) biquad_scan_kernel(BiquadLaunc
          const M2f M = P[0];
          float2 st;
          if (CLUSTER && K > 1) {
-            float2 pre = make_float2(0.f, 0.f); // from a zero state at the CTA's start
-            for (int i = 0; i < w; i++) pre = affinef(M, pre, sE[i * kPad + lane]);
-            // Push: the last warp holds this CTA's aggregates (the end of its span from a
-            // zero entry state) and stores them as one coalesced 256-byte row into every
-            // CTA's exchange buffer; after the cluster barrier each CTA reads all K rows from
-            // its own shared memory.  Writes of phase p + 2 into a row cannot overtake its
-            // reads of phase p: those precede this CTA's arrival at the barrier of phase p + 1.
             float2 *in = sAggIn + (phase & 1) * (K * 32);
             if (w == W - 1) {
-               const float2 agg = affinef(M, pre, e);
-               for (int d = 0; d < K; d++) cg::this_cluster().map_shared_rank(in, d)[rank * 32 + lane] = agg;
+               // This CTA's aggregate (the end of its span from a zero entry state) by a
+               // pairwise tree over the W chunk end states with P[k] = M^(2^k), pushed as one
+               // coalesced 256-byte row into every CTA's exchange buffer.  After the cluster
+               // barrier each CTA reads all K rows from its own shared memory.  Writes of phase
+               // p + 2 into a row cannot overtake its reads of phase p: those precede this CTA's
+               // arrival at the barrier of phase p + 1.
+               float2 t[W];
+#pragma unroll
+               for (int i = 0; i < W; i++) t[i] = sE[i * kPad + lane];
+#pragma unroll
+               for (int k = 0; k < LOGW; k++) {
+                  const M2f Pk = P[k];
+#pragma unroll
+                  for (int i = 0; i < (W >> (k + 1)); i++) t[i] = affinef(Pk, t[2 * i], t[2 * i + 1]);
+               }
+               for (int d = 0; d < K; d++) cg::this_cluster().map_shared_rank(in, d)[rank * 32 + lane] = t[0];
             }
-            cg::this_cluster().sync();
-            // 3. entry state of this CTA: the window entry carried over the aggregates of the
-            //    CTAs before it with Mc = A^(W*L); over all K, the state at the window's end
-            const M2f Mc = P[LOGW];
-            float2 acc = win, mine = win;
-            for (int r = 0; r < K; r++) {
-               if (r == rank) mine = acc;
-               acc = affinef(Mc, acc, in[r * 32 + lane]);
+            asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+            // the chunks before this warp's, from a zero state at the CTA's start, while the
+            // other CTAs' aggregates arrive
+            const float2 pre = hornerF<W>(M, make_float2(0.f, 0.f), sE + lane, kPad, w);
+            asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+            // 3. entry state of this CTA, formed once by warp 0 and shared: the window entry
+            //    carried over the aggregates of the CTAs before it with Mc = A^(W*L); over all
+            //    K, the state at the window's end
+            if (w == 0) {
+               const M2f Mc = P[LOGW];
+               const float2 mine = hornerF<kMaxCluster>(Mc, win, in + lane, 32, rank);
+               sMine[lane] = mine;
+               sWin[s * 32 + lane] = hornerF<kMaxCluster>(Mc, mine, in + rank * 32 + lane, 32, K - rank);
             }
-            if (w == 0) sWin[s * 32 + lane] = acc;
+            __syncthreads();
             // true initial state of this chunk: M^w * entry + prefix
-            const float2 tv = powApplyF(P, w, LOGW, mine);
+            const float2 tv = powApplyF(P, w, LOGW, sMine[lane]);
             st = make_float2(tv.x + pre.x, tv.y + pre.y);
          }
          else {
-            float2 acc = win;
-            for (int i = 0; i < w; i++) acc = affinef(M, acc, sE[i * kPad + lane]);
+            const float2 acc = hornerF<W>(M, win, sE + lane, kPad, w);
             st = acc;
             if (w == W - 1) sWin[s * 32 + lane] = affinef(M, acc, e); // state at the window's end
          }
