@@ -20,12 +20,14 @@
 //                          Horner's rule with M = A^L (A: the stage's
 //                          one-sample state-transition matrix), lane =
 //                          channel; across the CTAs of the cluster the last
-//                          warp pushes the CTA's span aggregates into every
-//                          CTA's shared memory (distributed shared memory),
-//                          one cluster barrier, and each warp carries the
-//                          window entry over the earlier CTAs' aggregates
-//                          with Mc = A^(W*L); the matrix powers are formed in
-//                          FP64 and rounded once, the combination runs in FP32;
+//                          warp forms the CTA's span aggregates by a pairwise
+//                          tree and pushes them into every CTA's shared memory
+//                          (distributed shared memory), the warps form their
+//                          prefixes while the cluster barrier completes, and
+//                          one warp carries the window entry over the earlier
+//                          CTAs' aggregates with Mc = A^(W*L) for all; the
+//                          matrix powers are formed in FP64 and rounded once,
+//                          the combination runs in FP32;
 //                       3. every chunk reruns the recursion from its true
 //                          initial state and its outputs become the next
 //                          stage's input, kept in registers.
