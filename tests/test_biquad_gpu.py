@@ -219,6 +219,44 @@ def test_opt_in_place():
     assert np.max(rel_per_channel(host(xd), y64)) <= REL
 
 
+@pytest.mark.parametrize("form", FORMS)
+def test_opt_deep_cascade_lane_scan(form):
+    """Cascades of 26 - 160 stages stay on the lane-per-channel scan kernel with the matrix
+    powers formed per stage (no per-stage table): across a cluster of CTAs (5000 samples)
+    and within one CTA (600 samples), shared and per-channel coefficients."""
+    rng = np.random.default_rng(80 + form)
+    for (N, C, S, nch) in [(5000, 48, 40, 0), (600, 200, 33, 1), (2000, 40, 120, 1)]:
+        x = rng.standard_normal((N, C)).astype(np.float32)
+        nat = stable_sections(rng, C if nch else 1, S, rmax=0.8)
+        st = np.zeros((S * nv(form), C), np.float32)
+        opt, _ = D.opt_coefficients(nat, form, nch, C)
+        sd = dev(st)
+        y = host(D.cascade_biquad(dev(x), dev(opt), sd, form=form, nch=nch))
+        y32, st32, y64, s64 = oracle_run(form, x, nat, st, nch)
+        # against FP64 only (per channel, within 1e-4 or 4x the error of the sequential FP32
+        # recursion): over a deep high-gain cascade the FP32 restatement itself drifts beyond
+        # the reference's absolute 2^-10 criterion, in its own direction
+        seq = rel_per_channel(y32, y64)
+        assert np.all(rel_per_channel(y, y64) <= np.maximum(REL, 4 * seq + 1e-6)), (form, N, C, S)
+        got = host(sd).astype(np.float64)
+        if form != D.TIF:
+            # final states against FP64: within 1e-3 of their scale, or 4x the error of the
+            # sequential FP32 recursion when that is larger (deep cascades with large inner gain)
+            seq = float(np.max(np.abs(st32 - s64)))
+            tol = max(1e-3 * max(1.0, float(np.max(np.abs(s64)))), 4 * seq + 1e-6)
+            assert np.max(np.abs(got - s64)) <= tol, (form, N, C, S)
+        else:
+            # TIF keeps its own state form (no FP64 restatement): check it by what it does,
+            # continuing the signal for a second block from the returned state
+            x2 = rng.standard_normal((N, C)).astype(np.float32)
+            y2 = host(D.cascade_biquad(dev(x2), dev(opt), sd, form=form, nch=nch))
+            xx = np.concatenate([x, x2])
+            yy32, _, yy64, _ = oracle_run(form, xx, nat, st, nch)
+            seq = rel_per_channel(yy32, yy64)
+            got2 = rel_per_channel(np.concatenate([y, y2]), yy64)
+            assert np.all(got2 <= np.maximum(REL, 4 * seq + 1e-6)), (form, N, C, S, float(np.max(got2)))
+
+
 def test_opt_deep_cascade_uses_sequential_kernel():
     rng = np.random.default_rng(6)
     N, C, S = 300, 9, 170  # DF1 beyond the scan kernel's stage limit (160)
