@@ -162,6 +162,19 @@ def test_bf16x3_accuracy(nch):
         assert np.max(np.abs(y - oracle.fir(x, hh, T, nch=nch))) <= TOL_REF
 
 
+def test_bf16x3_tile_runs_per_cta():
+    """Enough channels that each CTA filters a run of four consecutive 8192-output tiles of
+    one channel (raw tiles two ahead in the ring, barrier phases carried across tiles);
+    per-channel taps, rows whose starts alternate between 16-byte aligned and not."""
+    rng = np.random.default_rng(41)
+    B, T = 300, 251
+    N = 4 * 8192 + T - 1
+    x = rng.standard_normal((B, N)).astype(np.float32)
+    hh = lowpass(rng, B, T)
+    y = host(D.fir(dev(x), dev(hh), T, nch=1, precision=D.FIR_BF16X3))
+    assert np.max(_relerr(y, oracle.fir_f64(x, hh, T, nch=1))) <= 1e-5
+
+
 def test_bf16x3_long_filter_uses_fp32_kernel():
     rng = np.random.default_rng(5)
     x = rng.standard_normal((2, 3000)).astype(np.float32)
