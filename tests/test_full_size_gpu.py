@@ -1,0 +1,102 @@
+"""The benchmark configurations at their full sizes, on the GPU through the C ABI.
+
+The oracle cannot recompute whole workloads of this size within a test, so each check
+uses what holds at any size: bit-exact agreement on a seeded sample of channels (the
+channels are independent, so a channel's output depends only on its own row), exact
+linearity of the wrapping integer FIR over the whole batch, and the FP64 error bound on
+sampled channels for the floating-point paths.
+
+Configurations: int8 / int16 FIR 4096 ch x 16384 samples, 128 shared taps (Q mode with
+shift 7 / 15, and the natural-C wrap); FP32 FIR 1024 ch x 65536 samples, 256 taps per
+channel (plain and split-BF16); DF2 cascade 4096 ch x 8192 samples x 4 stages.
+"""
+import numpy as np
+import pytest
+
+import c7x_dsplib_b200 as D
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+def sample_rows(rng, n, k):
+    return np.sort(rng.choice(n, size=k, replace=False))
+
+
+@pytest.mark.parametrize("dt,shift", [(np.int8, 7), (np.int16, 15)])
+def test_int_fir_full_size(dt, shift):
+    """4096 x 16384, 128 shared taps: Q mode and wrap bit-exact on 48 sampled channels;
+    wrap mode exactly linear over the whole batch (y(a) + y(b) == y(a + b) modulo 2^bits)."""
+    rng = np.random.default_rng(90 + shift)
+    B, N, T = 4096, 16384, 128
+    info = np.iinfo(dt)
+    a = rng.integers(info.min, info.max, size=(B, N), endpoint=True).astype(dt)
+    h = rng.integers(info.min, info.max, size=(1, T), endpoint=True).astype(dt)
+    rows = sample_rows(rng, B, 48)
+    ad, hd = dev(a), dev(h)
+    yq = D.fir(ad, hd, T, nch=0, func_style=D.OPTIMIZED, qmode=True, shift=shift)
+    assert np.array_equal(host(yq)[rows], oracle.fir_q(a[rows], h, T, shift, nch=0))
+    ya = host(D.fir(ad, hd, T, nch=0, func_style=D.OPTIMIZED))
+    assert np.array_equal(ya[rows], oracle.fir(a[rows], h, T, nch=0))
+    b = rng.integers(info.min, info.max, size=(B, N), endpoint=True).astype(dt)
+    yb = host(D.fir(dev(b), hd, T, nch=0, func_style=D.OPTIMIZED))
+    s = (a.astype(np.int64) + b).astype(dt)  # wraps like the data type
+    ys = host(D.fir(dev(s), hd, T, nch=0, func_style=D.OPTIMIZED))
+    assert np.array_equal(ys, (ya.astype(np.int64) + yb).astype(dt))
+
+
+@pytest.mark.parametrize("precision,tol", [(D.FIR_SIMT, 2e-6), (D.FIR_BF16X3, 1e-5)])
+def test_float_fir_full_size(precision, tol):
+    """1024 x 65536, 256 Hamming-windowed sinc taps per channel: max |y - y64| / max |y64|
+    within the stated bound on 16 sampled channels."""
+    rng = np.random.default_rng(95 + precision)
+    B, N, T = 1024, 65536, 256
+    x = rng.standard_normal((B, N)).astype(np.float32)
+    n = np.arange(T) - (T - 1) / 2.0
+    h = np.zeros((B, T), np.float32)
+    for r in range(B):
+        fc = rng.uniform(0.05, 0.45)
+        w = fc * np.sinc(fc * n) * np.hamming(T)
+        h[r] = (w / w.sum())[::-1]
+    y = host(D.fir(dev(x), dev(h), T, nch=1, precision=precision))
+    rows = sample_rows(rng, B, 16)
+    y64 = oracle.fir_f64(x[rows], h[rows], T, nch=1)
+    err = np.max(np.abs(y[rows].astype(np.float64) - y64), axis=1) / np.max(np.abs(y64), axis=1)
+    assert np.max(err) <= tol, float(np.max(err))
+
+
+def test_biquad_full_size():
+    """DF2 cascade 4096 ch x 8192 x 4 stages, shared coefficients, zero state: outputs and
+    final states within 1e-4 relative of FP64 on 64 sampled channels."""
+    rng = np.random.default_rng(97)
+    N, C, S = 8192, 4096, 4
+    x = rng.standard_normal((N, C)).astype(np.float32)
+    nat = np.zeros((1, S, 5))
+    for s in range(S):
+        r, th, ph = rng.uniform(0.5, 0.95), rng.uniform(0, np.pi), rng.uniform(0, np.pi)
+        bb = np.array([1.0, -2 * np.cos(ph), 1.0])
+        aa = np.array([1.0, -2 * r * np.cos(th), r * r])
+        z = np.exp(-1j * th * np.arange(3))
+        g = 1.0 / max(abs(np.dot(bb, z) / np.dot(aa, z)), 1e-12)
+        nat[0, s] = [g * bb[0], g * bb[1], g * bb[2], aa[1], aa[2]]
+    nat = nat.reshape(1, S * 5).astype(np.float32)
+    opt, _ = D.opt_coefficients(nat, D.DF2, 0, C)
+    sd = dev(np.zeros((2 * S, C), np.float32))
+    y = host(D.cascade_biquad(dev(x), dev(opt), sd, form=D.DF2, nch=0))
+    cols = sample_rows(rng, C, 64)
+    s64 = np.zeros((2 * S, len(cols)), np.float64)
+    y64 = oracle.biquad_f64(D.DF2, x[:, cols], nat, s64, nch=0)
+    err = np.max(np.abs(y[:, cols].astype(np.float64) - y64), axis=0) / np.max(np.abs(y64), axis=0)
+    assert np.max(err) <= 1e-4, float(np.max(err))
+    st = host(sd)[:, cols].astype(np.float64)
+    assert np.max(np.abs(st - s64)) <= 1e-4 * max(1.0, float(np.max(np.abs(s64))))
