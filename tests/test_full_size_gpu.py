@@ -8,7 +8,8 @@ sampled channels for the floating-point paths.
 
 Configurations: int8 / int16 FIR 4096 ch x 16384 samples, 128 shared taps (Q mode with
 shift 7 / 15, and the natural-C wrap); FP32 FIR 1024 ch x 65536 samples, 256 taps per
-channel (plain and split-BF16); DF2 cascade 4096 ch x 8192 samples x 4 stages.
+channel (plain and split-BF16); DF2 cascade 4096 ch x 8192 samples x 4 stages; the
+filter-bank training step's data (2048 ragged channels, forward and adjoint).
 """
 import numpy as np
 import pytest
@@ -100,3 +101,50 @@ def test_biquad_full_size():
     assert np.max(err) <= 1e-4, float(np.max(err))
     st = host(sd)[:, cols].astype(np.float64)
     assert np.max(np.abs(st - s64)) <= 1e-4 * max(1.0, float(np.max(np.abs(s64))))
+
+
+def test_filter_bank_full_size():
+    """The filter-bank benchmark's own data (2048 channels, lengths log-uniform in
+    [256, 262144], about 77 M samples; taps 32-512; 2-8 stages, pole radius up to 0.98):
+    forward and adjoint of the whole bank on the GPU; y and the input, tap and
+    coefficient gradients within 1e-4 of each channel's peak against the FP64
+    restatement on six channels, the longest among them."""
+    import bench
+    from c7x_dsplib_b200.filterbank import RaggedFilterBank
+    from filterbank_ref import channel_adjoint, channel_forward
+
+    wl = bench.FilterBankWorkload()
+    L, T, S = wl.lengths, wl.taps, wl.stages
+    rng = np.random.default_rng(98)
+    gy = rng.standard_normal(wl.samples).astype(np.float32)
+    xo = np.concatenate([[0], np.cumsum(L)]).astype(np.int64)
+    ho = np.concatenate([[0], np.cumsum(T)]).astype(np.int64)
+    co = np.concatenate([[0], np.cumsum(5 * S)]).astype(np.int64)
+    for k in range(wl.C):  # the tail samples past each channel's valid outputs carry no gradient
+        gy[xo[k] + L[k] - T[k] + 1:xo[k + 1]] = 0.0
+    bank = RaggedFilterBank(L, T, S)
+    xt, ht, ct, gyt = dev(wl.x), dev(wl.h), dev(wl.c), dev(gy)
+    y = torch.empty(bank.sizes[0], device="cuda")
+    work = torch.empty(bank.sizes[3], device="cuda")
+    bank.forward_raw(xt, ht, ct, y, work)
+    gx, gh, gc = torch.empty_like(xt), torch.empty_like(ht), torch.empty_like(ct)
+    scratch = torch.empty(bank.sizes[4], device="cuda")
+    bank.backward_raw(xt, ht, ct, work, gyt, gx, gh, gc, scratch)
+    y, gx, gh, gc = (host(t).astype(np.float64) for t in (y, gx, gh, gc))
+
+    def rel(got, want):
+        return float(np.max(np.abs(got - want)) / max(float(np.max(np.abs(want))), 1e-30))
+
+    chans = [int(np.argmax(L))] + [int(k) for k in rng.choice(wl.C, size=5, replace=False)]
+    for k in chans:
+        xs = wl.x[xo[k]:xo[k + 1]].astype(np.float64)
+        hs = wl.h[ho[k]:ho[k + 1]].astype(np.float64)
+        cs = wl.c[co[k]:co[k + 1]].astype(np.float64)
+        n = L[k] - T[k] + 1
+        y64, _ = channel_forward(xs, hs, cs)
+        gx64, gh64, gc64 = channel_adjoint(xs, hs, cs, gy[xo[k]:xo[k] + n].astype(np.float64))
+        what = (k, int(L[k]), int(T[k]), int(S[k]))
+        assert rel(y[xo[k]:xo[k] + n], y64) <= 1e-4, what
+        assert rel(gx[xo[k]:xo[k + 1]], gx64) <= 1e-4, what
+        assert rel(gh[ho[k]:ho[k + 1]], gh64) <= 1e-4, what
+        assert rel(gc[co[k]:co[k + 1]], gc64.reshape(-1)) <= 1e-4, what
