@@ -222,8 +222,10 @@ class _Handle:
         raw = getattr(stream, "cuda_stream", stream)
         return lib().DSPLIB_gpu_setStream(self.h, raw or None)
 
-    def set_async(self, on: bool):
-        return lib().DSPLIB_gpu_setAsync(self.h, int(bool(on)))
+    def set_async(self, level):
+        """False / 0: exec returns complete; True / 1: returns once queued (device buffers);
+        2: returns once queued also with page-locked host buffers used in place."""
+        return lib().DSPLIB_gpu_setAsync(self.h, int(level))
 
     def _check(self, what, st):
         if st != SUCCESS:

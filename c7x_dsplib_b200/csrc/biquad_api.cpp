@@ -396,7 +396,8 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_exec(DSPLIB_kernelHandle handle,
          return cudaFail(hc, e, "pipeline join");
    }
    if ((e = regionOut(rst, s)) != cudaSuccess) return cudaFail(hc, e, "copy state");
-   if (!hc->async || rin.onHost || rout.onHost || rst.onHost || rc.onHost) {
+   if (mustSync(hc, rin.staged || rout.staged || rst.staged || rc.staged,
+                rin.onHost || rout.onHost || rst.onHost || rc.onHost)) {
       if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, "biquad execution");
    }
    return DSPLIB_SUCCESS;

@@ -112,6 +112,15 @@ struct Region {
    size_t bytes() const { return height ? (height - 1) * pitch + width : 0; }
 };
 
+// Whether exec must synchronize its stream before returning: always in the synchronous
+// mode; whenever the per-thread staging buffers hold part of the call (the next call may
+// reuse them); and for host buffers used in place unless the caller asked for asynchronous
+// completion of those too (async level 2).
+inline bool mustSync(const HandleCommon *hc, bool staged, bool onHost)
+{
+   return !hc->async || staged || (onHost && hc->async < 2);
+}
+
 // Prepare a region: device pointers, and (zeroCopy regions) pinned host buffers
 // of at most kZeroCopyMaxBytes (of any size for streamed regions), are used in
 // place through their mapped addresses; other host pointers are

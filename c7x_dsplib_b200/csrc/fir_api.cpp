@@ -244,7 +244,7 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
       if ((e = cudaEventRecord(pc->done, pc->out)) != cudaSuccess || (e = cudaStreamWaitEvent(s, pc->done, 0)))
          return cudaFail(hc, e, "pipeline join");
    }
-   if (!hc->async || rin.staged || rf.staged || rout.staged) {
+   if (mustSync(hc, rin.staged || rf.staged || rout.staged, rin.onHost || rf.onHost || rout.onHost)) {
       if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, "FIR execution");
       if ((kind == FIR_INT_WRAP_TC || kind == FIR_INT_Q_TC || kind == FIR_F32_BF16X3) && firTcErrorFlag(true) != 0) {
          setError(hc, "tensor-core FIR: a bounded wait for MMA completion expired; outputs are incomplete");

@@ -105,7 +105,9 @@ DSPLIB_STATUS DSPLIB_gpu_firStreamExec(DSPLIB_gpu_firStream stream, const void *
    if (st != DSPLIB_SUCCESS) return st;
    if (hb && (e = cudaMemcpy2DAsync(s->hist, hb, win + nb, wb, hb, s->channels, cudaMemcpyDeviceToDevice, cs)))
       return cudaFail(hc, e, "stream: save history");
-   if (!hc->async && (e = cudaStreamSynchronize(cs))) return cudaFail(hc, e, "stream: execution");
+   // a host block is copied in asynchronously: complete before returning unless async level 2
+   if (mustSync(hc, false, !isDevicePtr(pIn)) && (e = cudaStreamSynchronize(cs)))
+      return cudaFail(hc, e, "stream: execution");
    return DSPLIB_SUCCESS;
 }
 

@@ -101,7 +101,7 @@ DSPLIB_STATUS layoutExec(DSPLIB_kernelHandle handle, void *pIn, void *pOut, uint
    TransposeLaunch a{rin.dev, rout.dev, W, H, sInE, (long long) p->strideOut, elt};
    if ((e = launchTranspose(a, s)) != cudaSuccess) return cudaFail(hc, e, "transpose kernel");
    if ((e = regionOut(rout, s)) != cudaSuccess) return cudaFail(hc, e, "copy output");
-   if ((!hc->async || rin.staged || rout.staged) && (e = cudaStreamSynchronize(s)) != cudaSuccess)
+   if (mustSync(hc, rin.staged || rout.staged, rin.onHost || rout.onHost) && (e = cudaStreamSynchronize(s)) != cudaSuccess)
       return cudaFail(hc, e, "transpose execution");
    return DSPLIB_SUCCESS;
 }
@@ -300,7 +300,7 @@ DSPLIB_STATUS DSPLIB_addNCh_exec(DSPLIB_kernelHandle handle, void *pIn, void *pO
    AddNChLaunch a{rin.dev, rout.dev, S, C, (int) L, sY, sZ, C > 1 ? sO : S, p->dataType == DSPLIB_FLOAT64};
    if ((e = launchAddNCh(a, s)) != cudaSuccess) return cudaFail(hc, e, "addNCh kernel");
    if ((e = regionOut(rout, s)) != cudaSuccess) return cudaFail(hc, e, "copy output");
-   if ((!hc->async || rin.staged || rout.staged) && (e = cudaStreamSynchronize(s)) != cudaSuccess)
+   if (mustSync(hc, rin.staged || rout.staged, rin.onHost || rout.onHost) && (e = cudaStreamSynchronize(s)) != cudaSuccess)
       return cudaFail(hc, e, "addNCh execution");
    return DSPLIB_SUCCESS;
 }

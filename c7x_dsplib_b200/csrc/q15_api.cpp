@@ -71,7 +71,7 @@ DSPLIB_STATUS convertExec(HandleCommon *hc, void *pIn, size_t eltIn, void *pOut,
    if (!in.staged && !out.staged) {
       if ((e = launch(in.dev, out.dev, n, s)) != cudaSuccess) return cudaFail(hc, e, what);
       const bool hostSide = in.dev != in.host || out.dev != out.host;
-      if ((!hc->async || hostSide) && (e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, what);
+      if (mustSync(hc, false, hostSide) && (e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, what);
       return DSPLIB_SUCCESS;
    }
    const size_t inBytes = (size_t) n * eltIn, outBytes = (size_t) n * eltOut;

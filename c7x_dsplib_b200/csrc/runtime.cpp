@@ -188,7 +188,7 @@ DSPLIB_STATUS DSPLIB_gpu_setAsync(DSPLIB_kernelHandle handle, int32_t async)
 {
    HandleCommon *c = common(handle);
    if (!c) return DSPLIB_ERR_NULL_POINTER;
-   c->async = async ? 1 : 0;
+   c->async = async <= 0 ? 0 : (async >= 2 ? 2 : 1);
    return DSPLIB_SUCCESS;
 }
 

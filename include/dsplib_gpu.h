@@ -19,9 +19,15 @@ extern "C" {
  *  (NULL = the legacy default stream, the default). */
 DSPLIB_STATUS DSPLIB_gpu_setStream(DSPLIB_kernelHandle handle, void *cudaStream);
 
-/** async = 1: exec returns once the work is queued on the handle's stream
- *  (device buffers only; host buffers always complete before return).
- *  async = 0 (default): exec returns after the results are written. */
+/** async = 0 (default): exec returns after the results are written.
+ *  async = 1: exec returns once the work is queued on the handle's stream when every
+ *  buffer is device memory; calls with host buffers complete before returning.
+ *  async = 2: as 1, and also when host buffers are page-locked and read or written in
+ *  place by the kernels (no staging copy): exec returns once queued and the caller
+ *  synchronizes the handle's stream before touching those buffers.  Independent calls
+ *  on several handles and streams then overlap their PCIe reads, kernels and writes.
+ *  Calls that stage host data through the library's per-thread buffers (pageable
+ *  memory, pipelined copies) still complete before returning. */
 DSPLIB_STATUS DSPLIB_gpu_setAsync(DSPLIB_kernelHandle handle, int32_t async);
 
 /** Text of the last failure recorded on this handle ("" when none). */

@@ -368,8 +368,10 @@ def test_opt_pinned_host_buffers_read_in_place(form):
     want = host(D.cascade_biquad(dev(x), dev(opt), sd, form=form, nch=0))
     hx, hy = torch.from_numpy(x).pin_memory(), torch.zeros(N, C).pin_memory()
     hs, hc = torch.from_numpy(st0.copy()).pin_memory(), torch.from_numpy(opt).pin_memory()
+    args, pin, pout, pvar, _, popt = D.biquad_descs(C, N, S, form, 0)
     h = D.BiquadHandle()
-    h.set_async(True)
+    assert h.init(args, pin, popt, pvar, pout) == D.SUCCESS
+    assert h.set_async(True) == D.SUCCESS  # settings apply after the first init
     D.cascade_biquad(hx, hc, hs, form=form, nch=0, out=hy, handle=h)
     assert np.array_equal(hy.numpy(), want)
     assert np.array_equal(hs.numpy(), host(sd))
@@ -394,8 +396,10 @@ def test_opt_large_host_signals(form, C, pinned, in_place):
     if pinned:
         hx, hs, hc = hx.pin_memory(), hs.pin_memory(), hc.pin_memory()
     hy = hx if in_place else (torch.zeros(N, C).pin_memory() if pinned else torch.zeros(N, C))
+    args, pin, pout, pvar, _, popt = D.biquad_descs(C, N, S, form, 0)
     h = D.BiquadHandle()
-    h.set_async(True)
+    assert h.init(args, pin, popt, pvar, pout) == D.SUCCESS
+    assert h.set_async(True) == D.SUCCESS
     D.cascade_biquad(hx, hc, hs, form=form, nch=0, out=hy, handle=h)
     y32, st32, y64, _ = oracle_run(form, x, nat, st0, 0)
     if form != D.TIF:
@@ -422,3 +426,34 @@ def test_natc_host_signals_pipelined_bitexact(form):
     D.cascade_biquad(hx, hn, hs, form=form, nch=1, func_style=D.NATC, out=hy)
     assert np.array_equal(hy.numpy(), want)
     assert np.array_equal(hs.numpy(), s_ref)
+
+
+def test_opt_async_level2_pinned_calls_overlap():
+    """DSPLIB_gpu_setAsync(h, 2): calls on page-locked host buffers read and written in place
+    return once queued.  Three handles on three streams filter independent signals
+    concurrently; once each stream is synchronized, every output and final state equals the
+    synchronous call's."""
+    rng = np.random.default_rng(71)
+    N, C, S = 8192, 32, 4
+    nat = stable_sections(rng, 1, S)
+    opt, _ = D.opt_coefficients(nat, D.DF2, 0, C)
+    hc = torch.from_numpy(opt).pin_memory()
+    runs = []
+    for k in range(3):
+        x = rng.standard_normal((N, C)).astype(np.float32)
+        st0 = (rng.standard_normal((2 * S, C)) * 0.1).astype(np.float32)
+        sd = dev(st0)
+        want = host(D.cascade_biquad(dev(x), dev(opt), sd, form=D.DF2, nch=0))
+        args, pin, pout, pvar, _, popt = D.biquad_descs(C, N, S, D.DF2, 0)
+        h, stream = D.BiquadHandle(), torch.cuda.Stream()
+        assert h.init(args, pin, popt, pvar, pout) == D.SUCCESS
+        assert h.set_stream(stream) == D.SUCCESS and h.set_async(2) == D.SUCCESS
+        hx, hy = torch.from_numpy(x).pin_memory(), torch.zeros(N, C).pin_memory()
+        hs = torch.from_numpy(st0.copy()).pin_memory()
+        runs.append((h, stream, hx, hy, hs, want, host(sd)))
+    for h, stream, hx, hy, hs, _, _ in runs:
+        assert h.exec(hx, hc, hs, hy) == D.SUCCESS
+    for h, stream, hx, hy, hs, want, st_want in runs:
+        stream.synchronize()
+        assert np.array_equal(hy.numpy(), want)
+        assert np.array_equal(hs.numpy(), st_want)

@@ -212,6 +212,25 @@ def test_transpose_large_and_host_buffers():
 
 
 @pytest.mark.gpu
+def test_async_level_one_completes_with_pinned_host_buffers():
+    """DSPLIB_gpu_setAsync(h, 1) applies to device buffers only: page-locked host buffers,
+    which the kernel reads and writes in place, hold the result when exec returns."""
+    torch = _torch()
+    rng = np.random.default_rng(8)
+    W, H = 2, 1 << 21
+    x = rng.standard_normal(W * H).astype(np.float32)
+    want = np.zeros(W * H, np.float32)
+    oracle.transpose(x, W, H, W * 4, H * 4, want)
+    hx, hy = torch.from_numpy(x).pin_memory(), torch.zeros(W * H).pin_memory()
+    h = D.LayoutHandle("DSPLIB_interleave")
+    args = D.StyleInitArgs(funcStyle=D.OPTIMIZED)
+    assert h.init(args, D.bp(D.FLOAT32, W, H, W * 4), D.bp(D.FLOAT32, H, W, H * 4)) == D.SUCCESS
+    assert h.set_async(1) == D.SUCCESS
+    assert h.exec(hx, hy) == D.SUCCESS
+    assert np.array_equal(hy.numpy(), want)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("style", [D.NATC, D.OPTIMIZED])
 def test_addnch_golden_cases_on_device(golden, style):
     torch = _torch()
