@@ -16,7 +16,9 @@ extern "C" {
 #endif
 
 /** Launch this handle's kernels (and staging copies) on the given cudaStream_t
- *  (NULL = the legacy default stream, the default). */
+ *  (NULL = the legacy default stream, the default).  This and DSPLIB_gpu_setAsync apply to
+ *  an initialised handle (DSPLIB_ERR_NULL_POINTER before its first init) and persist across
+ *  later inits of the same handle. */
 DSPLIB_STATUS DSPLIB_gpu_setStream(DSPLIB_kernelHandle handle, void *cudaStream);
 
 /** async = 0 (default): exec returns after the results are written.
