@@ -165,7 +165,9 @@ class BiquadWorkload(Workload):
         # completion on page-locked buffers (DSPLIB_gpu_setAsync level 2): one call's PCIe
         # reads overlap another's kernel and writes.  Each call still reads its input and
         # writes its output and state across PCIe; a slot is reused once its call completed.
-        self.e2e_in_flight = 3
+        # Signals of 4 MB or more go through the library's staged block pipeline, whose calls
+        # complete before returning, so they run one at a time.
+        self.e2e_in_flight = 3 if (self.C >= 32 and self.x.nbytes < (4 << 20)) else 1
         self.slots = []
         for _ in range(self.e2e_in_flight):
             h, stream = D.BiquadHandle(), torch.cuda.Stream()
