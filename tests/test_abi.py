@@ -268,3 +268,18 @@ def test_release_handle():
     x = np.zeros(8, np.float32)
     assert h.exec(x, x, x) == D.ERR_FAILURE
     assert D.lib().DSPLIB_gpu_releaseHandle(None) == D.ERR_NULL_POINTER
+
+
+def test_stream_and_async_settings_apply_after_init_and_persist():
+    """DSPLIB_gpu_setStream / setAsync need an initialised handle (NULL_POINTER before the
+    first init); every async level is accepted afterwards and a later init keeps it."""
+    args, pin, pout, pvar, _, popt = D.biquad_descs(32, 64, 2, D.DF2, 0)
+    h = D.BiquadHandle()
+    assert h.set_async(2) == D.ERR_NULL_POINTER
+    assert h.set_stream(None) == D.ERR_NULL_POINTER
+    assert h.init(args, pin, popt, pvar, pout) == D.SUCCESS
+    for level in (0, 1, 2, True, False):
+        assert h.set_async(level) == D.SUCCESS
+    assert h.set_stream(None) == D.SUCCESS
+    assert h.init(args, pin, popt, pvar, pout) == D.SUCCESS  # re-init keeps the handle's settings
+    assert h.set_async(2) == D.SUCCESS
