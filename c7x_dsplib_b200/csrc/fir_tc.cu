@@ -74,6 +74,20 @@ template <int QMODE> __device__ __forceinline__ int8_t outStage8(int acc, int sh
    return (int8_t) max(-128, min(127, acc));
 }
 
+// Four int8 Q-mode outputs (round half up, shift, saturate) packed into one word, byte k =
+// output k: two saturating pack conversions instead of a clamp per output and byte moves.
+__device__ __forceinline__ uint32_t outStage8x4(int v0, int v1, int v2, int v3, int shift)
+{
+   if (shift > 0) {
+      const int r = 1 << (shift - 1);
+      v0 = (v0 + r) >> shift, v1 = (v1 + r) >> shift, v2 = (v2 + r) >> shift, v3 = (v3 + r) >> shift;
+   }
+   uint32_t hi, d;
+   asm("cvt.pack.sat.s8.s32.b32 %0, %1, %2, 0;" : "=r"(hi) : "r"(v3), "r"(v2));
+   asm("cvt.pack.sat.s8.s32.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(v1), "r"(v0), "r"(hi));
+   return d;
+}
+
 template <typename T, int QMODE>
 __device__ __forceinline__ T outStage(long long acc, int shift)
 {
@@ -353,11 +367,19 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 2 ? 6 : 8) fir_int_tc_k
             tc::tmemWaitLoad();
             const int row = warp * 32 + lane;
             __align__(16) T out[16];
+            if (!SPLIT && QMODE) {
+               uint4 w;
+               w.x = outStage8x4((int) acc[0][0], (int) acc[0][1], (int) acc[0][2], (int) acc[0][3], a.shift);
+               w.y = outStage8x4((int) acc[0][4], (int) acc[0][5], (int) acc[0][6], (int) acc[0][7], a.shift);
+               w.z = outStage8x4((int) acc[0][8], (int) acc[0][9], (int) acc[0][10], (int) acc[0][11], a.shift);
+               w.w = outStage8x4((int) acc[0][12], (int) acc[0][13], (int) acc[0][14], (int) acc[0][15], a.shift);
+               *(uint4 *) &out[0] = w;
+            }
 #pragma unroll
             for (int b = 0; b < 16; b++) {
                long long v;
                if (!SPLIT) {
-                  out[b] = (T) outStage8<QMODE>((int) acc[0][b], a.shift);
+                  if (!QMODE) out[b] = (T) outStage8<QMODE>((int) acc[0][b], a.shift);
                   continue;
                }
                if (QMODE) {
