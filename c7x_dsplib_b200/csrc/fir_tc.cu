@@ -88,6 +88,22 @@ __device__ __forceinline__ uint32_t outStage8x4(int v0, int v1, int v2, int v3, 
    return d;
 }
 
+// Two int16 Q-mode outputs packed into one word (low half = v0): round half up and shift in
+// 64 bits, narrow to 32 bits with saturation, then one saturating pack conversion.
+__device__ __forceinline__ uint32_t outStage16x2(long long v0, long long v1, int shift)
+{
+   if (shift > 0) {
+      const long long r = 1LL << (shift - 1);
+      v0 = (v0 + r) >> shift, v1 = (v1 + r) >> shift;
+   }
+   int w0, w1;
+   uint32_t d;
+   asm("cvt.sat.s32.s64 %0, %1;" : "=r"(w0) : "l"(v0));
+   asm("cvt.sat.s32.s64 %0, %1;" : "=r"(w1) : "l"(v1));
+   asm("cvt.pack.sat.s16.s32 %0, %1, %2;" : "=r"(d) : "r"(w1), "r"(w0));
+   return d;
+}
+
 template <typename T, int QMODE>
 __device__ __forceinline__ T outStage(long long acc, int shift)
 {
@@ -367,6 +383,19 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 2 ? 6 : 8) fir_int_tc_k
             tc::tmemWaitLoad();
             const int row = warp * 32 + lane;
             __align__(16) T out[16];
+            if (SPLIT && QMODE) {
+               uint32_t w[8];
+#pragma unroll
+               for (int b = 0; b < 16; b += 2) {
+                  const long long v0 = ((long long) (int) acc[0][b] << 16) + ((long long) (int) acc[1][b] << 8) +
+                                       (long long) (int) acc[2][b];
+                  const long long v1 = ((long long) (int) acc[0][b + 1] << 16) +
+                                       ((long long) (int) acc[1][b + 1] << 8) + (long long) (int) acc[2][b + 1];
+                  w[b / 2] = outStage16x2(v0, v1, a.shift);
+               }
+               *(uint4 *) &out[0] = make_uint4(w[0], w[1], w[2], w[3]);
+               *(uint4 *) &out[8] = make_uint4(w[4], w[5], w[6], w[7]);
+            }
             if (!SPLIT && QMODE) {
                uint4 w;
                w.x = outStage8x4((int) acc[0][0], (int) acc[0][1], (int) acc[0][2], (int) acc[0][3], a.shift);
@@ -382,13 +411,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 2 ? 6 : 8) fir_int_tc_k
                   if (!QMODE) out[b] = (T) outStage8<QMODE>((int) acc[0][b], a.shift);
                   continue;
                }
-               if (QMODE) {
-                  v = ((long long) (int) acc[0][b] << 16) + ((long long) (int) acc[1][b] << 8) +
-                      (long long) (int) acc[2][b];
-               }
-               else {
-                  v = (long long) (int) (((uint32_t) acc[1][b] << 8) + (uint32_t) acc[2][b]);
-               }
+               if (QMODE) continue; // packed above
+               v = (long long) (int) (((uint32_t) acc[1][b] << 8) + (uint32_t) acc[2][b]);
                out[b] = outStage<T, QMODE>(v, a.shift);
             }
             int4 *os = (int4 *) (ostage + row * kPhases);
