@@ -379,21 +379,21 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_exec(DSPLIB_kernelHandle handle,
                            cudaMemcpyHostToDevice, pc->in)) != cudaSuccess ||
              (e = cudaEventRecord(pc->copied[b], pc->in)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->comp, pc->copied[b], 0)) != cudaSuccess)
-            return cudaFail(hc, e, "copy input block");
+            return pipeFail(hc, pc, e, "copy input block");
          BiquadLaunch blk = a;
          blk.x = a.x + (size_t) r0 * a.inPitch;
          blk.y = a.y + (size_t) r0 * a.outPitch;
          blk.N = rows;
-         if ((e = launch(blk, pc->comp)) != cudaSuccess) return cudaFail(hc, e, "biquad kernel launch");
+         if ((e = launch(blk, pc->comp)) != cudaSuccess) return pipeFail(hc, pc, e, "biquad kernel launch");
          if ((e = cudaEventRecord(pc->computed[b], pc->comp)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->out, pc->computed[b], 0)) != cudaSuccess ||
              (e = copyRows((char *) rout.host + outOff, (const char *) rout.dev + outOff, rout.width, rows,
                            rout.pitch, cudaMemcpyDeviceToHost, pc->out)) != cudaSuccess)
-            return cudaFail(hc, e, "copy output block");
+            return pipeFail(hc, pc, e, "copy output block");
       }
       // the state is final once the last block's kernel has run (the out stream waited for it)
       if ((e = cudaEventRecord(pc->done, pc->out)) != cudaSuccess || (e = cudaStreamWaitEvent(s, pc->done, 0)))
-         return cudaFail(hc, e, "pipeline join");
+         return pipeFail(hc, pc, e, "pipeline join");
    }
    if ((e = regionOut(rst, s)) != cudaSuccess) return cudaFail(hc, e, "copy state");
    if (mustSync(hc, rin.staged || rout.staged || rst.staged || rc.staged,

@@ -155,6 +155,9 @@ struct PipeContext {
    cudaEvent_t copied[kPipeMaxBlocks] = {}, computed[kPipeMaxBlocks] = {};
 };
 PipeContext *pipeContext();
+// A failure inside a pipeline: let the copies and kernels already queued on its streams
+// finish (they read and write the caller's host buffers) before reporting it.
+DSPLIB_STATUS pipeFail(HandleCommon *h, PipeContext *pc, cudaError_t e, const char *what);
 
 // ---------------------------------------------------------------- kernels
 

@@ -228,21 +228,21 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
                            cudaMemcpyHostToDevice, pc->in)) != cudaSuccess ||
              (e = cudaEventRecord(pc->copied[b], pc->in)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->comp, pc->copied[b], 0)) != cudaSuccess)
-            return cudaFail(hc, e, "copy input block");
+            return pipeFail(hc, pc, e, "copy input block");
          FirLaunch blk = a;
          blk.x = (const char *) a.x + inOff;
          blk.y = (char *) a.y + outOff;
          blk.h = (const char *) a.h + (nch ? (size_t) r0 * filtPitch * elt : 0);
          blk.batch = rows;
-         if ((e = launchFir(blk, kind, pc->comp)) != cudaSuccess) return cudaFail(hc, e, "FIR kernel launch");
+         if ((e = launchFir(blk, kind, pc->comp)) != cudaSuccess) return pipeFail(hc, pc, e, "FIR kernel launch");
          if ((e = cudaEventRecord(pc->computed[b], pc->comp)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->out, pc->computed[b], 0)) != cudaSuccess ||
              (e = copyRows((char *) rout.host + outOff, (const char *) rout.dev + outOff, rout.width, rows,
                            rout.pitch, cudaMemcpyDeviceToHost, pc->out)) != cudaSuccess)
-            return cudaFail(hc, e, "copy output block");
+            return pipeFail(hc, pc, e, "copy output block");
       }
       if ((e = cudaEventRecord(pc->done, pc->out)) != cudaSuccess || (e = cudaStreamWaitEvent(s, pc->done, 0)))
-         return cudaFail(hc, e, "pipeline join");
+         return pipeFail(hc, pc, e, "pipeline join");
    }
    if (mustSync(hc, rin.staged || rf.staged || rout.staged, rin.onHost || rf.onHost || rout.onHost)) {
       if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, "FIR execution");

@@ -101,20 +101,20 @@ DSPLIB_STATUS convertExec(HandleCommon *hc, void *pIn, size_t eltIn, void *pOut,
          char *di = (char *) in.dev + e0 * eltIn, *dout = (char *) out.dev + e0 * eltOut;
          if (in.staged &&
              (e = cudaMemcpyAsync(di, (char *) in.host + e0 * eltIn, cnt * eltIn, cudaMemcpyHostToDevice, pc->in)))
-            return cudaFail(hc, e, "copy input block");
+            return pipeFail(hc, pc, e, "copy input block");
          if ((e = cudaEventRecord(pc->copied[b], pc->in)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->comp, pc->copied[b], 0)) != cudaSuccess)
-            return cudaFail(hc, e, "pipeline");
-         if ((e = launch(di, dout, cnt, pc->comp)) != cudaSuccess) return cudaFail(hc, e, what);
+            return pipeFail(hc, pc, e, "pipeline");
+         if ((e = launch(di, dout, cnt, pc->comp)) != cudaSuccess) return pipeFail(hc, pc, e, what);
          if ((e = cudaEventRecord(pc->computed[b], pc->comp)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->out, pc->computed[b], 0)) != cudaSuccess)
-            return cudaFail(hc, e, "pipeline");
+            return pipeFail(hc, pc, e, "pipeline");
          if (out.staged && (e = cudaMemcpyAsync((char *) out.host + e0 * eltOut, dout, cnt * eltOut,
                                                 cudaMemcpyDeviceToHost, pc->out)))
-            return cudaFail(hc, e, "copy output block");
+            return pipeFail(hc, pc, e, "copy output block");
       }
       if ((e = cudaEventRecord(pc->done, pc->out)) != cudaSuccess || (e = cudaStreamWaitEvent(s, pc->done, 0)))
-         return cudaFail(hc, e, "pipeline join");
+         return pipeFail(hc, pc, e, "pipeline join");
    }
    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, what);
    return DSPLIB_SUCCESS;

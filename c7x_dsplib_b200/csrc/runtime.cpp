@@ -145,6 +145,16 @@ PipeContext *pipeContext()
    return &c;
 }
 
+DSPLIB_STATUS pipeFail(HandleCommon *h, PipeContext *pc, cudaError_t e, const char *what)
+{
+   if (pc) {
+      (void) cudaStreamSynchronize(pc->in);
+      (void) cudaStreamSynchronize(pc->comp);
+      (void) cudaStreamSynchronize(pc->out);
+   }
+   return cudaFail(h, e, what);
+}
+
 cudaError_t copyRows(void *dst, const void *src, size_t width, size_t rows, size_t pitch, cudaMemcpyKind kind,
                      cudaStream_t s)
 {
