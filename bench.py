@@ -3,20 +3,25 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
-Default workload (N = 1): the plain DSPLIB_cascadeBiquad fp32 configuration,
-32 channels x 8192 samples x 4 stages (DF2, OPTIMIZED path: chunked
-parallel-in-time scan), seeded synthetic coefficients: each stage a conjugate
-pole pair r ~ U[0.5, 0.95], theta ~ U[0, pi], a zero pair on the unit circle
-at phi ~ U[0, pi], gain normalised so |H(e^{j theta})| = 1; input N(0, 1);
-zero initial state.  Other workloads: the FIR configurations (see WORKLOADS).
+Default workload (N = 1): the batched, differentiable FIR -> cascaded-biquad
+filter bank the metric ("FIR+biquad Gsamples/s") is quoted on: 2048 channels of
+lengths log-uniform in [256, 262144] (75.4 M samples), FIR taps uniform in
+{32..512}, 2-8 DF2 stages (poles r <= 0.98), one training step = forward, MSE
+loss gradient against a fixed target bank's output and the adjoint w.r.t. the
+input, the taps and the biquad coefficients, replayed from one CUDA graph.
+Other workloads (--workload): the plain DSPLIB_cascadeBiquad configuration
+(32 channels x 8192 samples x 4 stages, and its 4096-channel scaled shape),
+the FIR configurations (int16 Q15, FP32 plain and split-BF16x3, int8 / int16
+tensor-core in Q mode and in the natural-C wrap mode) and the next-row kernels.
 
-One step = one exec call over the whole batch, inputs resident in HBM.  The
-batch is far smaller than L2, so L2 is flushed (256 MiB write) between steps,
-outside the CUDA events that time each step.  ``value`` = samples processed by
-all ranks / max-over-ranks device time.  ``e2e`` = the same metric through the
-C ABI with pinned host buffers (host->device and device->host copies inside
-the library call).  Multi-GPU: one process per GPU (torchrun), each rank runs
-its own channel block (no data-path collective), weak scaling.
+One step = one pass of the hot path over the whole batch, inputs resident in
+HBM.  L2 is flushed (256 MiB write) between steps, outside the CUDA events that
+time each step.  ``value`` = samples processed by all ranks / max-over-ranks
+device time.  ``e2e`` = the same metric through the library's public calls with
+page-locked host buffers (host->device copies of every input and device->host
+copies of every result inside the timed region).  Multi-GPU: one process per
+GPU (torchrun), each rank runs its own copy of the workload (no data-path
+collective), weak scaling.
 
 ``--impl reference`` times the reference's natural-C kernels (compiled from
 the reference sources into oracle/_ref) on the host cores with all threads,
@@ -120,7 +125,7 @@ class BiquadWorkload(Workload):
         rng = np.random.default_rng(seed)
         self.x = rng.standard_normal((N, C)).astype(np.float32)
         self.nat = biquad_coefficients(rng, 1, S)
-        self.opt, _ = D.opt_coefficients(self.nat, form, 0, C)
+        self.opt = None  # the OPT layout comes from the library's get_coefficients (setup_device)
         self.samples = N * C
         nv = 4 if form == 1 else 2
         self.alg_bytes = 4 * (2 * N * C) + 4 * 5 * S + 2 * 4 * (S * nv * C)
@@ -135,6 +140,8 @@ class BiquadWorkload(Workload):
     def setup_device(self, torch, func_style=None):
         D = self.D
         fs = D.OPTIMIZED if func_style is None else func_style
+        if self.opt is None:
+            self.opt, _ = D.opt_coefficients(self.nat, self.form, 0, self.C)
         self.xd = torch.from_numpy(self.x).cuda()
         self.yd = torch.zeros_like(self.xd)
         self.sd = torch.zeros((self.S * 2, self.C), device="cuda")
@@ -329,7 +336,17 @@ class FilterBankWorkload(Workload):
     MSE loss against a fixed target filter bank's output, adjoint w.r.t. input,
     taps and coefficients, captured in one CUDA graph.  2048 channels, lengths
     log-uniform in [256, 262144], taps uniform in {32..512} (N(0, 1/taps), at
-    most the channel length), 2-8 stages with poles of radius <= 0.98, input N(0, 1)."""
+    most the channel length), 2-8 stages with poles of radius <= 0.98, input N(0, 1).
+
+    Algorithmic work of one step (the roofline's numerator):
+      HBM     20 bytes per input sample: x in and y out (forward), target in and the
+              output gradient (loss), x and the gradient in and gx out (adjoint), FP32,
+              each touched once; activations a design keeps or recomputes are not counted.
+      tensor  6 T Lu flops per channel: the FIR forward, its input gradient and its taps
+              gradient, 2 T flops per output each.
+    The bound is whichever of the two takes longer at the measured peaks."""
+
+    BYTES_PER_SAMPLE = 20
 
     def __init__(self, C=2048, seed=5):
         import c7x_dsplib_b200 as D
@@ -348,14 +365,23 @@ class FilterBankWorkload(Workload):
         self.ht = np.concatenate([rng.standard_normal(T) / math.sqrt(T) for T in self.taps]).astype(np.float32)
         self.ct = np.concatenate([random_sections(rng, S).reshape(-1) for S in self.stages]).astype(np.float32)
         Lu = self.lengths - self.taps + 1
-        S = self.stages
-        # compulsory HBM bytes of one step with every stage output kept for the adjoint (FP32):
-        # forward x + (S + 2) Lu; loss 3 Lu; adjoint 6 S Lu + dx (Lu + L) + dh (L + Lu)
-        self.alg_bytes = int(4 * np.sum(3 * self.lengths + (7 * S + 7) * Lu))
-        self.alg_flops = float(np.sum(6.0 * self.taps * Lu))  # FIR forward, dx and dh multiply-adds x 2
-        self.bound = "hbm"
+        self.alg_bytes = self.BYTES_PER_SAMPLE * self.samples
+        self.alg_flops = float(np.sum(6.0 * self.taps * Lu))
+        hbm, bf16, _ = peaks()
+        t_hbm, t_tensor = self.alg_bytes / (hbm * 1e9), self.alg_flops / (bf16 * 1e12)
+        self.bound = "hbm" if t_hbm >= t_tensor else "tensor"
+        self.bound_times_ms = {"hbm": t_hbm * 1e3, "tensor": t_tensor * 1e3}
+        self.issued_flops = self._issued_tensor_flops()
         self.kernel = "fir_biquad_bank_step"
         self.launches_per_step = None
+
+    def _issued_tensor_flops(self):
+        """Tensor-core flops the split-BF16 kernels issue per step (Toeplitz inflation and
+        the hi/lo products included): 8 * K flops per output, K = round16(T + 63), for the
+        forward (Lu outputs), the input gradient (L outputs) and the taps gradient."""
+        K = ((self.taps + 63 + 15) // 16) * 16
+        Lu = self.lengths - self.taps + 1
+        return float(np.sum(8.0 * K * (Lu + self.lengths + Lu)))
 
     def config(self):
         return {"workload": self.name, "channels": self.C, "total_samples": self.samples,
@@ -374,12 +400,8 @@ class FilterBankWorkload(Workload):
         self.xd = torch.from_numpy(self.x).to(dev)
         self.hd = torch.from_numpy(self.h).to(dev)
         self.cd = torch.from_numpy(self.c).to(dev)
-        tgt = torch.empty(self.bank.sizes[0], device=dev)
-        work = torch.empty(self.bank.sizes[3], device=dev)
-        self.bank.forward_raw(self.xd, torch.from_numpy(self.ht).to(dev), torch.from_numpy(self.ct).to(dev), tgt,
-                              work)
-        del work
-        self.target = tgt
+        self.target = self.bank.apply(self.xd, torch.from_numpy(self.ht).to(dev),
+                                      torch.from_numpy(self.ct).to(dev)).detach()
         torch.cuda.synchronize()
         n0 = self.D.kernel_launch_count()
         self.replay, self.out = self.bank.graph_step(self.xd, self.hd, self.cd, self.target)
@@ -389,14 +411,39 @@ class FilterBankWorkload(Workload):
     def step(self):
         self.replay()
 
+    def phase_times(self, torch, reps=3):
+        """Event-timed C-ABI calls of one step, run eagerly (forward, loss, adjoint): median ms each."""
+        b, dev = self.bank, "cuda"
+        y = torch.empty(b.sizes[0], device=dev)
+        work = torch.empty(b.sizes[3], device=dev)
+        gy = torch.empty_like(y)
+        gx, gh, gc = torch.empty_like(self.xd), torch.empty_like(self.hd), torch.empty_like(self.cd)
+        scratch = torch.empty(b.sizes[4], device=dev)
+        loss = torch.empty(1, device=dev)
+        calls = {"forward": lambda: b.forward_raw(self.xd, self.hd, self.cd, y, work),
+                 "loss": lambda: b.mse_grad_raw(y, self.target, gy, loss, scratch),
+                 "adjoint": lambda: b.backward_raw(self.xd, self.hd, self.cd, work, gy, gx, gh, gc, scratch)}
+        times = {k: [] for k in calls}
+        s = torch.cuda.current_stream()
+        for _ in range(reps):
+            for k, f in calls.items():
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                f()
+                e1.record(s)
+                torch.cuda.synchronize()
+                times[k].append(e0.elapsed_time(e1))
+        return {k: statistics.median(v) for k, v in times.items()}
+
     def e2e_setup(self, torch):
+        # every input of the step from page-locked host memory, every result back
         self.hx = torch.from_numpy(self.x).pin_memory()
         self.htg = self.target.cpu().pin_memory()
-        self.h_loss = torch.empty(1).pin_memory()
-        self.h_gh = torch.empty(self.h.size).pin_memory()
-        self.h_gc = torch.empty(self.c.size).pin_memory()
-        self.h2d = self.hx.numel() * 4 + self.htg.numel() * 4
-        self.d2h = 4 + self.h_gh.numel() * 4 + self.h_gc.numel() * 4
+        self.hh = torch.from_numpy(self.h).pin_memory()
+        self.hc = torch.from_numpy(self.c).pin_memory()
+        self.h_out = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in self.out.items()}
+        self.h2d = 4 * (self.hx.numel() + self.htg.numel() + self.hh.numel() + self.hc.numel())
+        self.d2h = sum(4 * t.numel() for t in self.h_out.values())
 
     def e2e_step(self):
         import torch
@@ -404,10 +451,11 @@ class FilterBankWorkload(Workload):
         s = torch.cuda.current_stream()
         self.xd.copy_(self.hx, non_blocking=True)
         self.target.copy_(self.htg, non_blocking=True)
+        self.hd.copy_(self.hh, non_blocking=True)
+        self.cd.copy_(self.hc, non_blocking=True)
         self.replay()
-        self.h_loss.copy_(self.out["loss"], non_blocking=True)
-        self.h_gh.copy_(self.out["gtaps"], non_blocking=True)
-        self.h_gc.copy_(self.out["gcoefs"], non_blocking=True)
+        for k, t in self.h_out.items():
+            t.copy_(self.out[k], non_blocking=True)
         s.synchronize()
 
     def cpu_reference(self, threads, budget_s):
@@ -589,11 +637,18 @@ WORKLOADS = {
                                                          nch=0, qmode=True, shift=7, seed=4),
     "fir_int16_4096ch_16384_128taps": lambda: FirWorkload("fir_int16_4096ch_16384_128taps", np.int16, 4096, 16384,
                                                           128, nch=0, qmode=True, shift=15, seed=4),
+    # the natural-C wrap mode (modulo 2^bits, bit-exact to the reference _cn kernel)
+    "fir_int8_4096ch_16384_128taps_wrap": lambda: FirWorkload("fir_int8_4096ch_16384_128taps_wrap", np.int8, 4096,
+                                                              16384, 128, nch=0, qmode=False, seed=4),
+    "fir_int16_4096ch_16384_128taps_wrap": lambda: FirWorkload("fir_int16_4096ch_16384_128taps_wrap", np.int16,
+                                                               4096, 16384, 128, nch=0, qmode=False, seed=4),
+    "fir_int16_16ch_4096_64taps_wrap": lambda: FirWorkload("fir_int16_16ch_4096_64taps_wrap", np.int16, 16, 4096,
+                                                           64, nch=0, qmode=False, seed=1),
 }
 for _k, _n, _c in (("fltoq15", 64 << 20, 2), ("q15tofl", 64 << 20, 2), ("interleave", 16 << 20, 2),
                    ("deinterleave", 16 << 20, 2), ("addnch", 1 << 20, 16)):
     WORKLOADS[stream_name(_k, _n, _c, 12)] = (lambda k=_k, n=_n, c=_c: StreamWorkload(k, n, channels=c))
-DEFAULT = "biquad_32x8192x4"
+DEFAULT = "fir_biquad_bank_2048ch_ragged"
 
 
 # ----------------------------------------------------------- clocks
@@ -787,6 +842,16 @@ def main():
     roof["traffic"] = traffic
     roof["kernel"] = wl.kernel
     roof["median_launch_ms"] = kernel_ms
+    if isinstance(wl, FilterBankWorkload):
+        # a step is one graph of several kernels: both floors, the issued tensor work, and
+        # the event-timed C-ABI calls of an eager step (outside the timed region)
+        roof["algorithmic_bytes_per_launch"] = wl.alg_bytes
+        roof["algorithmic_flops_per_launch"] = wl.alg_flops
+        roof["floor_ms"] = {"hbm": wl.alg_bytes / (hbm * 1e9) * 1e3, "tensor": wl.alg_flops / (bf16 * 1e12) * 1e3}
+        roof["issued_tensor_flops_per_step"] = wl.issued_flops
+        roof["issued_tensor_tflops"] = wl.issued_flops / (kernel_ms * 1e-3) / 1e12
+        roof["kernel"] = f"{wl.kernel} ({wl.launches_per_step} launches in one CUDA graph)"
+        roof["phases_ms"] = wl.phase_times(torch)
 
     # end to end through the C ABI with pinned host buffers
     wl.e2e_setup(torch)

@@ -94,9 +94,10 @@ void countLaunch(int n = 1);
 // True when p is device-accessible global memory (device or managed allocation).
 bool isDevicePtr(const void *p);
 
-// Per-device, per-thread growable scratch used to stage host buffers.
+// Per-device, per-thread growable scratch used to stage host buffers, from the
+// device's stream-ordered pool (a buffer that grows is replaced in the order of s).
 // Returns nullptr on allocation failure.
-void *stagingBuffer(int slot, size_t bytes);
+void *stagingBuffer(int slot, size_t bytes, cudaStream_t s);
 
 // A strided 2-D region of a caller buffer: rows of width bytes, pitch bytes apart.
 struct Region {
@@ -184,6 +185,9 @@ enum FirKernelKind {
    FIR_INT_Q_TC = 5     // tcgen05 kind::i8 kernel, int8/int16, Q-mode output
 };
 
+// Largest InitArgs.shift the Q-mode output stages accept.
+constexpr int kFirMaxQShift = 62;
+
 cudaError_t launchFir(const FirLaunch &a, FirKernelKind kind, cudaStream_t s);
 
 // Q.15 conversions over n elements (any alignment; 16-byte aligned pointers take the
@@ -234,6 +238,8 @@ struct RaggedChan {
 constexpr int kFirBfTile = 8192;
 constexpr int kFirBfRunTiles = 4;
 constexpr int kFirBfMaxTaps = 512;
+// Device the plan was built on (-1 for a null plan).
+int raggedPlanDevice(DSPLIB_gpu_raggedPlan plan);
 cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *in,
                                   const float *taps, float *out, bool dx, int Tmax, cudaStream_t s);
 

@@ -167,6 +167,14 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
       return DSPLIB_ERR_INVALID_DIMENSION;
    }
 
+   // Q mode rounds with 2^(shift-1) and shifts a 64-bit (int32 data: 128-bit) accumulator:
+   // shifts beyond 62 have no defined result there.  The natural-C wrap mode ignores shift.
+   const bool qmode = !natc && p->dtype != DSPLIB_FLOAT32 && hc->firQMode;
+   if (qmode && ia.shift > kFirMaxQShift) {
+      setError(hc, "exec: Q-mode shift %u out of range (at most %d)", ia.shift, kFirMaxQShift);
+      return DSPLIB_ERR_INVALID_VALUE;
+   }
+
    FirKernelKind kind;
    if (natc) kind = FIR_NATC;
    else if (p->dtype == DSPLIB_FLOAT32)

@@ -476,7 +476,11 @@ template <typename T, int QMODE> cudaError_t launchIntTc(const FirLaunch &a, cud
    }
    const long long wave = (long long) (perSm > 0 ? perSm : 1) * sms;
    const int grid = (int) (items < wave ? items : wave);
-   fn<<<grid, kThreads, smem, s>>>(a, tpc);
+   FirLaunch k = a;
+   // int8: |acc| <= 2048 * 2^14 = 2^25, so every shift from 27 up rounds to zero, as 31
+   // (the largest the 32-bit output stage can take) does.
+   if (!SPLIT && k.shift > 31) k.shift = 31;
+   fn<<<grid, kThreads, smem, s>>>(k, tpc);
    countLaunch();
    return cudaGetLastError();
 }

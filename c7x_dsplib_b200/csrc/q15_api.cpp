@@ -75,8 +75,8 @@ DSPLIB_STATUS convertExec(HandleCommon *hc, void *pIn, size_t eltIn, void *pOut,
       return DSPLIB_SUCCESS;
    }
    const size_t inBytes = (size_t) n * eltIn, outBytes = (size_t) n * eltOut;
-   if (in.staged && !(in.dev = stagingBuffer(0, inBytes))) return cudaFail(hc, cudaErrorMemoryAllocation, "staging");
-   if (out.staged && !(out.dev = stagingBuffer(2, outBytes)))
+   if (in.staged && !(in.dev = stagingBuffer(0, inBytes, s))) return cudaFail(hc, cudaErrorMemoryAllocation, "staging");
+   if (out.staged && !(out.dev = stagingBuffer(2, outBytes, s)))
       return cudaFail(hc, cudaErrorMemoryAllocation, "staging");
    const size_t staged = (in.staged ? inBytes : 0) + (out.staged ? outBytes : 0);
    PipeContext *pc = staged >= kConvPipeMinBytes ? pipeContext() : nullptr;

@@ -469,6 +469,35 @@ static void freePlan(RaggedPlan *p)
    delete p;
 }
 
+// Makes the plan's device current for the duration of a call (and restores the
+// caller's device afterwards): the plan's tables and the kernels' scratch live there.
+class PlanDevice {
+ public:
+   explicit PlanDevice(const RaggedPlan *p)
+   {
+      ok_ = cudaGetDevice(&prev_) == cudaSuccess;
+      if (ok_ && prev_ != p->device) {
+         ok_ = cudaSetDevice(p->device) == cudaSuccess;
+         switched_ = ok_;
+      }
+   }
+   ~PlanDevice()
+   {
+      if (switched_) (void) cudaSetDevice(prev_);
+   }
+   bool ok() const { return ok_; }
+
+ private:
+   int prev_ = 0;
+   bool ok_ = false, switched_ = false;
+};
+
+int raggedPlanDevice(DSPLIB_gpu_raggedPlan plan)
+{
+   const RaggedPlan *p = (const RaggedPlan *) plan;
+   return p ? p->device : -1;
+}
+
 } // namespace dsplib
 
 using namespace dsplib;
@@ -563,6 +592,8 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_fwd(DSPLIB_gpu_raggedPlan plan, const 
 {
    RaggedPlan *p = (RaggedPlan *) plan;
    if (!p || !x || !taps || (!coefs && p->totalCoefs) || !y || !work) return DSPLIB_ERR_NULL_POINTER;
+   PlanDevice dev(p);
+   if (!dev.ok()) return DSPLIB_ERR_FAILURE;
    cudaStream_t s = (cudaStream_t) stream;
    if (launchFirBf16x3Ragged(p->dChan, p->dFirFwdRuns, p->nFirFwdRuns, x, taps, work, false, p->Tmax, s) !=
        cudaSuccess)
@@ -583,6 +614,8 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
    RaggedPlan *p = (RaggedPlan *) plan;
    if (!p || !x || !taps || ((!coefs || !gcoefs) && p->totalCoefs) || !work || !gy || !gx || !gtaps || !scratch)
       return DSPLIB_ERR_NULL_POINTER;
+   PlanDevice dev(p);
+   if (!dev.ok()) return DSPLIB_ERR_FAILURE;
    cudaStream_t s = (cudaStream_t) stream;
    float *g = scratch;                      // gradient at the FIR output
    float *part = scratch + 2 * p->totalLen; // per-tile taps-gradient partials
@@ -606,6 +639,8 @@ DSPLIB_STATUS DSPLIB_gpu_raggedMseGrad(DSPLIB_gpu_raggedPlan plan, const float *
    RaggedPlan *p = (RaggedPlan *) plan;
    if (!p || !y || !target || !gy || !loss || !scratch) return DSPLIB_ERR_NULL_POINTER;
    if (p->totalOut <= 0) return DSPLIB_ERR_INVALID_DIMENSION;
+   PlanDevice dev(p);
+   if (!dev.ok()) return DSPLIB_ERR_FAILURE;
    cudaStream_t s = (cudaStream_t) stream;
    double *part = (double *) scratch;
    mse_partial_kernel<<<p->nFwdItems, 256, 0, s>>>(p->dChan, p->dFwdItems, y, target, gy, part,

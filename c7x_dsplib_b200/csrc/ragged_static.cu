@@ -18,9 +18,11 @@
 //     serialise them (one stream, or event dependencies).
 //   * Nothing in the array needs to start at zero: every word the adjoint reads is
 //     written earlier in the same call.
-//   * The first call on a device looks up the array's device address (one-time
-//     set-up, done with that device current); make that first call before any
-//     stream capture begins.
+//   * The array's device address is looked up (cudaGetSymbolAddress, with the
+//     plan's device current) on every call made outside stream capture, so it stays
+//     valid after a cudaDeviceReset; a call made while its stream is being captured
+//     uses the address the last call outside capture found.  So the first call on a
+//     device must come before any stream capture begins.
 //   * Plans whose scratch exceeds the array (DSPLIB_GPU_STATIC_SCRATCH_FLOATS
 //     floats) are rejected with DSPLIB_ERR_BUFFER_TOO_SMALL before any work is queued.
 #include <cuda_runtime.h>
@@ -37,22 +39,25 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) float g_staticScratch[DSPLIB_GPU_STATIC_SCRATCH_FLOATS];
 
 std::mutex g_scratchMutex;
-float *g_scratchAddr[kMaxDevices]; // device address of g_staticScratch, per device (null until looked up)
+float *g_scratchAddr[kMaxDevices]; // device address of g_staticScratch per device, from the last lookup
 
-// Address of this device's scratch array; looked up once per device (the device must be current).
-cudaError_t staticScratch(float **out)
+// Device address of the scratch array on `dev` (the current device).  Looked up on
+// every call outside stream capture; a captured call reuses the last lookup.
+cudaError_t staticScratch(int dev, cudaStream_t stream, float **out)
 {
-   int dev = 0;
-   cudaError_t e = cudaGetDevice(&dev);
-   if (e != cudaSuccess) return e;
    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+   cudaError_t e = cudaStreamIsCapturing(stream, &cs);
+   if (e != cudaSuccess) return e;
    std::lock_guard<std::mutex> lock(g_scratchMutex);
-   if (!g_scratchAddr[dev]) {
+   if (cs == cudaStreamCaptureStatusNone) {
       void *p = nullptr;
       e = cudaGetSymbolAddress(&p, g_staticScratch);
       if (e != cudaSuccess) return e;
       g_scratchAddr[dev] = (float *) p;
    }
+   else if (!g_scratchAddr[dev])
+      return cudaErrorStreamCaptureUnsupported; // first call on this device made under capture
    *out = g_scratchAddr[dev];
    return cudaSuccess;
 }
@@ -69,7 +74,15 @@ extern "C" DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwdStaticScratch(DSPLIB_gpu
    const int64_t need = DSPLIB_gpu_raggedPlanSize(plan, DSPLIB_GPU_RAGGED_SCRATCH);
    if (need < 0) return DSPLIB_ERR_FAILURE;
    if (need > (int64_t) DSPLIB_GPU_STATIC_SCRATCH_FLOATS) return DSPLIB_ERR_BUFFER_TOO_SMALL;
+   // the lookup needs the plan's device current: switch to it for the call
+   const int dev = dsplib::raggedPlanDevice(plan);
+   int prev = 0;
+   if (cudaGetDevice(&prev) != cudaSuccess) return DSPLIB_ERR_FAILURE;
+   if (prev != dev && cudaSetDevice(dev) != cudaSuccess) return DSPLIB_ERR_FAILURE;
    float *scratch = nullptr;
-   if (dsplib::staticScratch(&scratch) != cudaSuccess) return DSPLIB_ERR_FAILURE;
-   return DSPLIB_gpu_firBiquadBatched_bwd(plan, x, taps, coefs, work, gy, gx, gtaps, gcoefs, scratch, stream);
+   DSPLIB_STATUS st = DSPLIB_ERR_FAILURE;
+   if (dsplib::staticScratch(dev, (cudaStream_t) stream, &scratch) == cudaSuccess)
+      st = DSPLIB_gpu_firBiquadBatched_bwd(plan, x, taps, coefs, work, gy, gx, gtaps, gcoefs, scratch, stream);
+   if (prev != dev) (void) cudaSetDevice(prev);
+   return st;
 }

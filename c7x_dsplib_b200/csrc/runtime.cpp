@@ -22,9 +22,22 @@ void setError(HandleCommon *h, const char *fmt, ...)
    va_end(ap);
 }
 
+// Wait for what is already queued on s (copies into or out of the caller's host
+// buffers, kernels reading them) unless s is being captured into a graph.
+static void drainStream(cudaStream_t s)
+{
+   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+   if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone)
+      (void) cudaStreamSynchronize(s);
+   (void) cudaGetLastError();
+}
+
 DSPLIB_STATUS cudaFail(HandleCommon *h, cudaError_t e, const char *what)
 {
    setError(h, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+   // A failing call returns only after the work it already queued has finished, so no
+   // copy touches the caller's buffers after the error is reported.
+   if (h) drainStream(h->stream);
    return DSPLIB_ERR_FAILURE;
 }
 
@@ -55,26 +68,41 @@ void *mappedHostPtr(const void *p) { return pinnedDevicePtr(p); }
 namespace {
 constexpr int kMaxDevices = 16;
 constexpr int kSlots = 6;
+// Staging buffers of one host thread.  They come from the device's stream-ordered
+// memory pool (no device-wide synchronisation when one grows) and go back to it
+// when the thread exits.
 struct Scratch {
    void *ptr[kMaxDevices][kSlots] = {};
    size_t cap[kMaxDevices][kSlots] = {};
+   ~Scratch()
+   {
+      int prev = -1;
+      if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+      for (int d = 0; d < kMaxDevices; d++)
+         for (int k = 0; k < kSlots; k++)
+            if (ptr[d][k] && cudaSetDevice(d) == cudaSuccess) (void) cudaFree(ptr[d][k]);
+      if (prev >= 0) (void) cudaSetDevice(prev);
+      (void) cudaGetLastError();
+   }
 };
 thread_local Scratch t_scratch;
 } // namespace
 
-void *stagingBuffer(int slot, size_t bytes)
+void *stagingBuffer(int slot, size_t bytes, cudaStream_t s)
 {
    int dev = 0;
    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices || slot < 0 || slot >= kSlots)
       return nullptr;
    if (bytes == 0) bytes = 16;
    if (t_scratch.cap[dev][slot] < bytes) {
-      if (t_scratch.ptr[dev][slot]) cudaFree(t_scratch.ptr[dev][slot]);
+      // Every call that staged through this buffer completed before it returned, so the
+      // old buffer can go back to the pool in the order of s.
+      if (t_scratch.ptr[dev][slot]) (void) cudaFreeAsync(t_scratch.ptr[dev][slot], s);
       t_scratch.ptr[dev][slot] = nullptr;
       t_scratch.cap[dev][slot] = 0;
       size_t want = bytes + bytes / 4; // grow with headroom
       void *p = nullptr;
-      if (cudaMalloc(&p, want) != cudaSuccess) {
+      if (cudaMallocAsync(&p, want, s) != cudaSuccess) {
          (void) cudaGetLastError();
          return nullptr;
       }
@@ -103,7 +131,7 @@ cudaError_t regionIn(Region &r, int slot, bool copyIn, cudaStream_t s)
          return cudaSuccess;
       }
    }
-   void *buf = stagingBuffer(slot, r.bytes());
+   void *buf = stagingBuffer(slot, r.bytes(), s);
    if (!buf) return cudaErrorMemoryAllocation;
    r.dev = buf;
    r.staged = true;
@@ -121,9 +149,33 @@ cudaError_t regionOut(const Region &r, cudaStream_t s)
    return cudaMemcpy2DAsync(r.host, r.pitch, r.dev, r.pitch, r.width, r.height, cudaMemcpyDeviceToHost, s);
 }
 
+namespace {
+// The pipeline streams and events of one host thread, destroyed when it exits.
+struct PipeContexts {
+   PipeContext ctx[kMaxDevices];
+   ~PipeContexts()
+   {
+      for (PipeContext &c : ctx) {
+         if (!c.ready) continue;
+         (void) cudaStreamDestroy(c.in);
+         (void) cudaStreamDestroy(c.comp);
+         (void) cudaStreamDestroy(c.out);
+         (void) cudaEventDestroy(c.start);
+         (void) cudaEventDestroy(c.done);
+         for (int b = 0; b < kPipeMaxBlocks; b++) {
+            (void) cudaEventDestroy(c.copied[b]);
+            (void) cudaEventDestroy(c.computed[b]);
+         }
+      }
+      (void) cudaGetLastError();
+   }
+};
+thread_local PipeContexts t_pipes;
+} // namespace
+
 PipeContext *pipeContext()
 {
-   static thread_local PipeContext ctx[kMaxDevices];
+   PipeContext *ctx = t_pipes.ctx;
    int dev = 0;
    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
    PipeContext &c = ctx[dev];

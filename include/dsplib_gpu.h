@@ -165,8 +165,10 @@ DSPLIB_STATUS DSPLIB_gpu_raggedMseGrad(DSPLIB_gpu_raggedPlan plan, const float *
  *  - All calls on a device share the array: calls that overlap in time race and
  *    corrupt each other's results; order them (same stream or events).
  *  - No part of the array needs to start at zero.
- *  - The first call on a device does a one-time lookup of the array's address with
- *    that device current; make it before any stream capture begins.
+ *  - The array's device address is looked up, with the plan's device current, on
+ *    every call made outside stream capture (so it survives cudaDeviceReset); a call
+ *    made while its stream is being captured reuses the last address found, so make
+ *    the first call on a device before any stream capture begins.
  *  Results are those of DSPLIB_gpu_firBiquadBatched_bwd with the same inputs. */
 DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwdStaticScratch(DSPLIB_gpu_raggedPlan plan, const float *x,
                                                            const float *taps, const float *coefs, const float *work,

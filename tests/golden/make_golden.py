@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference's own Python
 test models.  Run in a checkout that has the reference project available:
 
-    python tests/golden/make_golden.py --ref /root/reference
+    python tests/golden/make_golden.py --ref <reference checkout>
 
 Outputs (committed; the GPU box never needs the reference tree):
   fir_golden.npz     FIR cases drawn from test/DSPLIB_idat_gen/DSPLIB_fir/test_cases_list.csv
@@ -212,7 +212,7 @@ def layout_cases(ref, max_elems=4096, max_sum_elems=16000):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="path of the reference checkout")
     ap.add_argument("--what", default="all", choices=["all", "layout"])
     a = ap.parse_args()
     if a.what == "all":

@@ -73,13 +73,37 @@ def test_opt_integer_default_is_wrap(dt):
 
 
 @pytest.mark.parametrize("dt,shift", [(np.int8, 7), (np.int8, 0), (np.int16, 15), (np.int16, 3), (np.int32, 31),
-                                      (np.int32, 0)])
+                                      (np.int32, 0), (np.int8, 26), (np.int8, 31), (np.int8, 32), (np.int8, 62),
+                                      (np.int16, 40), (np.int16, 62), (np.int32, 62)])
 def test_qmode_bitexact(dt, shift):
     rng = np.random.default_rng(shift + 1)
     for (B, N, T) in [(2, 700, 64), (3, 4096, 128), (1, 40, 40)]:
         x, h = rand(dt, (B, N), rng), rand(dt, (B, T), rng)
         got = host(D.fir(dev(x), dev(h), T, nch=1, func_style=D.OPTIMIZED, qmode=True, shift=shift))
         assert np.array_equal(got, oracle.fir_q(x, h, T, shift, nch=1)), (B, N, T)
+
+
+@pytest.mark.parametrize("dt", [np.int8, np.int16, np.int32])
+def test_qmode_shift_beyond_accumulator_rejected(dt):
+    """Q mode takes shifts up to 62; beyond, exec refuses with DSPLIB_ERR_INVALID_VALUE and
+    leaves the output untouched (the wrap mode ignores the shift, as the natural-C kernel)."""
+    B, N, T = 2, 300, 16
+    rng = np.random.default_rng(23)
+    x, hh = rand(dt, (B, N), rng), rand(dt, (1, T), rng)
+    args, pin, pfilt, pout = D.fir_setup(_NP_CODE[dt], B, N, T, nch=0, shift=63)
+    h = D.FirHandle()
+    assert h.init(args, pin, pfilt, pout) == D.SUCCESS
+    out = dev(np.full((B, N - T + 1), 5, dt))
+    h.set_qmode(True)
+    assert h.exec(dev(x), dev(hh), out) == D.ERR_INVALID_VALUE
+    assert "shift" in h.last_error()
+    assert np.all(host(out) == 5)
+    h.set_qmode(False)
+    assert h.exec(dev(x), dev(hh), out) == D.SUCCESS
+    assert np.array_equal(host(out), oracle.fir(x, hh, T, nch=0))
+
+
+_NP_CODE = {np.int8: D.INT8, np.int16: D.INT16, np.int32: D.INT32}
 
 
 @pytest.mark.parametrize("dt", [np.int8, np.int16])

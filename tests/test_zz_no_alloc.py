@@ -54,7 +54,7 @@ def test_static_scratch_adjoint_matches_buffer_adjoint_twice():
         assert st == SUCCESS
         torch.cuda.synchronize()
         for g, w in zip(got, want):
-            assert torch.allclose(g, w, rtol=1e-6, atol=1e-7)
+            assert torch.equal(g, w)  # the adjoint is bitwise repeatable: same inputs, same bits
 
 
 @pytest.mark.gpu
