@@ -231,6 +231,7 @@ int firTcErrorFlag(bool clear);
 struct RaggedChan {
    long long xOff, hOff, cOff, pOff;
    int L, T, S, Lu;
+   long long ckOff; // first checkpoint (float2) of the channel: one per 512-sample span and stage
 };
 // Split-BF16x3 tensor-core FIR over a list of runs {channel, first tile, tiles, 0}
 // of kFirBfTile outputs: forward (valid correlation of the channel's x with its
@@ -242,6 +243,46 @@ constexpr int kFirBfMaxTaps = 512;
 int raggedPlanDevice(DSPLIB_gpu_raggedPlan plan);
 cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *in,
                                   const float *taps, float *out, bool dx, int Tmax, cudaStream_t s);
+
+// Cascade of the filter bank split along time (bank_scan.cu).  Forward segments of
+// kBankFwdSeg samples, adjoint segments of kBankBwdSeg, checkpoints every kBankSpan
+// samples; per stage a table of kBankTabFloats floats (coefficients, transition
+// powers, free-response rows).
+constexpr int kBankFwdSeg = 4096;
+constexpr int kBankBwdSeg = 2048;
+constexpr int kBankSpan = 512;
+constexpr int kBankTabFloats = 80;
+constexpr size_t kBankBwdSharedLimit = 200 * 1024; // stage sequences beyond this go to global scratch
+constexpr int kBankErrWait = 1;                    // error word bit: a look-back wait expired
+constexpr int kBankDefaultWaitPolls = 1 << 22;
+
+struct BankLaunch {
+   const RaggedChan *chans;
+   const int4 *units; // {channel, segment, segments of the channel, first record}
+   int nUnits;
+   int Smax;
+   const float *tables;
+   const float *u;    // FIR output plane
+   float *y;          // forward output
+   const float *gy;   // adjoint: output gradient
+   float *g;          // adjoint: gradient w.r.t. the FIR output
+   float2 *ckpt;
+   float4 *recs;
+   int *flags;
+   double *gpart;
+   int *chanDone;
+   int *ticket;
+   float *gcoefs;
+   int *err;
+   int waitLimit;
+   float *wGlobal;
+};
+cudaError_t launchBankTables(const float *coefs, int totalStages, float *tables, cudaStream_t s);
+cudaError_t launchBankForward(const BankLaunch &b, cudaStream_t s);
+cudaError_t launchBankBackward(const BankLaunch &b, int ctas, cudaStream_t s);
+int bankBackwardCtas(int Smax, int nUnits);
+bool bankBackwardFitsShared(int Smax);
+long long bankBackwardGlobalFloats(int Smax, int ctas);
 
 struct BiquadLaunch {
    const float *x;

@@ -258,3 +258,113 @@ def test_mse_grad():
     assert np.array_equal(gy.cpu().numpy(), want_gy)
     want = float(np.sum(d[mask].astype(np.float64) ** 2) / n)
     assert float(loss.item()) == pytest.approx(want, rel=1e-6)
+
+
+# ------------------------------------------------------------------ poles near the unit circle
+
+
+def _fp32_channel_step(x, h, c, gy):
+    """The same step in sequential FP32 (numpy / scipy single-precision recursions): the
+    error an FP32 implementation of this filter makes anyway, the yardstick for the
+    bound below."""
+    from scipy.signal import lfilter
+
+    f = np.float32
+    u = np.convolve(x.astype(f), h.astype(f), "valid").astype(f)
+    coefs = np.asarray(c, f).reshape(-1, 5)
+    acts = [u]
+    for b0, b1, b2, a1, a2 in coefs:
+        acts.append(lfilter(np.array([b0, b1, b2], f), np.array([1, a1, a2], f), acts[-1]).astype(f))
+    g = gy.astype(f)
+    gc = np.zeros_like(coefs)
+    for s in range(len(coefs) - 1, -1, -1):
+        b0, b1, b2, a1, a2 = coefs[s]
+        uu, yy = acts[s], acts[s + 1]
+        v = lfilter(np.array([1], f), np.array([1, a1, a2], f), g[::-1]).astype(f)[::-1]
+        vp = np.concatenate([v, np.zeros(2, f)])
+        g = (b0 * vp[:-2] + b1 * vp[1:-1] + b2 * vp[2:]).astype(f)
+        gc[s] = [v @ uu, v[1:] @ uu[:-1], v[2:] @ uu[:-2], -(v[1:] @ yy[:-1]), -(v[2:] @ yy[:-2])]
+    gx = np.convolve(g, h.astype(f)[::-1], "full").astype(f)
+    gh = np.correlate(x.astype(f), g, "valid")[::-1].astype(f)
+    return acts[-1], gx, gh, gc.reshape(-1)
+
+
+def _rel(got, want):
+    return float(np.abs(np.asarray(got, np.float64) - want).max() / max(np.abs(want).max(), 1e-30))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("radius", [0.99, 0.995, 0.999])
+def test_bank_poles_near_unit_circle(radius):
+    """Every pole at radius 0.99 / 0.995 / 0.999 (the regime the FP64-formed transition
+    powers exist for), channels of many scan segments, against FP64.  Bound per channel
+    and quantity: max(1e-4, 4 x the error of the sequential FP32 step), the FP32
+    recursion's own error growing like 1 / (1 - r)."""
+    rng = np.random.default_rng(int(radius * 1000))
+    lengths, taps, stages = [70000, 23000, 9000, 4200], [64, 17, 200, 1], [2, 3, 4, 1]
+    x = rng.standard_normal(sum(lengths)).astype(np.float32).astype(np.float64)
+    h = np.concatenate([rng.standard_normal(T) / np.sqrt(T) for T in taps]).astype(np.float32).astype(np.float64)
+    c = np.concatenate([stable_sections(rng, S, radius=(radius, radius)).reshape(-1) for S in stages])
+    c = c.astype(np.float32).astype(np.float64)
+    gy = rng.standard_normal(len(x)).astype(np.float32).astype(np.float64)
+    o = 0
+    for L, T in zip(lengths, taps):
+        gy[o + L - T + 1:o + L] = 0.0
+        o += L
+    bank, (y, gx, gh, gc) = _run_bank(lengths, taps, stages, x, h, c, gy)
+    bank.status()
+    xo = ho = co = 0
+    for L, T, S in zip(lengths, taps, stages):
+        xs, hs, cs = x[xo:xo + L], h[ho:ho + T], c[co:co + 5 * S]
+        gys = gy[xo:xo + L - T + 1]
+        y64, _ = channel_forward(xs, hs, cs)
+        gx64, gh64, gc64 = channel_adjoint(xs, hs, cs, gys)
+        y32, gx32, gh32, gc32 = _fp32_channel_step(xs, hs, cs, gys)
+        for name, got, want, seq in (("y", y[xo:xo + L - T + 1], y64, y32), ("gx", gx[xo:xo + L], gx64, gx32),
+                                     ("gtaps", gh[ho:ho + T], gh64, gh32),
+                                     ("gcoefs", gc[co:co + 5 * S], gc64.reshape(-1), gc32)):
+            bound = max(1e-4, 4 * _rel(seq, want))
+            assert _rel(got, want) <= bound, (radius, L, name, _rel(got, want), _rel(seq, want))
+        xo, ho, co = xo + L, ho + T, co + 5 * S
+
+
+@pytest.mark.gpu
+def test_bank_deep_cascades_beyond_shared_memory():
+    """24 stages: the adjoint keeps the stage sequences in global scratch instead of
+    shared memory (a different code path of the same kernel)."""
+    lengths, taps, stages, x, h, c = _bank_case(8, 5, Lrange=(2000, 12000), Tmax=32, Smax=4,
+                                                force=[(9000, 16, 24), (3000, 3, 22)])
+    _check_bank(lengths, taps, stages, x, h, c)
+
+
+@pytest.mark.gpu
+def test_bank_wait_expiry_is_reported_and_recoverable():
+    """A cross-segment wait that gives up (here: a wait limit of 0 polls, so every wait
+    gives up at once) raises the plan's error word; the calls still terminate, and with
+    the default limit restored the same plan computes correct results again."""
+    import torch
+
+    from c7x_dsplib_b200 import DsplibError
+
+    lengths, taps, stages, x, h, c = _bank_case(9, 3, Lrange=(20000, 30000), Tmax=16, Smax=3,
+                                                force=[(17000, 8, 2)])
+    gy = np.random.default_rng(3).standard_normal(len(x))
+    bank, _ = _run_bank(lengths, taps, stages, x, h, c, gy)
+    bank.status()
+    bank.set_wait_limit(0)
+    dev = "cuda"
+    xt = torch.tensor(x, dtype=torch.float32, device=dev)
+    ht = torch.tensor(h, dtype=torch.float32, device=dev)
+    ct = torch.tensor(c, dtype=torch.float32, device=dev)
+    y = torch.empty(bank.sizes[0], device=dev)
+    work = torch.empty(bank.sizes[3], device=dev)
+    bank.forward_raw(xt, ht, ct, y, work)
+    with pytest.raises(DsplibError):
+        bank.status()
+    bank.status()  # the query cleared the word
+    bank.set_wait_limit(1 << 22)
+    bank.forward_raw(xt, ht, ct, y, work)
+    bank.status()
+    y64 = bank_forward(lengths, taps, stages, x.astype(np.float32).astype(np.float64),
+                       h.astype(np.float32).astype(np.float64), c.astype(np.float32).astype(np.float64))
+    assert _per_channel_err(lengths, lengths, y.cpu().numpy().astype(np.float64), y64) <= Y_TOL

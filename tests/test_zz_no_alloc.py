@@ -64,8 +64,9 @@ def test_static_scratch_rejects_plans_beyond_its_size():
     from c7x_dsplib_b200 import ERR_BUFFER_TOO_SMALL, lib
     from c7x_dsplib_b200.filterbank import RaggedFilterBank
 
-    # 3 channels of 1M samples: the adjoint needs > 6M floats of scratch, the array holds 4M
-    bank = RaggedFilterBank([1 << 20] * 3, [8] * 3, [1] * 3)
+    # 4 channels of 1M samples: the adjoint needs > 4M floats of scratch (the gradient
+    # w.r.t. the FIR output alone is 4M), the array holds 4M
+    bank = RaggedFilterBank([1 << 20] * 4, [8] * 4, [1] * 4)
     assert bank.sizes[4] > (4 << 20)
     d = torch.zeros(16, device="cuda")
     p = d.data_ptr()
