@@ -150,8 +150,6 @@ SIGNATURES = {
                                                    _P(ctypes.c_int32), _P(ctypes.c_int32)]),
     "DSPLIB_gpu_raggedPlanSize": (ctypes.c_int64, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_raggedPlanDestroy": (ctypes.c_int, [_VP]),
-    "DSPLIB_gpu_raggedPlanStatus": (ctypes.c_int, [_VP, _VP]),
-    "DSPLIB_gpu_raggedPlanSetWaitLimit": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_firBiquadBatched_fwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_gpu_firBiquadBatched_bwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_gpu_raggedMseGrad": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),

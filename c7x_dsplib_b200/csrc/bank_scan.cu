@@ -1,49 +1,37 @@
 // Cascade of direct-form-II biquads of the batched filter bank, forward and
-// adjoint, split along time: every channel is cut into segments that
-// independent CTAs filter at the same time, so a 262144-sample channel keeps
-// 64 CTAs busy instead of one.
+// adjoint, split along time into 512-sample units that warps filter
+// independently, with no wait between CTAs and no CTA barrier.
 //
-// Within a segment (one CTA) each thread owns a chunk of 16 consecutive
-// samples.  Per stage:
-//   1. the chunk is filtered from a zero state (the only serial pass);
-//   2. the chunk end states are combined by a chunked scan: lanes of a warp
-//      (shuffles), warps of the CTA (shared memory), segments of the channel
-//      (decoupled look-back over records in global memory); the combine is
-//      the affine map s -> M s + e with M = A^16 and its powers, A the
-//      stage's 2x2 companion matrix, formed in FP64 and rounded once;
-//   3. the true output follows without a serial chain: the free response
-//      of the chunk's true initial state (w1, w2) is added sample by sample,
-//      w[i] = w_zs[i] + alpha_i w1 + beta_i w2 with (alpha_i, beta_i) the
-//      first row of A^(i+1), then y[i] = b0 w[i] + b1 w[i-1] + b2 w[i-2].
+// A unit is one warp; each lane owns a chunk of 16 consecutive samples.  Per
+// stage the chunk is filtered from a zero state (the only serial pass), the
+// chunk end states are combined by a warp scan of the affine maps
+// s -> M s + e (M = A^16 and its powers, A the stage's 2x2 companion matrix,
+// formed in FP64 and rounded once), and the true output follows without a
+// serial chain: w[i] = w_zs[i] + alpha_i w1 + beta_i w2 with (alpha_i, beta_i)
+// the first row of A^(i+1) and (w1, w2) the chunk's initial state, then
+// y[i] = b0 w[i] + b1 w[i-1] + b2 w[i-2].
 //
-// Decoupled look-back: a CTA takes its segment from a ticket counter, so every
-// earlier segment of its channel is already running or done.  It publishes the
-// segment's zero-entry end state (aggregate, flag 1) as soon as its local scan
-// is done, then walks back over its predecessors, adding each one's aggregate
-// times the segment transition power until it meets an inclusive state (flag 2)
-// or the power has become exactly zero in FP32 (older segments then contribute
-// exactly nothing), and publishes its own inclusive state.  Every wait is
-// bounded; on expiry the kernel raises the plan's error word and continues with
-// what it has, so it always terminates.
-//
-// Forward (bank_fwd_kernel, 256 threads, 4096-sample segments): all stages of
-// the cascade, the last one's output to y.  It stores no stage output: the
-// state at the start of every 512-sample span (one warp) of every stage is kept
-// as a checkpoint, 2 floats per 512 samples per stage.
-//
-// Adjoint (bank_bwd_kernel, 128 threads, 2048-sample segments, persistent):
-// the forward of the segment is recomputed warp by warp from the checkpoints
-// (no CTA barrier: every warp knows its entry state), keeping each stage's
-// internal sequence w_s in shared memory; then the stages run in reverse
-// order, each as the reverse-time recursion of the DF2 adjoint,
-//     v[t] = g[t] - a1 v[t+1] - a2 v[t+2],  lambda[t] = b0 v[t] + b1 v[t+1] + b2 v[t+2],
-// with the same chunked scan in reverse (segments in decreasing time order,
-// look-back toward later segments), g = the stage's output gradient and lambda
-// its input gradient.  Coefficient gradients:
-//     dL/db_i = sum_t g[t] w[t-i],   dL/da_i = -sum_t lambda[t] w[t-i],
-// summed per chunk in FP32, per warp by shuffles, per segment in FP64, and
-// per channel in FP64 in segment order by the last segment's CTA (bitwise
-// repeatable whatever the CTA schedule).
+// Units are chained through the whole cascade at once.  With the state of
+// all S stages at a unit's start as one 2S-vector z, the state at its end is
+// Phi z + e, where e is the end state when every stage starts the unit from
+// zero and Phi = A_c^512, A_c the cascade's 2S x 2S one-step transition (block
+// lower-triangular: stage p's output drives stage p + 1).  So:
+//   pass 1 (bank_unit_kernel<AGG>): every unit, all stages from a zero state:
+//           e, 2 floats per stage;
+//   pass 2 (bank_chain_kernel): per channel, z_0 = 0, z_{j+1} = Phi z_j + e_j
+//           in FP64, j over the channel's units; z_j is stored (2 floats per
+//           unit and stage): the checkpoints;
+//   pass 3 (bank_unit_kernel<OUT>): every unit again from its checkpoint: y.
+// The adjoint is the same cascade run backwards in time with the stages in
+// reverse order (v[t] = g[t] - a1 v[t+1] - a2 v[t+2], lambda[t] = b0 v[t] +
+// b1 v[t+1] + b2 v[t+2]: g the stage's output gradient, lambda its input
+// gradient), chained the same way from the channel's end; its last pass
+// (bank_adjoint_kernel) recomputes each unit's forward from the forward
+// checkpoints, keeping every stage's internal sequence w_s in shared memory,
+// and accumulates the coefficient gradients
+//     dL/db_i = sum_t g[t] w[t-i],   dL/da_i = -sum_t lambda[t] w[t-i]
+// in FP32 per unit, then in FP64 per channel in unit order (bank_coef_kernel):
+// bitwise repeatable.
 #include <cuda_runtime.h>
 
 #include "dsplib_internal.h"
@@ -55,17 +43,14 @@ namespace {
 using scan::M2;
 using scan::M2f;
 
-constexpr int kL = 16;          // samples per chunk (thread)
-constexpr int kSpan = 32 * kL;  // samples per warp: checkpoint granularity
-constexpr int kFwdWarps = 8;
-constexpr int kFwdThreads = kFwdWarps * 32;
-constexpr int kFwdSeg = kFwdThreads * kL; // 4096: transition A^4096 = M^256 = P[8]
-constexpr int kBwdWarps = 4;
-constexpr int kBwdThreads = kBwdWarps * 32;
-constexpr int kBwdSeg = kBwdThreads * kL; // 2048: transition A^2048 = M^128 = P[7]
-constexpr int kOutPad = kL + 1;           // padded shared row per chunk (conflict-free staging)
+constexpr int kL = 16;          // samples per chunk (lane)
+constexpr int kUnit = 32 * kL;  // samples per unit (warp): 512
+constexpr int kWarps = 4;       // units per CTA
+constexpr int kThreads = 32 * kWarps;
+constexpr int kOutPad = kL + 1; // padded shared row per chunk (conflict-free staging)
+constexpr int kUnitLog2 = 9;    // Phi = A_c^(2^9)
 
-static_assert(kFwdSeg == kBankFwdSeg && kBwdSeg == kBankBwdSeg && kSpan == kBankSpan, "segment sizes");
+static_assert(kUnit == kBankSpan, "unit size");
 
 // Stage table (floats): [0, 5) b0 b1 b2 a1 a2; [8 + 4k, 12 + 4k) P[k] = M^(2^k), M = A^16,
 // k = 0..8, row-major; [44 + 2i, 46 + 2i) alpha_i, beta_i = row 0 of A^(i+1), i = 0..15.
@@ -86,65 +71,6 @@ __device__ __forceinline__ float2 shflDown(float2 v, int d)
    v.x = __shfl_down_sync(0xffffffffu, v.x, d);
    v.y = __shfl_down_sync(0xffffffffu, v.y, d);
    return v;
-}
-
-__device__ __forceinline__ M2f mmulF(const M2f &x, const M2f &y)
-{
-   return {fmaf(x.a, y.a, x.b * y.c), fmaf(x.a, y.b, x.b * y.d), fmaf(x.c, y.a, x.d * y.c),
-           fmaf(x.c, y.b, x.d * y.d)};
-}
-
-// ------------------------------------------------------------------ decoupled look-back
-
-// Bounded wait for a record flag set by another CTA; 0 when the wait gave up
-// (limit 0: give up at once, which tests use to exercise the expiry path).
-__device__ __forceinline__ int waitFlag(const int *flag, int limit)
-{
-   for (int i = 0; i < limit; i++) {
-      int f;
-      asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(f) : "l"(flag) : "memory");
-      if (f) return f;
-      __nanosleep(64);
-   }
-   return 0;
-}
-
-__device__ __forceinline__ float2 loadRecord(const float4 *rec, int which)
-{
-   const float *p = (const float *) rec + 2 * which;
-   float2 v;
-   asm volatile("ld.relaxed.gpu.global.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p) : "memory");
-   return v;
-}
-
-// Record r: (aggregate, inclusive); flag 1 = aggregate valid, 2 = inclusive valid.
-__device__ __forceinline__ void publish(float4 *recs, int *flags, int r, float2 v, int state)
-{
-   float *p = (float *) (recs + r) + 2 * (state - 1);
-   p[0] = v.x;
-   p[1] = v.y;
-   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(flags + r), "r"(state) : "memory");
-}
-
-// State entering a segment from the `preds` segments before it (in the scan's
-// direction): records r, r - S, r - 2S, ... of the same stage.
-__device__ float2 lookBack(const float4 *recs, const int *flags, int r, int preds, int S, const M2f &PW, int limit,
-                           int *err)
-{
-   float2 z = make_float2(0.0f, 0.0f);
-   M2f Mp = {1.0f, 0.0f, 0.0f, 1.0f};
-   for (int j = 0; j < preds; j++, r -= S) {
-      const int f = waitFlag(flags + r, limit);
-      if (!f) {
-         atomicOr(err, kBankErrWait);
-         break;
-      }
-      z = scan::affine(Mp, loadRecord(recs + r, f - 1), z);
-      if (f == 2) break;
-      Mp = mmulF(Mp, PW);
-      if (Mp.a == 0.0f && Mp.b == 0.0f && Mp.c == 0.0f && Mp.d == 0.0f) break;
-   }
-   return z;
 }
 
 // ------------------------------------------------------------------ stage tables
@@ -177,21 +103,130 @@ __global__ void __launch_bounds__(128) bank_tables_kernel(const float *coefs, in
    for (int k = kTabAB + 2 * kL; k < kBankTabFloats; k++) tb[k] = 0.0f;
 }
 
-// ------------------------------------------------------------------ forward
+// ------------------------------------------------------------------ cascade transitions
 
-struct FwdArgs {
-   const RaggedChan *chans;
-   const int4 *units; // {channel, segment, segments of the channel, first record}
-   const float *tables;
-   const float *u;    // FIR output plane (channel c at pOff)
-   float *y;
-   float2 *ckpt;
-   float4 *recs;
-   int *flags;
-   int *ticket;
-   int *err;
-   int limit;
-};
+// Lower block-triangular 2S x 2S matrix in 2x2 blocks (p, q), q <= p, block index
+// p (p + 1) / 2 + q, each block 4 doubles row-major.
+__host__ __device__ inline int blk(int p, int q) { return p * (p + 1) / 2 + q; }
+
+// Processing position p -> stage: forward p, adjoint S - 1 - p.
+__device__ __forceinline__ int stageAt(int p, int S, bool adj) { return adj ? S - 1 - p : p; }
+
+// Phi = A_c^512 for one channel and direction, one CTA: A_c in shared memory, nine
+// squarings C(p,q) = sum_{m=q..p} B(p,m) B(m,q) between two shared buffers.
+__global__ void __launch_bounds__(128) bank_transition_kernel(const RaggedChan *chans, const float *coefs,
+                                                              double *phi)
+{
+   extern __shared__ double dynT[];
+   const RaggedChan c = chans[blockIdx.x];
+   const bool adj = blockIdx.y != 0;
+   const int S = c.S;
+   if (S == 0) return;
+   const int nb = S * (S + 1) / 2;
+   double *B = dynT, *C = dynT + 4 * nb;
+   const float *cf = coefs + c.cOff;
+   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+      int p = 0;
+      while (blk(p + 1, 0) <= b) p++;
+      const int q = b - blk(p, 0);
+      const int sp = stageAt(p, S, adj);
+      double *o = B + 4 * b;
+      if (q == p) {
+         o[0] = -(double) cf[5 * sp + 3];
+         o[1] = -(double) cf[5 * sp + 4];
+         o[2] = 1.0;
+         o[3] = 0.0;
+      }
+      else {
+         // stage q's state reaches stage p's input through the direct terms b0 of the stages between
+         const int sq = stageAt(q, S, adj);
+         const double b0 = cf[5 * sq], b1 = cf[5 * sq + 1], b2 = cf[5 * sq + 2];
+         double d0 = b1 - b0 * (double) cf[5 * sq + 3], d1 = b2 - b0 * (double) cf[5 * sq + 4];
+         for (int m = q + 1; m < p; m++) {
+            const double g = cf[5 * stageAt(m, S, adj)];
+            d0 *= g;
+            d1 *= g;
+         }
+         o[0] = d0;
+         o[1] = d1;
+         o[2] = 0.0;
+         o[3] = 0.0;
+      }
+   }
+   __syncthreads();
+   for (int it = 0; it < kUnitLog2; it++) {
+      for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+         int p = 0;
+         while (blk(p + 1, 0) <= b) p++;
+         const int q = b - blk(p, 0);
+         double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
+         for (int m = q; m <= p; m++) {
+            const double *x = B + 4 * blk(p, m), *y = B + 4 * blk(m, q);
+            r0 = fma(x[0], y[0], fma(x[1], y[2], r0));
+            r1 = fma(x[0], y[1], fma(x[1], y[3], r1));
+            r2 = fma(x[2], y[0], fma(x[3], y[2], r2));
+            r3 = fma(x[2], y[1], fma(x[3], y[3], r3));
+         }
+         double *o = C + 4 * b;
+         o[0] = r0;
+         o[1] = r1;
+         o[2] = r2;
+         o[3] = r3;
+      }
+      __syncthreads();
+      double *t = B;
+      B = C;
+      C = t;
+   }
+   double *dst = phi + c.phiOff + (adj ? 4LL * nb : 0);
+   for (int i = threadIdx.x; i < 4 * nb; i += blockDim.x) dst[i] = B[i];
+}
+
+// Per channel (one warp): z_0 = 0, checkpoint z_j, z_{j+1} = Phi z_j + e_j over the
+// channel's units (adjoint: from the last unit back).  z in FP64.
+__global__ void __launch_bounds__(32) bank_chain_kernel(const RaggedChan *chans, const double *phi,
+                                                        const float2 *agg, float2 *ckpt, int adj)
+{
+   extern __shared__ double dynC[];
+   const RaggedChan c = chans[blockIdx.x];
+   const int S = c.S, lane = threadIdx.x;
+   if (S == 0) return;
+   const int nb = S * (S + 1) / 2, n2 = 2 * S;
+   double *P = dynC, *z = dynC + 4 * nb;
+   const double *src = phi + c.phiOff + (adj ? 4LL * nb : 0);
+   for (int i = lane; i < 4 * nb; i += 32) P[i] = src[i];
+   for (int r = lane; r < n2; r += 32) z[r] = 0.0;
+   __syncwarp();
+   const int units = (c.Lu + kUnit - 1) / kUnit;
+   for (int k = 0; k < units; k++) {
+      const int j = adj ? units - 1 - k : k;
+      const long long base = c.ckOff + (long long) j * S;
+      for (int p = lane; p < S; p += 32) ckpt[base + p] = make_float2((float) z[2 * p], (float) z[2 * p + 1]);
+      if (k + 1 == units) break;
+      double nz[4];
+      for (int i = 0; i < 4; i++) {
+         const int r = lane + 32 * i;
+         if (r >= n2) break;
+         const int p = r >> 1, row = r & 1;
+         const float2 e = agg[base + p];
+         double acc0 = row ? e.y : e.x, acc1 = 0.0;
+         for (int q = 0; q <= p; q++) {
+            const double *x = P + 4 * blk(p, q) + 2 * row;
+            acc0 = fma(x[0], z[2 * q], acc0);
+            acc1 = fma(x[1], z[2 * q + 1], acc1);
+         }
+         nz[i] = acc0 + acc1;
+      }
+      __syncwarp();
+      for (int i = 0; i < 4; i++) {
+         const int r = lane + 32 * i;
+         if (r < n2) z[r] = nz[i];
+      }
+      __syncwarp();
+   }
+}
+
+// ------------------------------------------------------------------ unit passes
 
 // Load the 16 samples of a chunk from a 16-float-aligned plane row, zero at t >= n.
 __device__ __forceinline__ void loadChunk(float (&v)[kL], const float *row, int t0, int n)
@@ -213,6 +248,26 @@ __device__ __forceinline__ void loadChunk(float (&v)[kL], const float *row, int 
    }
 }
 
+// The chunk of an unaligned packed row (x, y, gradients), through the warp's staging
+// area so that every access of the warp covers 32 consecutive samples.
+__device__ __forceinline__ void loadPacked(float (&v)[kL], const float *row, int t0, int n, float *stage, int lane)
+{
+   for (int k = lane; k < kUnit; k += 32) stage[(k >> 4) * kOutPad + (k & 15)] = t0 + k < n ? row[t0 + k] : 0.0f;
+   __syncwarp();
+#pragma unroll
+   for (int i = 0; i < kL; i++) v[i] = stage[lane * kOutPad + i];
+   __syncwarp();
+}
+
+__device__ __forceinline__ void storePacked(const float (&v)[kL], float *row, int t0, int n, float *stage, int lane)
+{
+#pragma unroll
+   for (int i = 0; i < kL; i++) stage[lane * kOutPad + i] = v[i];
+   __syncwarp();
+   for (int k = lane; k < kUnit && t0 + k < n; k += 32) row[t0 + k] = stage[(k >> 4) * kOutPad + (k & 15)];
+   __syncwarp();
+}
+
 // DF2 over the chunk from a zero state (w[i]), returning the end state (w[15], w[14]).
 __device__ __forceinline__ float2 zeroStatePass(const float (&v)[kL], float (&w)[kL], float a1, float a2)
 {
@@ -226,25 +281,54 @@ __device__ __forceinline__ float2 zeroStatePass(const float (&v)[kL], float (&w)
    return make_float2(w[kL - 1], w[kL - 2]);
 }
 
-// Warp-level inclusive scan in time order (lane L combines the chunks of lanes <= L).
-__device__ __forceinline__ float2 warpScanUp(float2 val, const float *tb, int lane)
+// The same in reverse time: v[i] = g[i] - a1 v[i+1] - a2 v[i+2]; end state (v[0], v[1]).
+__device__ __forceinline__ float2 zeroStatePassRev(const float (&g)[kL], float (&v)[kL], float a1, float a2)
 {
+   float p1 = 0.0f, p2 = 0.0f;
+#pragma unroll
+   for (int i = kL - 1; i >= 0; i--) {
+      v[i] = fmaf(-a1, p1, fmaf(-a2, p2, g[i]));
+      p2 = p1;
+      p1 = v[i];
+   }
+   return make_float2(v[0], v[1]);
+}
+
+// Initial state of this lane's chunk from the unit's entry state, forward time:
+// M^lane entry + the scan of the lanes before.  Returns the inclusive scan in *incl.
+__device__ __forceinline__ float2 chunkStateUp(float2 end, float2 entry, const float *tb, int lane, float2 *incl)
+{
+   float2 val = end;
 #pragma unroll
    for (int k = 0; k < 5; k++) {
       const float2 o = scan::shflUp(val, 1 << k, 32);
       if (lane >= (1 << k)) val = scan::affine(tabP(tb, k), o, val);
    }
-   return val;
-}
-
-// Chunk initial state: M^lane * warp entry + the exclusive prefix of the lanes before.
-__device__ __forceinline__ float2 chunkInitUp(float2 val, float2 entry, const float *tb, int lane)
-{
    float2 ex = scan::shflUp(val, 1, 32);
    if (lane == 0) ex = make_float2(0.0f, 0.0f);
 #pragma unroll
    for (int k = 0; k < 5; k++)
       if ((lane >> k) & 1) entry = scan::affine(tabP(tb, k), entry, make_float2(0.0f, 0.0f));
+   *incl = val;
+   return f2add(entry, ex);
+}
+
+// Reverse time: M^(31 - lane) entry + the scan of the lanes after.
+__device__ __forceinline__ float2 chunkStateDown(float2 end, float2 entry, const float *tb, int lane, float2 *incl)
+{
+   float2 val = end;
+#pragma unroll
+   for (int k = 0; k < 5; k++) {
+      const float2 o = shflDown(val, 1 << k);
+      if (lane + (1 << k) < 32) val = scan::affine(tabP(tb, k), o, val);
+   }
+   float2 ex = shflDown(val, 1);
+   if (lane == 31) ex = make_float2(0.0f, 0.0f);
+   const int m = 31 - lane;
+#pragma unroll
+   for (int k = 0; k < 5; k++)
+      if ((m >> k) & 1) entry = scan::affine(tabP(tb, k), entry, make_float2(0.0f, 0.0f));
+   *incl = val;
    return f2add(entry, ex);
 }
 
@@ -265,310 +349,229 @@ __device__ __forceinline__ void correctAndOutput(float (&w)[kL], float (&out)[kL
    }
 }
 
-__global__ void __launch_bounds__(kFwdThreads) bank_fwd_kernel(FwdArgs a)
+// Reverse time, from (v[16], v[17]): lambda[i] = b0 v[i] + b1 v[i+1] + b2 v[i+2].
+__device__ __forceinline__ void correctAndOutputRev(float (&v)[kL], float (&lam)[kL], const float *tb, float v16,
+                                                    float v17)
 {
-   extern __shared__ float4 dynF[];
-   float *sTab = (float *) dynF; // the channel's stage tables
-   __shared__ float sOut[kFwdThreads * kOutPad];
-   __shared__ float2 sAgg[kFwdWarps], sEntry[kFwdWarps];
-   __shared__ int sTicket;
-   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-   if (tid == 0) sTicket = atomicAdd(a.ticket, 1);
-   __syncthreads();
-   const int4 U = a.units[sTicket];
-   const RaggedChan c = a.chans[U.x];
-   const int S = c.S, Lu = c.Lu;
-   {
-      const float4 *src = (const float4 *) (a.tables + (c.cOff / 5) * kBankTabFloats);
-      for (int i = tid; i < S * (kBankTabFloats / 4); i += kFwdThreads) dynF[i] = src[i];
+   const float b0 = tb[0], b1 = tb[1], b2 = tb[2];
+   float n1 = v16, n2 = v17;
+#pragma unroll
+   for (int i = kL - 1; i >= 0; i--) {
+      const float2 ab = *(const float2 *) (tb + kTabAB + 2 * (kL - 1 - i));
+      const float vt = fmaf(ab.x, v16, fmaf(ab.y, v17, v[i]));
+      lam[i] = fmaf(b0, vt, fmaf(b1, n1, b2 * n2));
+      v[i] = vt;
+      n2 = n1;
+      n1 = vt;
    }
-   const int segStart = U.y * kFwdSeg;
-   float v[kL];
-   loadChunk(v, a.u + c.pOff, segStart + tid * kL, Lu);
-   __syncthreads();
-   const float2 zero = make_float2(0.0f, 0.0f);
-   for (int s = 0; s < S; s++) {
-      const float *tb = sTab + s * kBankTabFloats;
-      float w[kL];
-      float2 val = warpScanUp(zeroStatePass(v, w, tb[3], tb[4]), tb, lane);
-      if (lane == 31) sAgg[warp] = val;
-      __syncthreads();
-      if (warp == 0) {
-         float2 tv = lane < kFwdWarps ? sAgg[lane] : zero;
-#pragma unroll
-         for (int k = 0; k < 3; k++) {
-            const float2 o = scan::shflUp(tv, 1 << k, 32);
-            if (lane >= (1 << k) && lane < kFwdWarps) tv = scan::affine(tabP(tb, 5 + k), o, tv);
-         }
-         const float2 agg = scan::shflIdx(tv, kFwdWarps - 1);
-         float2 z = zero;
-         if (lane == 0 && U.z > 1) {
-            const int r = U.w + s;
-            const bool succ = U.y + 1 < U.z;
-            if (U.y == 0) {
-               if (succ) publish(a.recs, a.flags, r, agg, 2);
-            }
-            else {
-               if (succ) publish(a.recs, a.flags, r, agg, 1);
-               z = lookBack(a.recs, a.flags, r - S, U.y, S, tabP(tb, 8), a.limit, a.err);
-               if (succ) publish(a.recs, a.flags, r, scan::affine(tabP(tb, 8), z, agg), 2);
-            }
-         }
-         z = scan::shflIdx(z, 0);
-         const float2 before = scan::shflUp(tv, 1, 32);
-         if (lane < kFwdWarps) {
-            float2 e = z;
-#pragma unroll
-            for (int k = 0; k < 3; k++)
-               if ((lane >> k) & 1) e = scan::affine(tabP(tb, 5 + k), e, zero);
-            if (lane > 0) e = f2add(e, before);
-            sEntry[lane] = e;
-            const int span = U.y * kFwdWarps + lane;
-            if (span * kSpan < Lu) a.ckpt[c.ckOff + (long long) span * S + s] = e;
-         }
-      }
-      __syncthreads();
-      const float2 st = chunkInitUp(val, sEntry[warp], tb, lane);
-      correctAndOutput(w, v, tb, st.x, st.y);
-   }
-   // output through shared memory: each warp store covers 32 consecutive samples
-#pragma unroll
-   for (int i = 0; i < kL; i++) sOut[tid * kOutPad + i] = v[i];
-   __syncthreads();
-   float *yc = a.y + c.xOff;
-   const int n = min(kFwdSeg, Lu - segStart);
-   for (int k = tid; k < n; k += kFwdThreads) yc[segStart + k] = sOut[(k >> 4) * kOutPad + (k & 15)];
-   if (U.y + 1 == U.z)
-      for (int t = Lu + tid; t < c.L; t += kFwdThreads) yc[t] = 0.0f;
 }
 
-// ------------------------------------------------------------------ adjoint
-
-struct BwdArgs {
+struct UnitArgs {
    const RaggedChan *chans;
-   const int4 *units; // segments in decreasing time order within each channel
+   const int2 *units; // (channel, unit index within the channel)
    int nUnits;
-   const float *tables;
-   const float *u;
-   const float *gy;
-   const float2 *ckpt;
-   float *g;          // gradient w.r.t. the FIR output (channel c at xOff, Lu samples)
-   float4 *recs;
-   int *flags;
-   double *gpart;     // per record: 5 coefficient-gradient partial sums
-   int *chanDone;
-   int *ticket;
-   float *gcoefs;
-   int *err;
-   int limit;
-   float *wGlobal;    // stage sequences when they do not fit in shared memory (per CTA)
-   int wInShared;
    int Smax;
+   const float *tables;
+   const float *in;   // forward: FIR output plane; adjoint aggregates: output gradient (packed)
+   float *out;        // OUT: y (packed, tail zeros)
+   float2 *agg;       // AGG: unit aggregates, 2 floats per stage (processing order)
+   const float2 *ckpt;
 };
 
-// Stage sequences of one chunk: w[0..15] and the initial state w[-1], w[-2] for each
-// stage, laid out [stage][18][thread] so that the threads of a warp touch distinct banks.
-constexpr int kWRows = kL + 2;
-
-__global__ void __launch_bounds__(kBwdThreads) bank_bwd_kernel(BwdArgs a)
+// Copy the channel's stage tables into the warp's slice of shared memory.
+__device__ __forceinline__ void loadTables(float *dst, const float *tables, const RaggedChan &c, int lane)
 {
-   extern __shared__ float4 dynB[];
-   float *sTab = (float *) dynB;
-   float *W = a.wInShared ? sTab + (size_t) a.Smax * kBankTabFloats
-                          : a.wGlobal + (size_t) blockIdx.x * a.Smax * kWRows * kBwdThreads;
-   __shared__ float sIO[kBwdThreads * kOutPad];
-   __shared__ float2 sAgg[kBwdWarps], sEntry[kBwdWarps];
-   __shared__ float sRed[2][kBwdWarps][5];
-   __shared__ int sTicket, sLast;
-   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-   const float2 zero = make_float2(0.0f, 0.0f);
-   for (;;) {
-      if (tid == 0) sTicket = atomicAdd(a.ticket, 1);
-      __syncthreads();
-      const int ti = sTicket;
-      if (ti >= a.nUnits) break;
-      const int4 U = a.units[ti];
-      const RaggedChan c = a.chans[U.x];
-      const int S = c.S, Lu = c.Lu;
-      const int segStart = U.y * kBwdSeg;
-      const int n = min(kBwdSeg, Lu - segStart);
-      {
-         const float4 *src = (const float4 *) (a.tables + (c.cOff / 5) * kBankTabFloats);
-         for (int i = tid; i < S * (kBankTabFloats / 4); i += kBwdThreads) dynB[i] = src[i];
-      }
-      // output gradient of the last stage, staged for coalesced reads
-      for (int k = tid; k < kBwdSeg; k += kBwdThreads)
-         sIO[(k >> 4) * kOutPad + (k & 15)] = k < n ? a.gy[c.xOff + segStart + k] : 0.0f;
-      float v[kL];
-      loadChunk(v, a.u + c.pOff, segStart + tid * kL, Lu);
-      __syncthreads();
-      float g[kL];
-#pragma unroll
-      for (int i = 0; i < kL; i++) g[i] = sIO[tid * kOutPad + i];
+   const float4 *src = (const float4 *) (tables + (c.cOff / 5) * kBankTabFloats);
+   for (int i = lane; i < c.S * (kBankTabFloats / 4); i += 32) ((float4 *) dst)[i] = src[i];
+   __syncwarp();
+}
 
-      // 1. recompute the forward of this segment, warp by warp from the checkpoints
-      const int span = U.y * kBwdWarps + warp;
-      const bool spanValid = span * kSpan < Lu;
-      for (int s = 0; s < S; s++) {
-         const float *tb = sTab + s * kBankTabFloats;
-         float w[kL];
-         const float2 val = warpScanUp(zeroStatePass(v, w, tb[3], tb[4]), tb, lane);
-         const float2 entry = spanValid ? a.ckpt[c.ckOff + (long long) span * S + s] : zero;
-         const float2 st = chunkInitUp(val, entry, tb, lane);
+// Forward passes: AGG = from a zero state, write the unit aggregate of every stage;
+// OUT = from the checkpoints, write y.  ADJ_AGG: adjoint aggregates over the output
+// gradient (reverse time, stages in reverse order).
+enum UnitMode { UNIT_AGG = 0, UNIT_OUT = 1, UNIT_ADJ_AGG = 2 };
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) bank_unit_kernel(UnitArgs a)
+{
+   extern __shared__ float4 dynU[];
+   __shared__ float sStage[kWarps][32 * kOutPad];
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int ui = blockIdx.x * kWarps + warp;
+   if (ui >= a.nUnits) return;
+   float *sTab = (float *) dynU + (size_t) warp * a.Smax * kBankTabFloats;
+   const int2 U = a.units[ui];
+   const RaggedChan c = a.chans[U.x];
+   const int S = c.S, Lu = c.Lu, t0 = U.y * kUnit;
+   const long long base = c.ckOff + (long long) U.y * S;
+   loadTables(sTab, a.tables, c, lane);
+   float v[kL];
+   if (MODE == UNIT_ADJ_AGG) loadPacked(v, a.in + c.xOff, t0, Lu, sStage[warp], lane);
+   else loadChunk(v, a.in + c.pOff, t0 + lane * kL, Lu);
+   for (int p = 0; p < S; p++) {
+      const int s = MODE == UNIT_ADJ_AGG ? S - 1 - p : p;
+      const float *tb = sTab + s * kBankTabFloats;
+      float w[kL];
+      const float2 entry = MODE == UNIT_OUT ? a.ckpt[base + p] : make_float2(0.0f, 0.0f);
+      float2 incl;
+      if (MODE == UNIT_ADJ_AGG) {
+         const float2 st = chunkStateDown(zeroStatePassRev(v, w, tb[3], tb[4]), entry, tb, lane, &incl);
+         correctAndOutputRev(w, v, tb, st.x, st.y);
+         if (lane == 0) a.agg[base + p] = incl;
+      }
+      else {
+         const float2 st = chunkStateUp(zeroStatePass(v, w, tb[3], tb[4]), entry, tb, lane, &incl);
          correctAndOutput(w, v, tb, st.x, st.y);
-         float *Ws = W + (size_t) s * kWRows * kBwdThreads + tid;
-#pragma unroll
-         for (int i = 0; i < kL; i++) Ws[i * kBwdThreads] = w[i];
-         Ws[kL * kBwdThreads] = st.x;       // w[-1]
-         Ws[(kL + 1) * kBwdThreads] = st.y; // w[-2]
+         if (MODE == UNIT_AGG && lane == 31) a.agg[base + p] = incl;
       }
+   }
+   if (MODE == UNIT_OUT) {
+      storePacked(v, a.out + c.xOff, t0, Lu, sStage[warp], lane);
+      if (t0 + kUnit >= Lu)
+         for (int t = Lu + lane; t < c.L; t += 32) a.out[c.xOff + t] = 0.0f;
+   }
+}
 
-      // 2. the stages' adjoints, last stage first, in reverse time
-      for (int s = S - 1; s >= 0; s--) {
-         const float *tb = sTab + s * kBankTabFloats;
-         const float b0 = tb[0], b1 = tb[1], b2 = tb[2], a1 = tb[3], a2 = tb[4];
-         float vz[kL];
-         {
-            float p1 = 0.0f, p2 = 0.0f;
+struct AdjArgs {
+   const RaggedChan *chans;
+   const int2 *units;
+   int nUnits;
+   int Smax;
+   const float *tables;
+   const float *u;       // FIR output plane
+   const float *gy;      // output gradient (packed)
+   const float2 *ckptF;  // forward checkpoints
+   const float2 *ckptA;  // adjoint checkpoints (processing order)
+   float *g;             // gradient w.r.t. the FIR output (packed)
+   float *part;          // 5 coefficient-gradient sums per unit and stage
+};
+
+// Stage sequences of one unit in shared memory: per stage (the last excepted, which
+// stays in registers) 16 rows of 32 lanes, so that the lanes of the warp touch
+// distinct banks.  One warp per CTA: the sequences are the bulk of the CTA's
+// shared memory, and single-warp CTAs pack the SM most tightly.
+__global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
+{
+   extern __shared__ float4 dynA[];
+   __shared__ float sStage[32 * kOutPad];
+   const int lane = threadIdx.x;
+   float *sTab = (float *) dynA;
+   float *W = sTab + (size_t) a.Smax * kBankTabFloats;
+   const int2 U = a.units[blockIdx.x];
+   const RaggedChan c = a.chans[U.x];
+   const int S = c.S, Lu = c.Lu, t0 = U.y * kUnit;
+   const long long base = c.ckOff + (long long) U.y * S;
+   loadTables(sTab, a.tables, c, lane);
+   float v[kL], w[kL];
+   loadChunk(v, a.u + c.pOff, t0 + lane * kL, Lu);
+   // 1. the forward of this unit from its checkpoints; every stage's sequence kept
+   for (int s = 0; s < S; s++) {
+      const float *tb = sTab + s * kBankTabFloats;
+      float2 incl;
+      const float2 st = chunkStateUp(zeroStatePass(v, w, tb[3], tb[4]), a.ckptF[base + s], tb, lane, &incl);
+      correctAndOutput(w, v, tb, st.x, st.y);
+      if (s + 1 < S) {
+         float *Ws = W + s * kL * 32 + lane;
 #pragma unroll
-            for (int i = kL - 1; i >= 0; i--) {
-               vz[i] = fmaf(-a1, p1, fmaf(-a2, p2, g[i]));
-               p2 = p1;
-               p1 = vz[i];
-            }
-         }
-         // reverse-time scan: lane L combines the chunks of lanes >= L
-         float2 val = make_float2(vz[0], vz[1]);
-#pragma unroll
-         for (int k = 0; k < 5; k++) {
-            const float2 o = shflDown(val, 1 << k);
-            if (lane + (1 << k) < 32) val = scan::affine(tabP(tb, k), o, val);
-         }
-         if (lane == 0) sAgg[warp] = val;
-         __syncthreads();
-         // partial sums of the stage before (one stage later in time) are complete in sRed
-         if (tid == 0 && s + 1 < S) {
-            double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-            for (int w = 0; w < kBwdWarps; w++)
-               for (int k = 0; k < 5; k++) acc[k] += (double) sRed[(s + 1) & 1][w][k];
-            for (int k = 0; k < 5; k++) a.gpart[(long long) (U.w + s + 1) * 5 + k] = acc[k];
-         }
-         if (warp == 0) {
-            float2 tv = lane < kBwdWarps ? sAgg[lane] : zero;
-#pragma unroll
-            for (int k = 0; k < 2; k++) {
-               const float2 o = shflDown(tv, 1 << k);
-               if (lane + (1 << k) < kBwdWarps) tv = scan::affine(tabP(tb, 5 + k), o, tv);
-            }
-            const float2 agg = scan::shflIdx(tv, 0);
-            float2 z = zero;
-            if (lane == 0 && U.z > 1) {
-               const int r = U.w + s;
-               const int preds = U.z - 1 - U.y; // later segments of the channel
-               const bool succ = U.y > 0;
-               if (preds == 0) {
-                  if (succ) publish(a.recs, a.flags, r, agg, 2);
-               }
-               else {
-                  if (succ) publish(a.recs, a.flags, r, agg, 1);
-                  z = lookBack(a.recs, a.flags, r - S, preds, S, tabP(tb, 7), a.limit, a.err);
-                  if (succ) publish(a.recs, a.flags, r, scan::affine(tabP(tb, 7), z, agg), 2);
-               }
-            }
-            z = scan::shflIdx(z, 0);
-            const float2 after = shflDown(tv, 1);
-            if (lane < kBwdWarps) {
-               float2 e = z;
-               const int m = kBwdWarps - 1 - lane;
-#pragma unroll
-               for (int k = 0; k < 2; k++)
-                  if ((m >> k) & 1) e = scan::affine(tabP(tb, 5 + k), e, zero);
-               if (lane + 1 < kBwdWarps) e = f2add(e, after);
-               sEntry[lane] = e;
-            }
-         }
-         __syncthreads();
-         // this chunk's reverse-time initial state (v[16], v[17])
-         float2 ex = shflDown(val, 1);
-         if (lane == 31) ex = zero;
-         float2 st = sEntry[warp];
-         const int m = 31 - lane;
-#pragma unroll
-         for (int k = 0; k < 5; k++)
-            if ((m >> k) & 1) st = scan::affine(tabP(tb, k), st, zero);
-         st = f2add(st, ex);
-         // forward sequence of this stage: wr[i + 2] = w[i], wr[1] = w[-1], wr[0] = w[-2]
-         float wr[kL + 2];
-         {
-            const float *Ws = W + (size_t) s * kWRows * kBwdThreads + tid;
-#pragma unroll
-            for (int i = 0; i < kL; i++) wr[i + 2] = Ws[i * kBwdThreads];
-            wr[1] = Ws[kL * kBwdThreads];
-            wr[0] = Ws[(kL + 1) * kBwdThreads];
-         }
-         float pb0 = 0.0f, pb1 = 0.0f, pb2 = 0.0f, pa1 = 0.0f, pa2 = 0.0f;
-         float n1 = st.x, n2 = st.y; // v[i+1], v[i+2]
-#pragma unroll
-         for (int i = kL - 1; i >= 0; i--) {
-            const float2 ab = *(const float2 *) (tb + kTabAB + 2 * (kL - 1 - i));
-            const float vi = fmaf(ab.x, st.x, fmaf(ab.y, st.y, vz[i]));
-            const float lam = fmaf(b0, vi, fmaf(b1, n1, b2 * n2));
-            n2 = n1;
-            n1 = vi;
-            pb0 = fmaf(g[i], wr[i + 2], pb0);
-            pb1 = fmaf(g[i], wr[i + 1], pb1);
-            pb2 = fmaf(g[i], wr[i], pb2);
-            pa1 = fmaf(-lam, wr[i + 1], pa1);
-            pa2 = fmaf(-lam, wr[i], pa2);
-            g[i] = lam;
-         }
-         float p[5] = {pb0, pb1, pb2, pa1, pa2};
-#pragma unroll
-         for (int k = 0; k < 5; k++) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) p[k] += __shfl_xor_sync(0xffffffffu, p[k], o);
-         }
-         if (lane == 0)
-#pragma unroll
-            for (int k = 0; k < 5; k++) sRed[s & 1][warp][k] = p[k];
+         for (int i = 0; i < kL; i++) Ws[i * 32] = w[i];
       }
-      // input gradient of the cascade (gradient w.r.t. the FIR output), coalesced store
+   }
+   // 2. the stages' adjoints, last stage first, in reverse time
+   float g[kL];
+   loadPacked(g, a.gy + c.xOff, t0, Lu, sStage, lane);
+   for (int p = 0; p < S; p++) {
+      const int s = S - 1 - p;
+      const float *tb = sTab + s * kBankTabFloats;
+      float vz[kL], lam[kL];
+      float2 incl;
+      const float2 st = chunkStateDown(zeroStatePassRev(g, vz, tb[3], tb[4]), a.ckptA[base + p], tb, lane, &incl);
+      correctAndOutputRev(vz, lam, tb, st.x, st.y);
+      // forward sequence of this stage: wr[i + 2] = w[i]; w[-1], w[-2] are the previous
+      // lane's last two samples (lane 0: the unit's checkpoint state)
+      float wr[kL + 2];
+      if (p > 0) {
+         const float *Ws = W + s * kL * 32 + lane;
 #pragma unroll
-      for (int i = 0; i < kL; i++) sIO[tid * kOutPad + i] = g[i];
-      __syncthreads();
-      if (tid == 0 && S > 0) {
-         double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-         for (int w = 0; w < kBwdWarps; w++)
-            for (int k = 0; k < 5; k++) acc[k] += (double) sRed[0][w][k];
-         for (int k = 0; k < 5; k++) a.gpart[(long long) U.w * 5 + k] = acc[k];
+         for (int i = 0; i < kL; i++) wr[i + 2] = Ws[i * 32];
       }
-      for (int k = tid; k < n; k += kBwdThreads) a.g[c.xOff + segStart + k] = sIO[(k >> 4) * kOutPad + (k & 15)];
-      // the last segment of the channel to finish sums the coefficient gradients in segment order
-      if (S > 0) {
-         __threadfence();
-         __syncthreads();
-         if (tid == 0) sLast = atomicAdd(a.chanDone + U.x, 1) == U.z - 1;
-         __syncthreads();
-         if (sLast) {
-            __threadfence();
-            const int r0 = U.w - (U.z - 1 - U.y) * S; // records of segment U.z - 1 (the channel's first ticket)
-            for (int q = tid; q < 5 * S; q += kBwdThreads) {
-               double acc = 0.0;
-               for (int j = 0; j < U.z; j++) acc += __ldcg(a.gpart + (long long) (r0 + (U.z - 1 - j) * S) * 5 + q);
-               a.gcoefs[c.cOff + q] = (float) acc;
-            }
-         }
+      else {
+#pragma unroll
+         for (int i = 0; i < kL; i++) wr[i + 2] = w[i];
       }
-      __syncthreads(); // shared memory is reused by the next segment
+      wr[1] = __shfl_up_sync(0xffffffffu, wr[kL + 1], 1);
+      wr[0] = __shfl_up_sync(0xffffffffu, wr[kL], 1);
+      if (lane == 0) {
+         const float2 e = a.ckptF[base + s];
+         wr[1] = e.x;
+         wr[0] = e.y;
+      }
+      float pr[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+      for (int i = 0; i < kL; i++) {
+         pr[0] = fmaf(g[i], wr[i + 2], pr[0]);
+         pr[1] = fmaf(g[i], wr[i + 1], pr[1]);
+         pr[2] = fmaf(g[i], wr[i], pr[2]);
+         pr[3] = fmaf(-lam[i], wr[i + 1], pr[3]);
+         pr[4] = fmaf(-lam[i], wr[i], pr[4]);
+         g[i] = lam[i];
+      }
+#pragma unroll
+      for (int k = 0; k < 5; k++) {
+#pragma unroll
+         for (int o = 16; o > 0; o >>= 1) pr[k] += __shfl_xor_sync(0xffffffffu, pr[k], o);
+      }
+      if (lane < 5) {
+         float val = pr[0];
+#pragma unroll
+         for (int k = 1; k < 5; k++)
+            if (lane == k) val = pr[k];
+         a.part[(base + s) * 5 + lane] = val;
+      }
+   }
+   storePacked(g, a.g + c.xOff, t0, Lu, sStage, lane);
+}
+
+// Coefficient gradients of one channel (one warp): the units' partial sums in unit order, FP64.
+__global__ void __launch_bounds__(32) bank_coef_kernel(const RaggedChan *chans, const float *part, float *gcoefs)
+{
+   const RaggedChan c = chans[blockIdx.x];
+   const int S = c.S, units = (c.Lu + kUnit - 1) / kUnit;
+   for (int q = threadIdx.x; q < 5 * S; q += 32) {
+      double acc = 0.0;
+      for (int j = 0; j < units; j++) acc += (double) part[(c.ckOff + (long long) j * S) * 5 + q];
+      gcoefs[c.cOff + q] = (float) acc;
    }
 }
 
 } // namespace
 
-cudaError_t launchBankTables(const float *coefs, int totalStages, float *tables, cudaStream_t s)
+long long bankTransitionDoubles(int S) { return 4LL * S * (S + 1); } // both directions
+
+cudaError_t launchBankTables(const RaggedChan *chans, int C, const float *coefs, int totalStages, int Smax,
+                             float *tables, double *phi, cudaStream_t s)
 {
    if (totalStages <= 0) return cudaSuccess;
    bank_tables_kernel<<<(totalStages + 127) / 128, 128, 0, s>>>(coefs, totalStages, tables);
+   const size_t dyn = (size_t) 8 * Smax * (Smax + 1) / 2 * sizeof(double);
+   cudaError_t e = cudaFuncSetAttribute(bank_transition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dyn);
+   if (e != cudaSuccess) return e;
+   bank_transition_kernel<<<dim3(C, 2), 128, dyn, s>>>(chans, coefs, phi);
+   countLaunch(2);
+   return cudaGetLastError();
+}
+
+static size_t unitShared(int Smax) { return (size_t) kWarps * Smax * kBankTabFloats * sizeof(float); }
+static size_t adjointShared(int Smax)
+{
+   return ((size_t) Smax * kBankTabFloats + (size_t) (Smax > 0 ? Smax - 1 : 0) * kL * 32) * sizeof(float);
+}
+
+template <int MODE> static cudaError_t launchUnits(const UnitArgs &a, cudaStream_t s)
+{
+   const size_t dyn = unitShared(a.Smax);
+   cudaError_t e = cudaFuncSetAttribute(bank_unit_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dyn);
+   if (e != cudaSuccess) return e;
+   bank_unit_kernel<MODE><<<(a.nUnits + kWarps - 1) / kWarps, kThreads, dyn, s>>>(a);
    countLaunch();
    return cudaGetLastError();
 }
@@ -576,56 +579,40 @@ cudaError_t launchBankTables(const float *coefs, int totalStages, float *tables,
 cudaError_t launchBankForward(const BankLaunch &b, cudaStream_t s)
 {
    if (b.nUnits <= 0) return cudaSuccess;
-   const size_t dyn = (size_t) b.Smax * kBankTabFloats * sizeof(float);
-   cudaError_t e = cudaFuncSetAttribute(bank_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dyn);
+   UnitArgs a{b.chans, b.units, b.nUnits, b.Smax, b.tables, b.u, nullptr, b.aggF, nullptr};
+   cudaError_t e = launchUnits<UNIT_AGG>(a, s);
    if (e != cudaSuccess) return e;
-   FwdArgs a{b.chans, b.units, b.tables, b.u, b.y, b.ckpt, b.recs, b.flags, b.ticket, b.err, b.waitLimit};
-   bank_fwd_kernel<<<b.nUnits, kFwdThreads, dyn, s>>>(a);
+   const size_t dynC = (size_t) (4 * b.Smax * (b.Smax + 1) / 2 + 2 * b.Smax) * sizeof(double);
+   if ((e = cudaFuncSetAttribute(bank_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dynC)) !=
+       cudaSuccess)
+      return e;
+   bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.phi, b.aggF, b.ckptF, 0);
    countLaunch();
-   return cudaGetLastError();
+   a.out = b.y;
+   a.ckpt = b.ckptF;
+   return launchUnits<UNIT_OUT>(a, s);
 }
 
-size_t bankBackwardShared(int Smax, bool wInShared)
-{
-   return (size_t) Smax * kBankTabFloats * sizeof(float) +
-          (wInShared ? (size_t) Smax * kWRows * kBwdThreads * sizeof(float) : 0);
-}
-
-bool bankBackwardFitsShared(int Smax) { return bankBackwardShared(Smax, true) <= kBankBwdSharedLimit; }
-
-long long bankBackwardGlobalFloats(int Smax, int ctas) { return (long long) ctas * Smax * kWRows * kBwdThreads; }
-
-cudaError_t launchBankBackward(const BankLaunch &b, int ctas, cudaStream_t s)
+cudaError_t launchBankBackward(const BankLaunch &b, cudaStream_t s)
 {
    if (b.nUnits <= 0) return cudaSuccess;
-   const bool inShared = bankBackwardFitsShared(b.Smax);
-   const size_t dyn = bankBackwardShared(b.Smax, inShared);
-   cudaError_t e = cudaFuncSetAttribute(bank_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dyn);
+   UnitArgs a{b.chans, b.units, b.nUnits, b.Smax, b.tables, b.gy, nullptr, b.aggA, nullptr};
+   cudaError_t e = launchUnits<UNIT_ADJ_AGG>(a, s);
    if (e != cudaSuccess) return e;
-   BwdArgs a{b.chans, b.units, b.nUnits, b.tables, b.u, b.gy, b.ckpt, b.g, b.recs, b.flags, b.gpart,
-             b.chanDone, b.ticket, b.gcoefs, b.err, b.waitLimit, b.wGlobal, inShared ? 1 : 0, b.Smax};
-   bank_bwd_kernel<<<ctas, kBwdThreads, dyn, s>>>(a);
-   countLaunch();
+   const size_t dynC = (size_t) (4 * b.Smax * (b.Smax + 1) / 2 + 2 * b.Smax) * sizeof(double);
+   if ((e = cudaFuncSetAttribute(bank_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dynC)) !=
+       cudaSuccess)
+      return e;
+   bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.phi, b.aggA, b.ckptA, 1);
+   const size_t dyn = adjointShared(b.Smax);
+   if ((e = cudaFuncSetAttribute(bank_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dyn)) !=
+       cudaSuccess)
+      return e;
+   AdjArgs d{b.chans, b.units, b.nUnits, b.Smax, b.tables, b.u, b.gy, b.ckptF, b.ckptA, b.g, b.part};
+   bank_adjoint_kernel<<<b.nUnits, 32, dyn, s>>>(d);
+   bank_coef_kernel<<<b.C, 32, 0, s>>>(b.chans, b.part, b.gcoefs);
+   countLaunch(3);
    return cudaGetLastError();
-}
-
-int bankBackwardCtas(int Smax, int nUnits)
-{
-   const bool inShared = bankBackwardFitsShared(Smax);
-   const size_t dyn = bankBackwardShared(Smax, inShared);
-   int dev = 0, sms = 148, perSm = 1;
-   if (cudaGetDevice(&dev) == cudaSuccess) (void) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-   if (cudaFuncSetAttribute(bank_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dyn) ==
-           cudaSuccess &&
-       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, bank_bwd_kernel, kBwdThreads, dyn) == cudaSuccess) {
-      if (perSm < 1) perSm = 1;
-   }
-   else {
-      (void) cudaGetLastError();
-      perSm = 1;
-   }
-   const long long ctas = (long long) sms * perSm;
-   return (int) (ctas < nUnits ? ctas : nUnits);
 }
 
 } // namespace dsplib

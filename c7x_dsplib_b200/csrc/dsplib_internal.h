@@ -231,7 +231,8 @@ int firTcErrorFlag(bool clear);
 struct RaggedChan {
    long long xOff, hOff, cOff, pOff;
    int L, T, S, Lu;
-   long long ckOff; // first checkpoint (float2) of the channel: one per 512-sample span and stage
+   long long ckOff;  // first unit state (float2) of the channel: one per 512-sample unit and stage
+   long long phiOff; // first double of the channel's unit transitions
 };
 // Split-BF16x3 tensor-core FIR over a list of runs {channel, first tile, tiles, 0}
 // of kFirBfTile outputs: forward (valid correlation of the channel's x with its
@@ -244,45 +245,35 @@ int raggedPlanDevice(DSPLIB_gpu_raggedPlan plan);
 cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *in,
                                   const float *taps, float *out, bool dx, int Tmax, cudaStream_t s);
 
-// Cascade of the filter bank split along time (bank_scan.cu).  Forward segments of
-// kBankFwdSeg samples, adjoint segments of kBankBwdSeg, checkpoints every kBankSpan
-// samples; per stage a table of kBankTabFloats floats (coefficients, transition
-// powers, free-response rows).
-constexpr int kBankFwdSeg = 4096;
-constexpr int kBankBwdSeg = 2048;
+// Cascade of the filter bank split along time (bank_scan.cu): units of kBankSpan
+// samples (one warp each), chained per channel through the 2S-dimensional cascade
+// state; per stage a table of kBankTabFloats floats (coefficients, transition
+// powers, free-response rows), per channel the unit transitions of both directions.
 constexpr int kBankSpan = 512;
 constexpr int kBankTabFloats = 80;
-constexpr size_t kBankBwdSharedLimit = 200 * 1024; // stage sequences beyond this go to global scratch
-constexpr int kBankErrWait = 1;                    // error word bit: a look-back wait expired
-constexpr int kBankDefaultWaitPolls = 1 << 22;
 
 struct BankLaunch {
    const RaggedChan *chans;
-   const int4 *units; // {channel, segment, segments of the channel, first record}
+   int C;
+   const int2 *units; // (channel, unit index within the channel)
    int nUnits;
    int Smax;
    const float *tables;
+   const double *phi;
    const float *u;    // FIR output plane
    float *y;          // forward output
    const float *gy;   // adjoint: output gradient
    float *g;          // adjoint: gradient w.r.t. the FIR output
-   float2 *ckpt;
-   float4 *recs;
-   int *flags;
-   double *gpart;
-   int *chanDone;
-   int *ticket;
+   float2 *aggF, *ckptF, *aggA, *ckptA;
+   float *part;       // adjoint: 5 coefficient-gradient sums per unit and stage
    float *gcoefs;
-   int *err;
-   int waitLimit;
-   float *wGlobal;
 };
-cudaError_t launchBankTables(const float *coefs, int totalStages, float *tables, cudaStream_t s);
+// Doubles of both unit transitions of a channel of S stages.
+long long bankTransitionDoubles(int S);
+cudaError_t launchBankTables(const RaggedChan *chans, int C, const float *coefs, int totalStages, int Smax,
+                             float *tables, double *phi, cudaStream_t s);
 cudaError_t launchBankForward(const BankLaunch &b, cudaStream_t s);
-cudaError_t launchBankBackward(const BankLaunch &b, int ctas, cudaStream_t s);
-int bankBackwardCtas(int Smax, int nUnits);
-bool bankBackwardFitsShared(int Smax);
-long long bankBackwardGlobalFloats(int Smax, int ctas);
+cudaError_t launchBankBackward(const BankLaunch &b, cudaStream_t s);
 
 struct BiquadLaunch {
    const float *x;

@@ -11,23 +11,26 @@
 //                          input gradient (full convolution with the same taps)
 //                          as split-BF16x3 tcgen05 contractions over runs of
 //                          8192-output tiles, one run per CTA.
-//   bank_tables_kernel, bank_fwd_kernel, bank_bwd_kernel (bank_scan.cu)
-//                          the cascade split along time into segments filtered
-//                          by independent CTAs, chained by decoupled look-back;
-//                          the forward keeps a checkpoint state per 512-sample
-//                          span and stage, the adjoint recomputes each segment
-//                          from them (no stage output is stored).
+//   bank_tables_kernel, bank_transition_kernel, bank_unit_kernel, bank_chain_kernel,
+//   bank_adjoint_kernel, bank_coef_kernel (bank_scan.cu)
+//                          the cascade split along time into 512-sample units
+//                          (one warp each) chained per channel through the
+//                          cascade's 2S-dimensional state: unit aggregates, the
+//                          chain (one state per unit and stage: the checkpoints),
+//                          outputs; the adjoint the same in reverse time, with
+//                          each unit's forward recomputed from the checkpoints
+//                          (no stage output is stored).
+//   ragged_passthrough_kernel  channels without biquad stages: y = u, g = gy.
 //   fir_dh_partial_kernel / fir_dh_reduce_kernel  taps gradient
 //                          dh[T-1-c] = sum_j gu[j] x[j+c], split over tiles
 //                          and summed in tile order (deterministic).
 //   mse_partial_kernel / mse_reduce_kernel  loss and its gradient.
 //
 // Work buffer (forward -> adjoint, floats): FIR output plane (sum of round16(Lu)),
-// checkpoints, stage tables, forward look-back records and flags, ticket.
-// Scratch (adjoint): gradient w.r.t. u, adjoint records, coefficient-gradient
-// partial sums, flags, per-channel counters, ticket, taps-gradient partials (also
-// the loss partials), and the stage sequences of deep cascades that do not fit in
-// shared memory.  The flags, counters and tickets are cleared by each call.
+// forward checkpoints, forward unit aggregates, stage tables, unit transitions.
+// Scratch (adjoint): gradient w.r.t. u, adjoint aggregates and checkpoints,
+// coefficient-gradient partial sums per unit and stage, taps-gradient partials
+// (also the loss partials).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,24 +48,21 @@ struct RaggedPlan {
    int C = 0;
    long long totalLen = 0, totalTaps = 0, totalCoefs = 0, totalOut = 0;
    long long planeStride = 0; // floats of the FIR output plane: sum of round16(Lu)
-   int Smax = 0, Tmax = 0, totalStages = 0;
-   int nFwdItems = 0, nFirFwdRuns = 0, nFirDxRuns = 0;
-   int nFwdUnits = 0, nBwdUnits = 0, nFwdRecs = 0, nBwdRecs = 0, bwdCtas = 0;
-   long long nCk = 0; // checkpoints (float2)
+   int Smax = 0, Tmax = 0, totalStages = 0, noStage = 0;
+   int nFwdItems = 0, nFirFwdRuns = 0, nFirDxRuns = 0, nUnits = 0;
+   long long nCk = 0;  // unit states (float2): sum over channels of units x stages
+   long long nPhi = 0; // doubles of the unit transitions
    RaggedChan *dChan = nullptr;
    int2 *dFwdItems = nullptr;   // (channel, 2048-sample tile over Lu): taps-gradient partials, loss
    int4 *dFirFwdRuns = nullptr; // (channel, first tile, tiles): FIR forward, 8192-output tiles over Lu
    int4 *dFirDxRuns = nullptr;  // the same over L: FIR input gradient
    int *dFwdStart = nullptr;    // first forward item of each channel (C + 1 entries)
-   int4 *dFwdUnits = nullptr;   // cascade forward segments: channels longest first, time order
-   int4 *dBwdUnits = nullptr;   // cascade adjoint segments: channels longest first, reverse time order
-   int *dErr = nullptr;         // error word (kBankErrWait, ...)
-   int waitLimit = kBankDefaultWaitPolls;
+   int2 *dUnits = nullptr;      // cascade units (channel, unit index)
    int device = 0;
    // work buffer layout (float offsets)
-   long long wCk = 0, wTab = 0, wRec = 0, wFlag = 0, wTicket = 0, wTotal = 0;
+   long long wCk = 0, wAgg = 0, wTab = 0, wPhi = 0, wTotal = 0;
    // scratch layout (float offsets)
-   long long sRec = 0, sPart = 0, sFlag = 0, sDone = 0, sTicket = 0, sDh = 0, sW = 0, sTotal = 0;
+   long long sAgg = 0, sCk = 0, sPart = 0, sDh = 0, sTotal = 0;
 };
 
 namespace {
@@ -188,6 +188,19 @@ __global__ void __launch_bounds__(1024) mse_reduce_kernel(const double *part, in
    if (threadIdx.x == 0) loss[0] = (float) (red[0] * invCount);
 }
 
+// Channels without biquad stages: the cascade is the identity (forward y = u with the
+// T - 1 tail samples zero; adjoint g = gy).  One CTA per channel; others return.
+__global__ void __launch_bounds__(256) ragged_passthrough_kernel(const RaggedChan *chans, const float *in, float *out,
+                                                                 int fromPlane)
+{
+   const RaggedChan c = chans[blockIdx.x];
+   if (c.S != 0) return;
+   const float *src = in + (fromPlane ? c.pOff : c.xOff);
+   for (int t = threadIdx.x; t < c.Lu; t += 256) out[c.xOff + t] = src[t];
+   if (fromPlane)
+      for (int t = c.Lu + threadIdx.x; t < c.L; t += 256) out[c.xOff + t] = 0.0f;
+}
+
 template <typename T> cudaError_t upload(T **dst, const std::vector<T> &v)
 {
    cudaError_t e = cudaMalloc((void **) dst, std::max<size_t>(1, v.size()) * sizeof(T));
@@ -206,9 +219,7 @@ static void freePlan(RaggedPlan *p)
    cudaFree(p->dFirFwdRuns);
    cudaFree(p->dFirDxRuns);
    cudaFree(p->dFwdStart);
-   cudaFree(p->dFwdUnits);
-   cudaFree(p->dBwdUnits);
-   cudaFree(p->dErr);
+   cudaFree(p->dUnits);
    delete p;
 }
 
@@ -257,15 +268,15 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    RaggedPlan *p = new RaggedPlan();
    p->C = numChannels;
    std::vector<RaggedChan> ch(numChannels);
-   std::vector<int2> fwd;
-   std::vector<int4> firFwd, firDx, fwdUnits, bwdUnits;
-   std::vector<int> start(numChannels + 1), order(numChannels);
+   std::vector<int2> fwd, units;
+   std::vector<int4> firFwd, firDx;
+   std::vector<int> start(numChannels + 1);
    // runs of up to kFirBfRunTiles consecutive 8192-output tiles of one channel
    auto addRuns = [](std::vector<int4> &runs, int c, int outLen) {
       const int tiles = (outLen + kFirBfTile - 1) / kFirBfTile;
       for (int t = 0; t < tiles; t += kFirBfRunTiles) runs.push_back(make_int4(c, t, std::min(kFirBfRunTiles, tiles - t), 0));
    };
-   long long xo = 0, ho = 0, co = 0, po = 0, ck = 0;
+   long long xo = 0, ho = 0, co = 0, po = 0, ck = 0, ph = 0;
    for (int c = 0; c < numChannels; c++) {
       const int L = length[c], T = taps[c], S = stages[c];
       if (T < 1 || T > kFirBfMaxTaps || L < T || S < 0 || S > kRaggedMaxStages) {
@@ -273,37 +284,31 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
          return DSPLIB_ERR_INVALID_DIMENSION;
       }
       const int Lu = L - T + 1;
-      ch[c] = RaggedChan{xo, ho, co, po, L, T, S, Lu, ck};
+      const int nu = (Lu + kBankSpan - 1) / kBankSpan;
+      ch[c] = RaggedChan{xo, ho, co, po, L, T, S, Lu, ck, ph};
       po += (Lu + 15) & ~15;
-      ck += (long long) ((Lu + kBankSpan - 1) / kBankSpan) * S;
+      ck += (long long) nu * S;
+      ph += bankTransitionDoubles(S);
       xo += L;
       p->totalOut += Lu;
       ho += T;
       co += 5LL * S;
       p->Smax = std::max(p->Smax, S);
       p->Tmax = std::max(p->Tmax, T);
+      if (S == 0) p->noStage++;
       start[c] = (int) fwd.size();
       for (int t = 0; t * kRTile < Lu; t++) fwd.push_back(make_int2(c, t));
+      if (S > 0)
+         for (int j = 0; j < nu; j++) units.push_back(make_int2(c, j));
       addRuns(firFwd, c, Lu);
       addRuns(firDx, c, L);
-      order[c] = c;
    }
    start[numChannels] = (int) fwd.size();
    // longest runs first, so the short ones fill in behind them
    auto longer = [](const int4 &a, const int4 &b) { return a.z > b.z; };
    std::stable_sort(firFwd.begin(), firFwd.end(), longer);
    std::stable_sort(firDx.begin(), firDx.end(), longer);
-   // cascade segments: channels by decreasing length; the forward takes a channel's
-   // segments in time order, the adjoint in reverse, so each look-back goes to earlier tickets
-   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ch[a].Lu > ch[b].Lu; });
-   long long fr = 0, br = 0;
-   for (int c : order) {
-      const int S = ch[c].S, Lu = ch[c].Lu;
-      const int nf = (Lu + kBankFwdSeg - 1) / kBankFwdSeg, nb = (Lu + kBankBwdSeg - 1) / kBankBwdSeg;
-      for (int k = 0; k < nf; k++, fr += S) fwdUnits.push_back(make_int4(c, k, nf, (int) fr));
-      for (int k = nb - 1; k >= 0; k--, br += S) bwdUnits.push_back(make_int4(c, k, nb, (int) br));
-   }
-   if (fr > INT_MAX || br > INT_MAX || co / 5 > INT_MAX) {
+   if (co / 5 > INT_MAX || units.size() > (size_t) INT_MAX) {
       delete p;
       return DSPLIB_ERR_INVALID_DIMENSION;
    }
@@ -313,36 +318,27 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    p->totalCoefs = co;
    p->totalStages = (int) (co / 5);
    p->nCk = ck;
+   p->nPhi = ph;
    p->nFwdItems = (int) fwd.size();
    p->nFirFwdRuns = (int) firFwd.size();
    p->nFirDxRuns = (int) firDx.size();
-   p->nFwdUnits = (int) fwdUnits.size();
-   p->nBwdUnits = (int) bwdUnits.size();
-   p->nFwdRecs = (int) fr;
-   p->nBwdRecs = (int) br;
+   p->nUnits = (int) units.size();
    cudaGetDevice(&p->device);
-   p->bwdCtas = bankBackwardCtas(p->Smax, p->nBwdUnits);
-   // work buffer: u | checkpoints | stage tables | records | flags | ticket
+   // work buffer: u | forward checkpoints | forward aggregates | stage tables | unit transitions
    p->wCk = align4(p->planeStride);
-   p->wTab = p->wCk + align4(2 * p->nCk);
-   p->wRec = p->wTab + (long long) kBankTabFloats * p->totalStages;
-   p->wFlag = p->wRec + 4LL * p->nFwdRecs;
-   p->wTicket = p->wFlag + align4(p->nFwdRecs);
-   p->wTotal = p->wTicket + 4;
-   // scratch: g | records | partial sums | flags | channel counters | ticket | taps partials | stage sequences
-   p->sRec = align4(p->totalLen);
-   p->sPart = p->sRec + 4LL * p->nBwdRecs;
-   p->sFlag = p->sPart + 10LL * p->nBwdRecs;
-   p->sDone = p->sFlag + align4(p->nBwdRecs);
-   p->sTicket = p->sDone + align4(numChannels);
-   p->sDh = p->sTicket + 4;
-   p->sW = p->sDh + align4((long long) p->nFwdItems * kDhMaxT);
-   p->sTotal = p->sW + (bankBackwardFitsShared(p->Smax) ? 0 : bankBackwardGlobalFloats(p->Smax, p->bwdCtas));
+   p->wAgg = p->wCk + align4(2 * p->nCk);
+   p->wTab = p->wAgg + align4(2 * p->nCk);
+   p->wPhi = p->wTab + (long long) kBankTabFloats * p->totalStages;
+   p->wTotal = p->wPhi + align4(2 * p->nPhi);
+   // scratch: g | adjoint aggregates | adjoint checkpoints | coefficient partials | taps partials
+   p->sAgg = align4(p->totalLen);
+   p->sCk = p->sAgg + align4(2 * p->nCk);
+   p->sPart = p->sCk + align4(2 * p->nCk);
+   p->sDh = p->sPart + align4(5 * p->nCk);
+   p->sTotal = p->sDh + align4((long long) p->nFwdItems * kDhMaxT);
    const bool ok = upload(&p->dChan, ch) == cudaSuccess && upload(&p->dFwdItems, fwd) == cudaSuccess &&
                    upload(&p->dFirFwdRuns, firFwd) == cudaSuccess && upload(&p->dFirDxRuns, firDx) == cudaSuccess &&
-                   upload(&p->dFwdStart, start) == cudaSuccess && upload(&p->dFwdUnits, fwdUnits) == cudaSuccess &&
-                   upload(&p->dBwdUnits, bwdUnits) == cudaSuccess &&
-                   upload(&p->dErr, std::vector<int>(4, 0)) == cudaSuccess;
+                   upload(&p->dFwdStart, start) == cudaSuccess && upload(&p->dUnits, units) == cudaSuccess;
    if (!ok) {
       freePlan(p);
       return DSPLIB_ERR_FAILURE;
@@ -366,38 +362,26 @@ int64_t DSPLIB_gpu_raggedPlanSize(DSPLIB_gpu_raggedPlan plan, int32_t what)
    }
 }
 
-DSPLIB_STATUS DSPLIB_gpu_raggedPlanStatus(DSPLIB_gpu_raggedPlan plan, void *stream)
-{
-   RaggedPlan *p = (RaggedPlan *) plan;
-   if (!p) return DSPLIB_ERR_NULL_POINTER;
-   PlanDevice dev(p);
-   if (!dev.ok()) return DSPLIB_ERR_FAILURE;
-   cudaStream_t s = (cudaStream_t) stream;
-   int word = 0;
-   if (cudaMemcpyAsync(&word, p->dErr, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-       cudaStreamSynchronize(s) != cudaSuccess)
-      return DSPLIB_ERR_FAILURE;
-   if (word != 0) {
-      if (cudaMemsetAsync(p->dErr, 0, sizeof(int), s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
-         return DSPLIB_ERR_FAILURE;
-      return DSPLIB_ERR_FAILURE;
-   }
-   return DSPLIB_SUCCESS;
-}
-
-DSPLIB_STATUS DSPLIB_gpu_raggedPlanSetWaitLimit(DSPLIB_gpu_raggedPlan plan, int32_t polls)
-{
-   RaggedPlan *p = (RaggedPlan *) plan;
-   if (!p) return DSPLIB_ERR_NULL_POINTER;
-   if (polls < 0) return DSPLIB_ERR_INVALID_VALUE;
-   p->waitLimit = polls;
-   return DSPLIB_SUCCESS;
-}
-
 DSPLIB_STATUS DSPLIB_gpu_raggedPlanDestroy(DSPLIB_gpu_raggedPlan plan)
 {
    freePlan((RaggedPlan *) plan);
    return DSPLIB_SUCCESS;
+}
+
+static BankLaunch bankLaunch(const RaggedPlan *p, const float *work)
+{
+   BankLaunch b{};
+   b.chans = p->dChan;
+   b.C = p->C;
+   b.units = p->dUnits;
+   b.nUnits = p->nUnits;
+   b.Smax = p->Smax;
+   b.tables = work + p->wTab;
+   b.phi = (const double *) (work + p->wPhi);
+   b.u = work;
+   b.aggF = (float2 *) (work + p->wAgg);
+   b.ckptF = (float2 *) (work + p->wCk);
+   return b;
 }
 
 DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_fwd(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
@@ -409,27 +393,20 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_fwd(DSPLIB_gpu_raggedPlan plan, const 
    if (!dev.ok()) return DSPLIB_ERR_FAILURE;
    cudaStream_t s = (cudaStream_t) stream;
    float *u = work;
-   BankLaunch b{};
-   b.chans = p->dChan;
-   b.units = p->dFwdUnits;
-   b.nUnits = p->nFwdUnits;
-   b.Smax = p->Smax;
-   b.tables = work + p->wTab;
-   b.u = u;
+   BankLaunch b = bankLaunch(p, work);
    b.y = y;
-   b.ckpt = (float2 *) (work + p->wCk);
-   b.recs = (float4 *) (work + p->wRec);
-   b.flags = (int *) (work + p->wFlag);
-   b.ticket = (int *) (work + p->wTicket);
-   b.err = p->dErr;
-   b.waitLimit = p->waitLimit;
-   if (launchFirBf16x3Ragged(p->dChan, p->dFirFwdRuns, p->nFirFwdRuns, x, taps, u, false, p->Tmax, s) !=
-           cudaSuccess ||
-       cudaMemsetAsync(work + p->wFlag, 0, (size_t) (p->wTotal - p->wFlag) * sizeof(float), s) != cudaSuccess ||
-       launchBankTables(coefs, p->totalStages, work + p->wTab, s) != cudaSuccess ||
-       launchBankForward(b, s) != cudaSuccess)
+   if (launchFirBf16x3Ragged(p->dChan, p->dFirFwdRuns, p->nFirFwdRuns, x, taps, u, false, p->Tmax, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
-   return DSPLIB_SUCCESS;
+   if (p->nUnits > 0 &&
+       (launchBankTables(p->dChan, p->C, coefs, p->totalStages, p->Smax, work + p->wTab, (double *) (work + p->wPhi),
+                         s) != cudaSuccess ||
+        launchBankForward(b, s) != cudaSuccess))
+      return DSPLIB_ERR_FAILURE;
+   if (p->noStage > 0) {
+      ragged_passthrough_kernel<<<p->C, 256, 0, s>>>(p->dChan, u, y, 1);
+      countLaunch();
+   }
+   return cudaGetLastError() == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
 }
 
 DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
@@ -444,28 +421,18 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
    cudaStream_t s = (cudaStream_t) stream;
    float *g = scratch;              // gradient w.r.t. the FIR output
    float *part = scratch + p->sDh; // per-tile taps-gradient partials
-   BankLaunch b{};
-   b.chans = p->dChan;
-   b.units = p->dBwdUnits;
-   b.nUnits = p->nBwdUnits;
-   b.Smax = p->Smax;
-   b.tables = work + p->wTab;
-   b.u = work;
+   BankLaunch b = bankLaunch(p, work);
    b.gy = gy;
    b.g = g;
-   b.ckpt = (float2 *) (work + p->wCk);
-   b.recs = (float4 *) (scratch + p->sRec);
-   b.flags = (int *) (scratch + p->sFlag);
-   b.gpart = (double *) (scratch + p->sPart);
-   b.chanDone = (int *) (scratch + p->sDone);
-   b.ticket = (int *) (scratch + p->sTicket);
+   b.aggA = (float2 *) (scratch + p->sAgg);
+   b.ckptA = (float2 *) (scratch + p->sCk);
+   b.part = scratch + p->sPart;
    b.gcoefs = gcoefs;
-   b.err = p->dErr;
-   b.waitLimit = p->waitLimit;
-   b.wGlobal = scratch + p->sW;
-   if (cudaMemsetAsync(scratch + p->sFlag, 0, (size_t) (p->sDh - p->sFlag) * sizeof(float), s) != cudaSuccess ||
-       launchBankBackward(b, p->bwdCtas, s) != cudaSuccess)
-      return DSPLIB_ERR_FAILURE;
+   if (p->nUnits > 0 && launchBankBackward(b, s) != cudaSuccess) return DSPLIB_ERR_FAILURE;
+   if (p->noStage > 0) {
+      ragged_passthrough_kernel<<<p->C, 256, 0, s>>>(p->dChan, gy, g, 0);
+      countLaunch();
+   }
    if (launchFirBf16x3Ragged(p->dChan, p->dFirDxRuns, p->nFirDxRuns, g, taps, gx, true, p->Tmax, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
    fir_dh_partial_kernel<<<p->nFwdItems, 256, 0, s>>>(p->dChan, p->dFwdItems, x, g, part);

@@ -121,18 +121,6 @@ class RaggedFilterBank:
         if st != SUCCESS:
             raise DsplibError("DSPLIB_gpu_firBiquadBatched_bwd", st)
 
-    def status(self):
-        """Raise if a cross-segment wait of a call queued on this plan gave up (synchronises
-        torch's current stream; clears the plan's error word)."""
-        st = lib().DSPLIB_gpu_raggedPlanStatus(self._plan, _stream_ptr())
-        if st != SUCCESS:
-            raise DsplibError("DSPLIB_gpu_raggedPlanStatus", st)
-
-    def set_wait_limit(self, polls):
-        st = lib().DSPLIB_gpu_raggedPlanSetWaitLimit(self._plan, int(polls))
-        if st != SUCCESS:
-            raise DsplibError("DSPLIB_gpu_raggedPlanSetWaitLimit", st)
-
     def mse_grad_raw(self, y, target, gy, loss, scratch):
         """loss[0] = mean over valid samples of (y - target)^2; gy = its gradient (zero on tails)."""
         self._check(y, self.sizes[SAMPLES], "y")

@@ -118,11 +118,12 @@ typedef enum {
    DSPLIB_GPU_RAGGED_COEFS = 2,   /* floats in coefs / gcoefs (5 sum S_c) */
    DSPLIB_GPU_RAGGED_WORK = 3,    /* floats the forward leaves for the adjoint: the FIR output
                                      (sum_c round16(L_c - T_c + 1) floats), one 2-float state per
-                                     512 samples and stage (the cascade's checkpoints), per-stage
-                                     tables and the forward scan's records: about 4 bytes per sample
-                                     plus 0.03 per sample and stage; no stage output is kept */
-   DSPLIB_GPU_RAGGED_SCRATCH = 4, /* floats of adjoint scratch (about 4 bytes per sample plus the
-                                     scan's records and partial sums) */
+                                     512 samples and stage (the cascade's checkpoints) and the
+                                     unit aggregates, per-stage tables and per-channel unit
+                                     transitions: about 4 bytes per sample plus 0.03 per sample
+                                     and stage; no stage output is kept */
+   DSPLIB_GPU_RAGGED_SCRATCH = 4, /* floats of adjoint scratch (about 4 bytes per sample plus
+                                     0.07 per sample and stage) */
    DSPLIB_GPU_RAGGED_OUTPUTS = 5, /* valid output samples (sum L_c - T_c + 1) */
 } DSPLIB_gpu_raggedSize;
 
@@ -138,9 +139,7 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanDestroy(DSPLIB_gpu_raggedPlan plan);
 /** Forward: y from x, taps and coefs.  work (16-byte aligned) receives the FIR
  *  output and the cascade's checkpoint states (what the adjoint needs; it
  *  recomputes the stage outputs from them).  Queued on `stream`; no allocation,
- *  no host synchronisation.  The cascade is split along time into segments that
- *  wait, boundedly, for the states of the segments before them; if such a wait
- *  gives up, the plan's error word is set (DSPLIB_gpu_raggedPlanStatus). */
+ *  no host synchronisation. */
 DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_fwd(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
                                               const float *coefs, float *y, float *work, void *stream);
 /** Adjoint: given gy = dLoss/dy and the forward's work buffer, writes
@@ -156,16 +155,6 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
  *  is a DSPLIB_GPU_RAGGED_SCRATCH buffer (the same one the adjoint takes). */
 DSPLIB_STATUS DSPLIB_gpu_raggedMseGrad(DSPLIB_gpu_raggedPlan plan, const float *y, const float *target, float *gy,
                                        float *loss, float *scratch, void *stream);
-
-/** Whether every forward / adjoint queued on this plan so far ran its cross-segment
- *  waits to completion: DSPLIB_SUCCESS, or DSPLIB_ERR_FAILURE when a bounded wait
- *  gave up (the outputs of that call are then not valid) -- the error word is
- *  cleared by the query.  Synchronises `stream` (the one the calls were queued on). */
-DSPLIB_STATUS DSPLIB_gpu_raggedPlanStatus(DSPLIB_gpu_raggedPlan plan, void *stream);
-/** Polls after which a cross-segment wait gives up (default 4194304, each poll
- *  followed by a 64 ns pause); 0 makes every such wait give up at once, which
- *  exercises the failure path without a fault. */
-DSPLIB_STATUS DSPLIB_gpu_raggedPlanSetWaitLimit(DSPLIB_gpu_raggedPlan plan, int32_t polls);
 
 /** Size, in floats, of the scratch array built into the library for
  *  DSPLIB_gpu_firBiquadBatched_bwdStaticScratch (16 MiB per device). */
