@@ -242,6 +242,11 @@ constexpr int kFirBfRunTiles = 4;
 constexpr int kFirBfMaxTaps = 512;
 // Device the plan was built on (-1 for a null plan).
 int raggedPlanDevice(DSPLIB_gpu_raggedPlan plan);
+// Taps gradient of the filter bank on the tensor cores over runs {channel, first tile,
+// tiles, partial slot} of 8192 samples of the gradient at the FIR output:
+// part[slot * 512 + c] = sum over the run of gu[j] x[j + c], c < T.
+cudaError_t launchFirDhBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *x,
+                                    const float *gu, float *part, cudaStream_t s);
 cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *in,
                                   const float *taps, float *out, bool dx, int Tmax, cudaStream_t s);
 

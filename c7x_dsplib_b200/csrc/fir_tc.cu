@@ -862,6 +862,161 @@ __global__ void __launch_bounds__(kBfThreads, 1)
    bfEnd(L, pp, tmem, tid);
 }
 
+
+// ------------------------------------------------------------------ taps gradient (split-BF16x3)
+
+// Taps gradient of the filter bank, dh_lag[c] = sum_j gu[j] x[j + c] (c < T), on the
+// tensor cores.  With j = 64 r + s (row r, phase s) and t' = c + s:
+//     D[t'][s] = sum_r x[64 r + t'] gu[64 r + s],      dh_lag[c] = sum_s D[c + s][s],
+// a GEMM whose contraction runs over the rows r (time) and whose operands are both
+// the signal planes as staged for the forward kernels, read MN-major: A = X^T
+// (M = 128 positions t', 64 per 128-byte block, block r + t'/64 of the x plane, so the
+// second 64-wide atom of a tile starts one block (128 bytes) after the first), B = G
+// (N = 64 phases, block r of the gradient plane).  One accumulator tile per 128
+// positions (ceil((T + 63) / 128) <= 5 tiles of 64 TMEM columns) collects the three
+// split products x_hi g_hi + x_lo g_hi + x_hi g_lo over every row of a run of up to
+// four 8192-sample tiles; the diagonal sums are taken once per run, in a fixed order.
+// The next tile's planes are staged while the tensor core works on the current one.
+constexpr int kDhTile = kBfTile;                  // samples (128 rows) per staged tile
+constexpr int kDhMaxMt = (kBfMaxTaps + 63 + 127) / 128;
+constexpr int kDhXBlocks = 127 + 2 * kDhMaxMt;    // x blocks a tile's A operands reach
+constexpr size_t kDhXPlane = ((kDhXBlocks * 128 + 1023) / 1024) * 1024;
+constexpr size_t kDhGPlane = kRows * 128;
+constexpr size_t kDhBuf = 2 * kDhXPlane + 2 * kDhGPlane; // x hi, x lo, g hi, g lo
+constexpr size_t kDhSmem = 1024 + 2 * kDhBuf + 64;
+constexpr int kDhPitch = 65;                      // floats per staged accumulator row
+static_assert((size_t) kRows * kDhPitch * 4 <= kDhBuf, "accumulator staging fits one buffer");
+static_assert(kDhMaxMt * 64 <= 512, "accumulator tiles fit the TMEM columns");
+
+// MN-major operand with 128-byte swizzle: 64-element atoms (128-byte rows, 8 rows per
+// 1024-byte swizzle atom along K), lbo = byte distance between atoms along M/N,
+// sbo = byte distance between 8-row groups along K.
+__device__ __forceinline__ uint64_t descSw128Mn(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+   uint64_t d = 0;
+   d |= (uint64_t) ((saddr >> 4) & 0x3FFF);
+   d |= (uint64_t) ((lbo >> 4) & 0x3FFF) << 16;
+   d |= (uint64_t) ((sbo >> 4) & 0x3FFF) << 32;
+   d |= (uint64_t) 1 << 46;
+   d |= (uint64_t) 2 << 61;
+   return d;
+}
+
+__global__ void __launch_bounds__(kBfThreads, 1)
+    fir_dh_bf16x3_kernel(const RaggedChan *chans, const int4 *runs, const float *x, const float *gu, float *part)
+{
+   extern __shared__ __align__(16) unsigned char smraw[];
+   unsigned char *sm = (unsigned char *) (((uintptr_t) smraw + 1023) & ~(uintptr_t) 1023);
+   uint64_t *mbar = (uint64_t *) (sm + 2 * kDhBuf); // one per buffer
+   uint32_t *tslot = (uint32_t *) (mbar + 2);
+   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+   const int4 run = runs[blockIdx.x]; // {channel, first tile, tiles, partial slot}
+   const RaggedChan c = chans[run.x];
+   const int T = c.T;
+   const int Mt = (T + 63 + 127) / 128;
+   const int nbX = 127 + 2 * Mt;
+   const float *xc = x + c.xOff, *gc = gu + c.xOff;
+   auto buf = [&](int b) { return sm + (size_t) b * kDhBuf; };
+   auto stage = [&](int t, int b) {
+      unsigned char *B = buf(b);
+      const long long q0 = (long long) t * kDhTile;
+      bfStage(xc, q0, c.L, nbX, B, B + kDhXPlane, tid);
+      bfStage(gc, q0, c.Lu, kRows, B + 2 * kDhXPlane, B + 2 * kDhXPlane + kDhGPlane, tid);
+   };
+   if (warp == 0) tc::tmemAlloc(tslot, 512);
+   if (tid == 0) {
+      tc::mbarInit(mbar, 1);
+      tc::mbarInit(mbar + 1, 1);
+      tc::fenceMbarInit();
+   }
+   stage(run.y, 0);
+   tc::fenceProxyAsync();
+   tc::fenceBeforeSync();
+   __syncthreads();
+   tc::fenceAfterSync();
+   const uint32_t tmem = *tslot;
+   const uint32_t id = tc::idesc(1, 1, 1, kRows, 64) | (1u << 15) | (1u << 16); // both operands MN-major
+   uint32_t par[2] = {0, 0};
+   bool ok = true;
+   for (int k = 0; k < run.z && ok; k++) {
+      const int b = k & 1;
+      if (tid == 0) {
+         tc::fenceAfterSync();
+         unsigned char *B = buf(b);
+         const uint32_t xh = tc::smemAddr(B), xl = tc::smemAddr(B + kDhXPlane);
+         const uint32_t gh = tc::smemAddr(B + 2 * kDhXPlane), gl = tc::smemAddr(B + 2 * kDhXPlane + kDhGPlane);
+         for (int ks = 0; ks < kRows / 16; ks++) {
+            const uint64_t dGh = descSw128Mn(gh + ks * 2048, 128, 1024);
+            const uint64_t dGl = descSw128Mn(gl + ks * 2048, 128, 1024);
+            for (int m = 0; m < Mt; m++) {
+               const uint32_t off = (uint32_t) (ks * 16 + 2 * m) * 128;
+               const uint64_t dXh = descSw128Mn(xh + off, 128, 1024);
+               const uint64_t dXl = descSw128Mn(xl + off, 128, 1024);
+               const uint32_t d = tmem + 64 * m;
+               tc::mmaF16(d, dXh, dGh, id, k > 0 || ks > 0);
+               tc::mmaF16(d, dXl, dGh, id, true);
+               tc::mmaF16(d, dXh, dGl, id, true);
+            }
+         }
+         tc::commit(mbar + b);
+      }
+      if (k + 1 < run.z) {
+         // the other buffer is free once the MMAs of the tile before this one completed
+         if (k >= 1) {
+            const bool done = tid == 0 ? tc::mbarWait(mbar + (1 - b), par[1 - b]) : true;
+            par[1 - b] ^= 1;
+            if (!done && tid == 0) atomicExch(&g_firTcError, 1);
+            ok = !__syncthreads_or(!done);
+            if (!ok) break;
+         }
+         stage(run.y + k + 1, 1 - b);
+         tc::fenceProxyAsync();
+         tc::fenceBeforeSync();
+         __syncthreads();
+      }
+   }
+   // The loop waited for tiles 0 .. n-3; wait for the last two (bounded: after a failure
+   // above, waits for tiles never issued give up, and the kernel returns).
+   bool fail = !ok;
+   for (int k = run.z >= 2 ? run.z - 2 : 0; k < run.z; k++) {
+      const int b = k & 1;
+      const bool done = tid == 0 ? tc::mbarWait(mbar + b, par[b]) : true;
+      par[b] ^= 1;
+      if (!done && tid == 0) {
+         atomicExch(&g_firTcError, 1);
+         fail = true;
+      }
+   }
+   if (__syncthreads_or(fail)) {
+      if (warp == 0) tc::tmemFree(tmem, 512);
+      return;
+   }
+   tc::fenceAfterSync();
+   // diagonal sums: lag c (thread c) adds D[c + s][s] over s, accumulator tile by tile
+   float acc = 0.0f;
+   float *Ds = (float *) buf(0);
+   for (int m = 0; m < Mt; m++) {
+      {
+         const int quad = warp & 3, cg = warp >> 2; // TMEM lanes 32 quad.., columns 16 cg..
+         uint32_t r[16];
+         tc::tmemLoad16(tmem + ((uint32_t) (quad * 32) << 16) + 64 * m + 16 * cg, r);
+         tc::tmemWaitLoad();
+         float *row = Ds + (quad * 32 + lane) * kDhPitch + 16 * cg;
+#pragma unroll
+         for (int i = 0; i < 16; i++) row[i] = __uint_as_float(r[i]);
+      }
+      __syncthreads();
+      if (tid < T) {
+         const int lo = max(0, 128 * m - tid), hi = min(63, 128 * m + 127 - tid);
+         for (int sp = lo; sp <= hi; sp++) acc += Ds[(tid + sp - 128 * m) * kDhPitch + sp];
+      }
+      __syncthreads();
+   }
+   if (tid < T) part[(long long) run.w * kBfMaxTaps + tid] = acc;
+   tc::fenceBeforeSync();
+   __syncthreads();
+   if (warp == 0) tc::tmemFree(tmem, 512);
+}
 } // namespace
 
 bool firIntTcSupported(const FirLaunch &a)
@@ -903,6 +1058,18 @@ cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int
        cudaFuncSetAttribute(fir_bf16x3_ragged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
    if (e != cudaSuccess) return e;
    fir_bf16x3_ragged_kernel<<<nRuns, kBfThreads, smem, s>>>(chans, runs, in, taps, out, dx ? 1 : 0, Tmax);
+   countLaunch();
+   return cudaGetLastError();
+}
+
+cudaError_t launchFirDhBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *x,
+                                    const float *gu, float *part, cudaStream_t s)
+{
+   if (nRuns <= 0) return cudaSuccess;
+   cudaError_t e =
+       cudaFuncSetAttribute(fir_dh_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kDhSmem);
+   if (e != cudaSuccess) return e;
+   fir_dh_bf16x3_kernel<<<nRuns, kBfThreads, kDhSmem, s>>>(chans, runs, x, gu, part);
    countLaunch();
    return cudaGetLastError();
 }

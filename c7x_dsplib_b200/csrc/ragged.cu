@@ -21,9 +21,10 @@
 //                          each unit's forward recomputed from the checkpoints
 //                          (no stage output is stored).
 //   ragged_passthrough_kernel  channels without biquad stages: y = u, g = gy.
-//   fir_dh_partial_kernel / fir_dh_reduce_kernel  taps gradient
-//                          dh[T-1-c] = sum_j gu[j] x[j+c], split over tiles
-//                          and summed in tile order (deterministic).
+//   fir_dh_bf16x3_kernel (fir_tc.cu) / fir_dh_reduce_kernel  taps gradient
+//                          dh[T-1-c] = sum_j gu[j] x[j+c] as split-BF16x3
+//                          tcgen05 contractions over runs of 8192-sample tiles,
+//                          partial sums per run added in run order (deterministic).
 //   mse_partial_kernel / mse_reduce_kernel  loss and its gradient.
 //
 // Work buffer (forward -> adjoint, floats): FIR output plane (sum of round16(Lu)),
@@ -56,7 +57,9 @@ struct RaggedPlan {
    int2 *dFwdItems = nullptr;   // (channel, 2048-sample tile over Lu): taps-gradient partials, loss
    int4 *dFirFwdRuns = nullptr; // (channel, first tile, tiles): FIR forward, 8192-output tiles over Lu
    int4 *dFirDxRuns = nullptr;  // the same over L: FIR input gradient
-   int *dFwdStart = nullptr;    // first forward item of each channel (C + 1 entries)
+   int *dDhStart = nullptr;     // first taps-gradient slot of each channel (C + 1 entries)
+   int4 *dDhRuns = nullptr;     // (channel, first tile, tiles, slot): taps gradient, longest first
+   int nDhRuns = 0;
    int2 *dUnits = nullptr;      // cascade units (channel, unit index)
    int device = 0;
    // work buffer layout (float offsets)
@@ -71,68 +74,10 @@ namespace {
 constexpr int kRTile = 2048; // samples per item of the taps-gradient partials and the loss
 constexpr int kRaggedMaxStages = 64;
 
-// Taps gradient, partial over one (channel, tile) item:
-//     part[item][c] = sum_{j in tile} gu[j] x[j + c],  c < T.
-// Thread (cg, sl) accumulates 16 consecutive taps c0 = 16 cg .. c0 + 15 over
-// slice sl of the tile with a 24-sample register window: 128 multiply-adds per
-// 6 vector loads of x and 2 broadcast loads of gu.  x sits in shared memory
-// with 4 padding floats after every 32 (sxIdx), so the 16-byte loads of the
-// lanes of a warp, 16 floats apart, fall on distinct banks.  Slices are summed
-// in a fixed order.
+// Taps gradient: the per-run partial sums of fir_dh_bf16x3_kernel (fir_tc.cu), one
+// 512-float slot per run, slots of a channel consecutive and in time order, summed in
+// that order in FP64 (deterministic):  gtaps[T - 1 - c] = sum_slots part[slot][c].
 constexpr int kDhMaxT = 512;
-constexpr int kDhTaps = 16; // taps per thread
-constexpr int kDhX = kRTile + kDhMaxT + 32; // x samples staged per item
-__device__ __forceinline__ int sxIdx(int i) { return i + ((i >> 5) << 2); }
-
-__global__ void __launch_bounds__(256) fir_dh_partial_kernel(const RaggedChan *chans, const int2 *items,
-                                                              const float *x, const float *gu, float *part)
-{
-   __shared__ __align__(16) float sg[kRTile];
-   __shared__ __align__(16) float sx[kDhX + kDhX / 8];
-   __shared__ float red[256 * kDhTaps];
-   const int2 it = items[blockIdx.x];
-   const RaggedChan c = chans[it.x];
-   const int tid = threadIdx.x;
-   const int j0 = it.y * kRTile;
-   const int n = min(kRTile, c.Lu - j0);
-   for (int k = tid; k < kRTile; k += 256) sg[k] = k < n ? gu[c.xOff + j0 + k] : 0.0f;
-   for (int k = tid; k < kDhX; k += 256) {
-      const int idx = j0 + k;
-      sx[sxIdx(k)] = idx < c.L ? x[c.xOff + idx] : 0.0f;
-   }
-   __syncthreads();
-   const int ncg = (c.T + kDhTaps - 1) / kDhTaps; // <= 32 tap groups
-   const int slices = 256 / ncg;                    // threads beyond slices * ncg stay idle
-   const int slen = ((kRTile + slices - 1) / slices + 7) & ~7;
-   const int cg = tid % ncg, sl = tid / ncg;
-   float acc[kDhTaps];
-#pragma unroll
-   for (int r = 0; r < kDhTaps; r++) acc[r] = 0.0f;
-   if (sl < slices) {
-      const int c0 = cg * kDhTaps;
-      const int jb = sl * slen, je = min(jb + slen, (n + 7) & ~7);
-      for (int j = jb; j < je; j += 8) {
-         float w[kDhTaps + 8], gv[8];
-#pragma unroll
-         for (int v = 0; v < (kDhTaps + 8) / 4; v++) *(float4 *) &w[4 * v] = *(const float4 *) &sx[sxIdx(j + c0 + 4 * v)];
-         *(float4 *) &gv[0] = *(const float4 *) &sg[j];
-         *(float4 *) &gv[4] = *(const float4 *) &sg[j + 4];
-#pragma unroll
-         for (int i = 0; i < 8; i++)
-#pragma unroll
-            for (int r = 0; r < kDhTaps; r++) acc[r] = fmaf(gv[i], w[r + i], acc[r]);
-      }
-   }
-   if (sl < slices)
-#pragma unroll
-      for (int r = 0; r < kDhTaps; r++) red[(sl * ncg + cg) * kDhTaps + r] = acc[r];
-   __syncthreads();
-   for (int cc = tid; cc < c.T; cc += 256) {
-      float sum = 0.0f;
-      for (int q = 0; q < slices; q++) sum += red[q * ncg * kDhTaps + cc];
-      part[(long long) blockIdx.x * kDhMaxT + cc] = sum;
-   }
-}
 
 __global__ void __launch_bounds__(256) fir_dh_reduce_kernel(const RaggedChan *chans, const int *start,
                                                              const float *part, float *gtaps)
@@ -218,7 +163,8 @@ static void freePlan(RaggedPlan *p)
    cudaFree(p->dFwdItems);
    cudaFree(p->dFirFwdRuns);
    cudaFree(p->dFirDxRuns);
-   cudaFree(p->dFwdStart);
+   cudaFree(p->dDhStart);
+   cudaFree(p->dDhRuns);
    cudaFree(p->dUnits);
    delete p;
 }
@@ -269,7 +215,7 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    p->C = numChannels;
    std::vector<RaggedChan> ch(numChannels);
    std::vector<int2> fwd, units;
-   std::vector<int4> firFwd, firDx;
+   std::vector<int4> firFwd, firDx, dhRuns;
    std::vector<int> start(numChannels + 1);
    // runs of up to kFirBfRunTiles consecutive 8192-output tiles of one channel
    auto addRuns = [](std::vector<int4> &runs, int c, int outLen) {
@@ -296,18 +242,24 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
       p->Smax = std::max(p->Smax, S);
       p->Tmax = std::max(p->Tmax, T);
       if (S == 0) p->noStage++;
-      start[c] = (int) fwd.size();
+      start[c] = (int) dhRuns.size();
       for (int t = 0; t * kRTile < Lu; t++) fwd.push_back(make_int2(c, t));
+      {
+         const int tiles = (Lu + kFirBfTile - 1) / kFirBfTile;
+         for (int t = 0; t < tiles; t += kFirBfRunTiles)
+            dhRuns.push_back(make_int4(c, t, std::min(kFirBfRunTiles, tiles - t), (int) dhRuns.size()));
+      }
       if (S > 0)
          for (int j = 0; j < nu; j++) units.push_back(make_int2(c, j));
       addRuns(firFwd, c, Lu);
       addRuns(firDx, c, L);
    }
-   start[numChannels] = (int) fwd.size();
+   start[numChannels] = (int) dhRuns.size();
    // longest runs first, so the short ones fill in behind them
    auto longer = [](const int4 &a, const int4 &b) { return a.z > b.z; };
    std::stable_sort(firFwd.begin(), firFwd.end(), longer);
    std::stable_sort(firDx.begin(), firDx.end(), longer);
+   std::stable_sort(dhRuns.begin(), dhRuns.end(), longer);
    if (co / 5 > INT_MAX || units.size() > (size_t) INT_MAX) {
       delete p;
       return DSPLIB_ERR_INVALID_DIMENSION;
@@ -323,6 +275,7 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    p->nFirFwdRuns = (int) firFwd.size();
    p->nFirDxRuns = (int) firDx.size();
    p->nUnits = (int) units.size();
+   p->nDhRuns = (int) dhRuns.size();
    cudaGetDevice(&p->device);
    // work buffer: u | forward checkpoints | forward aggregates | stage tables | unit transitions
    p->wCk = align4(p->planeStride);
@@ -335,10 +288,11 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    p->sCk = p->sAgg + align4(2 * p->nCk);
    p->sPart = p->sCk + align4(2 * p->nCk);
    p->sDh = p->sPart + align4(5 * p->nCk);
-   p->sTotal = p->sDh + align4((long long) p->nFwdItems * kDhMaxT);
+   p->sTotal = p->sDh + align4(std::max((long long) p->nDhRuns * kDhMaxT, 2LL * p->nFwdItems));
    const bool ok = upload(&p->dChan, ch) == cudaSuccess && upload(&p->dFwdItems, fwd) == cudaSuccess &&
                    upload(&p->dFirFwdRuns, firFwd) == cudaSuccess && upload(&p->dFirDxRuns, firDx) == cudaSuccess &&
-                   upload(&p->dFwdStart, start) == cudaSuccess && upload(&p->dUnits, units) == cudaSuccess;
+                   upload(&p->dDhStart, start) == cudaSuccess && upload(&p->dDhRuns, dhRuns) == cudaSuccess &&
+                   upload(&p->dUnits, units) == cudaSuccess;
    if (!ok) {
       freePlan(p);
       return DSPLIB_ERR_FAILURE;
@@ -435,9 +389,10 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
    }
    if (launchFirBf16x3Ragged(p->dChan, p->dFirDxRuns, p->nFirDxRuns, g, taps, gx, true, p->Tmax, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
-   fir_dh_partial_kernel<<<p->nFwdItems, 256, 0, s>>>(p->dChan, p->dFwdItems, x, g, part);
-   fir_dh_reduce_kernel<<<p->C, 256, 0, s>>>(p->dChan, p->dFwdStart, part, gtaps);
-   countLaunch(2);
+   if (launchFirDhBf16x3Ragged(p->dChan, p->dDhRuns, p->nDhRuns, x, g, part, s) != cudaSuccess)
+      return DSPLIB_ERR_FAILURE;
+   fir_dh_reduce_kernel<<<p->C, 256, 0, s>>>(p->dChan, p->dDhStart, part, gtaps);
+   countLaunch(1);
    return cudaGetLastError() == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
 }
 
