@@ -49,6 +49,8 @@ constexpr int kWarps = 4;       // units per CTA
 constexpr int kThreads = 32 * kWarps;
 constexpr int kOutPad = kL + 1; // padded shared row per chunk (conflict-free staging)
 constexpr int kUnitLog2 = 9;    // Phi = A_c^(2^9)
+constexpr int kChainFastStages = 16; // cascades the FP32 register chain takes
+constexpr int kChainWin = 64;         // unit aggregates staged per window of that chain
 
 static_assert(kUnit == kBankSpan, "unit size");
 
@@ -183,14 +185,15 @@ __global__ void __launch_bounds__(128) bank_transition_kernel(const RaggedChan *
 }
 
 // Per channel (one warp): z_0 = 0, checkpoint z_j, z_{j+1} = Phi z_j + e_j over the
-// channel's units (adjoint: from the last unit back).  z in FP64.
+// channel's units (adjoint: from the last unit back).  z in FP64; cascades of more than
+// 16 stages (those of up to 16 take bank_chain_fast_kernel).
 __global__ void __launch_bounds__(32) bank_chain_kernel(const RaggedChan *chans, const double *phi,
                                                         const float2 *agg, float2 *ckpt, int adj)
 {
    extern __shared__ double dynC[];
    const RaggedChan c = chans[blockIdx.x];
    const int S = c.S, lane = threadIdx.x;
-   if (S == 0) return;
+   if (S <= kChainFastStages) return; // bank_chain_fast_kernel
    const int nb = S * (S + 1) / 2, n2 = 2 * S;
    double *P = dynC, *z = dynC + 4 * nb;
    const double *src = phi + c.phiOff + (adj ? 4LL * nb : 0);
@@ -223,6 +226,60 @@ __global__ void __launch_bounds__(32) bank_chain_kernel(const RaggedChan *chans,
          if (r < n2) z[r] = nz[i];
       }
       __syncwarp();
+   }
+}
+
+// The same chain for cascades of up to 16 stages (2S <= 32), in FP32 (Phi rounded once
+// from its FP64 product): lane r holds state component r and row r of Phi in registers;
+// each step broadcasts z by shuffles.  The unit aggregates are staged in shared memory
+// 64 units at a time (one coalesced read per window).
+
+__global__ void __launch_bounds__(32) bank_chain_fast_kernel(const RaggedChan *chans, const double *phi,
+                                                             const float2 *agg, float2 *ckpt, int adj)
+{
+   __shared__ float sE[kChainWin * 2 * kChainFastStages];
+   const RaggedChan c = chans[blockIdx.x];
+   const int S = c.S, lane = threadIdx.x;
+   if (S == 0 || S > kChainFastStages) return;
+   const int n2 = 2 * S, nb = S * (S + 1) / 2;
+   const double *P = phi + c.phiOff + (adj ? 4LL * nb : 0);
+   float row[2 * kChainFastStages];
+#pragma unroll
+   for (int k = 0; k < 2 * kChainFastStages; k++) row[k] = 0.0f;
+   if (lane < n2) {
+      const int p = lane >> 1, i = lane & 1;
+#pragma unroll
+      for (int k = 0; k < 2 * kChainFastStages; k++) {
+         const int q = k >> 1;
+         if (k < n2 && q <= p) row[k] = (float) P[4 * blk(p, q) + 2 * i + (k & 1)];
+      }
+   }
+   const float *ag = (const float *) (agg + c.ckOff);
+   float *ck = (float *) (ckpt + c.ckOff);
+   const int units = (c.Lu + kUnit - 1) / kUnit;
+   float z = 0.0f;
+   for (int w0 = 0; w0 < units; w0 += kChainWin) {
+      const int wn = min(kChainWin, units - w0);
+      // units [j0, j0 + wn) of this window in memory order
+      const int j0 = adj ? units - w0 - wn : w0;
+      __syncwarp();
+      for (int q = lane; q < wn * n2; q += 32) sE[q] = ag[(long long) j0 * n2 + q];
+      __syncwarp();
+      for (int k = 0; k < wn; k++) {
+         const int j = adj ? units - 1 - (w0 + k) : w0 + k;
+         if (lane < n2) ck[(long long) j * n2 + lane] = z;
+         if (w0 + k + 1 == units) break;
+         float a0 = lane < n2 ? sE[(j - j0) * n2 + lane] : 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+#pragma unroll
+         for (int q = 0; q < 2 * kChainFastStages; q += 4) {
+            if (q >= n2) break;
+            a0 = fmaf(row[q], __shfl_sync(0xffffffffu, z, q), a0);
+            a1 = fmaf(row[q + 1], __shfl_sync(0xffffffffu, z, q + 1), a1);
+            a2 = fmaf(row[q + 2], __shfl_sync(0xffffffffu, z, q + 2), a2);
+            a3 = fmaf(row[q + 3], __shfl_sync(0xffffffffu, z, q + 3), a3);
+         }
+         z = (a0 + a1) + (a2 + a3);
+      }
    }
 }
 
@@ -586,8 +643,12 @@ cudaError_t launchBankForward(const BankLaunch &b, cudaStream_t s)
    if ((e = cudaFuncSetAttribute(bank_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dynC)) !=
        cudaSuccess)
       return e;
-   bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.phi, b.aggF, b.ckptF, 0);
+   bank_chain_fast_kernel<<<b.C, 32, 0, s>>>(b.chans, b.phi, b.aggF, b.ckptF, 0);
    countLaunch();
+   if (b.Smax > kChainFastStages) {
+      bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.phi, b.aggF, b.ckptF, 0);
+      countLaunch();
+   }
    a.out = b.y;
    a.ckpt = b.ckptF;
    return launchUnits<UNIT_OUT>(a, s);
@@ -603,7 +664,12 @@ cudaError_t launchBankBackward(const BankLaunch &b, cudaStream_t s)
    if ((e = cudaFuncSetAttribute(bank_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dynC)) !=
        cudaSuccess)
       return e;
-   bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.phi, b.aggA, b.ckptA, 1);
+   bank_chain_fast_kernel<<<b.C, 32, 0, s>>>(b.chans, b.phi, b.aggA, b.ckptA, 1);
+   countLaunch();
+   if (b.Smax > kChainFastStages) {
+      bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.phi, b.aggA, b.ckptA, 1);
+      countLaunch();
+   }
    const size_t dyn = adjointShared(b.Smax);
    if ((e = cudaFuncSetAttribute(bank_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dyn)) !=
        cudaSuccess)
@@ -611,7 +677,7 @@ cudaError_t launchBankBackward(const BankLaunch &b, cudaStream_t s)
    AdjArgs d{b.chans, b.units, b.nUnits, b.Smax, b.tables, b.u, b.gy, b.ckptF, b.ckptA, b.g, b.part};
    bank_adjoint_kernel<<<b.nUnits, 32, dyn, s>>>(d);
    bank_coef_kernel<<<b.C, 32, 0, s>>>(b.chans, b.part, b.gcoefs);
-   countLaunch(3);
+   countLaunch(2);
    return cudaGetLastError();
 }
 
