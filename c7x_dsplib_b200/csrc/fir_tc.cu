@@ -729,13 +729,35 @@ __device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint3
    __syncthreads();
    // Taps band, K-major no swizzle: 16-byte chunk (q, n) at q*2048 + (n/8)*128 + (n%8)*16 holds
    // B[8q .. 8q+7][n]; rows n < 64: g_hi[m - n], rows n >= 64: g_lo[m - (n - 64)].
+   // Each chunk is 8 consecutive split taps from an arbitrary element offset o: the two
+   // aligned 16-byte vectors around it, shifted into place (funnel shifts by 16 bits for
+   // odd offsets), instead of 8 scalar reads.
    for (int cidx = tid; cidx < (Kt / 8) * 128; cidx += kBfThreads) {
       const int q = cidx >> 7, n = cidx & 127;
-      const uint16_t *src = (n < 64 ? L.gHi : L.gLo) + kBfPadLeft + 8 * q - (n & 63);
-      __align__(16) uint16_t v[8];
-#pragma unroll
-      for (int e = 0; e < 8; e++) v[e] = src[e];
-      *(uint4 *) (L.Bt + q * 2048 + (n >> 3) * 128 + (n & 7) * 16) = *(uint4 *) v;
+      const int o = kBfPadLeft + 8 * q - (n & 63);
+      const uint4 *base = (const uint4 *) (n < 64 ? L.gHi : L.gLo) + (o >> 3);
+      const uint4 lo4 = base[0], hi4 = base[1];
+      const int r = o & 7, h = r >> 1;
+      // words h .. h + 4 of the 8 (selects, not an indexed array: it stays in registers)
+      const uint32_t w0 = h == 0 ? lo4.x : h == 1 ? lo4.y : h == 2 ? lo4.z : lo4.w;
+      const uint32_t w1 = h == 0 ? lo4.y : h == 1 ? lo4.z : h == 2 ? lo4.w : hi4.x;
+      const uint32_t w2 = h == 0 ? lo4.z : h == 1 ? lo4.w : h == 2 ? hi4.x : hi4.y;
+      const uint32_t w3 = h == 0 ? lo4.w : h == 1 ? hi4.x : h == 2 ? hi4.y : hi4.z;
+      const uint32_t w4 = h == 0 ? hi4.x : h == 1 ? hi4.y : h == 2 ? hi4.z : hi4.w;
+      uint4 v;
+      if (r & 1) {
+         v.x = __funnelshift_r(w0, w1, 16);
+         v.y = __funnelshift_r(w1, w2, 16);
+         v.z = __funnelshift_r(w2, w3, 16);
+         v.w = __funnelshift_r(w3, w4, 16);
+      }
+      else {
+         v.x = w0;
+         v.y = w1;
+         v.z = w2;
+         v.w = w3;
+      }
+      *(uint4 *) (L.Bt + q * 2048 + (n >> 3) * 128 + (n & 7) * 16) = v;
    }
    for (int t = r.t0; t < r.t1; t++) {
       const int k = (t - r.t0) % S;
@@ -936,7 +958,7 @@ __global__ void __launch_bounds__(kBfThreads, 1)
    tc::fenceAfterSync();
    const uint32_t tmem = *tslot;
    const uint32_t id = tc::idesc(1, 1, 1, kRows, 64) | (1u << 15) | (1u << 16); // both operands MN-major
-   uint32_t par[2] = {0, 0};
+   uint32_t par = 0; // MMA barrier phase, one bit per buffer
    bool ok = true;
    for (int k = 0; k < run.z && ok; k++) {
       const int b = k & 1;
@@ -963,8 +985,8 @@ __global__ void __launch_bounds__(kBfThreads, 1)
       if (k + 1 < run.z) {
          // the other buffer is free once the MMAs of the tile before this one completed
          if (k >= 1) {
-            const bool done = tid == 0 ? tc::mbarWait(mbar + (1 - b), par[1 - b]) : true;
-            par[1 - b] ^= 1;
+            const bool done = tid == 0 ? tc::mbarWait(mbar + (1 - b), (par >> (1 - b)) & 1) : true;
+            par ^= 1u << (1 - b);
             if (!done && tid == 0) atomicExch(&g_firTcError, 1);
             ok = !__syncthreads_or(!done);
             if (!ok) break;
@@ -980,8 +1002,8 @@ __global__ void __launch_bounds__(kBfThreads, 1)
    bool fail = !ok;
    for (int k = run.z >= 2 ? run.z - 2 : 0; k < run.z; k++) {
       const int b = k & 1;
-      const bool done = tid == 0 ? tc::mbarWait(mbar + b, par[b]) : true;
-      par[b] ^= 1;
+      const bool done = tid == 0 ? tc::mbarWait(mbar + b, (par >> b) & 1) : true;
+      par ^= 1u << b;
       if (!done && tid == 0) {
          atomicExch(&g_firTcError, 1);
          fail = true;
