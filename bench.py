@@ -387,7 +387,7 @@ class FilterBankWorkload(Workload):
         return {"workload": self.name, "channels": self.C, "total_samples": self.samples,
                 "lengths": "log-uniform [256, 262144]", "taps": "uniform {32..512}", "stages": "uniform {2..8}",
                 "pole_radius": "U[0.5, 0.98]", "loss": "MSE vs fixed target bank output",
-                "graph": "forward + loss + adjoint in one CUDA graph"}
+                "graph": "one fused training-step call (forward + loss + adjoint) in one CUDA graph"}
 
     def bind_stream(self, stream):
         pass
@@ -412,7 +412,8 @@ class FilterBankWorkload(Workload):
         self.replay()
 
     def phase_times(self, torch, reps=3):
-        """Event-timed C-ABI calls of one step, run eagerly (forward, loss, adjoint): median ms each."""
+        """Event-timed C-ABI calls, run eagerly: forward, loss and adjoint as separate calls, and the
+        fused step the timed graph replays; median ms each."""
         b, dev = self.bank, "cuda"
         y = torch.empty(b.sizes[0], device=dev)
         work = torch.empty(b.sizes[3], device=dev)
@@ -422,7 +423,9 @@ class FilterBankWorkload(Workload):
         loss = torch.empty(1, device=dev)
         calls = {"forward": lambda: b.forward_raw(self.xd, self.hd, self.cd, y, work),
                  "loss": lambda: b.mse_grad_raw(y, self.target, gy, loss, scratch),
-                 "adjoint": lambda: b.backward_raw(self.xd, self.hd, self.cd, work, gy, gx, gh, gc, scratch)}
+                 "adjoint": lambda: b.backward_raw(self.xd, self.hd, self.cd, work, gy, gx, gh, gc, scratch),
+                 "fused_step": lambda: b.step_mse_raw(self.xd, self.hd, self.cd, self.target, y, gy, loss, gx, gh,
+                                                      gc, work, scratch)}
         times = {k: [] for k in calls}
         s = torch.cuda.current_stream()
         for _ in range(reps):

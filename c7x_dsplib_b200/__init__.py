@@ -153,6 +153,7 @@ SIGNATURES = {
     "DSPLIB_gpu_firBiquadBatched_fwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_gpu_firBiquadBatched_bwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_gpu_raggedMseGrad": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "DSPLIB_gpu_firBiquadBatched_stepMse": (ctypes.c_int, [_VP] * 14),
     "DSPLIB_gpu_firBiquadBatched_bwdStaticScratch": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                                                                     _VP]),
 }

@@ -423,6 +423,23 @@ __device__ __forceinline__ void correctAndOutputRev(float (&v)[kL], float (&lam)
    }
 }
 
+// A unit's per-stage states, read once: lane l holds stage l in lo and stage l + 32 in hi
+// (up to 64 stages); entryAt broadcasts stage p.
+struct UnitStates {
+   float2 lo, hi;
+};
+__device__ __forceinline__ UnitStates loadStates(const float2 *src, int S, int lane)
+{
+   UnitStates u;
+   u.lo = lane < S ? src[lane] : make_float2(0.0f, 0.0f);
+   u.hi = lane + 32 < S ? src[lane + 32] : make_float2(0.0f, 0.0f);
+   return u;
+}
+__device__ __forceinline__ float2 entryAt(const UnitStates &u, int p)
+{
+   return scan::shflIdx(p < 32 ? u.lo : u.hi, p & 31);
+}
+
 struct UnitArgs {
    const RaggedChan *chans;
    const int2 *units; // (channel, unit index within the channel)
@@ -433,6 +450,13 @@ struct UnitArgs {
    float *out;        // OUT: y (packed, tail zeros)
    float2 *agg;       // AGG: unit aggregates, 2 floats per stage (processing order)
    const float2 *ckpt;
+   // OUT_MSE: loss gradient gy = scale (y - target) on the valid samples, the unit's
+   // sum of (y - target)^2 in lossPart[unit], and the adjoint's unit aggregates in aggA
+   const float *target;
+   float *gy;
+   double *lossPart;
+   float2 *aggA;
+   float scale;
 };
 
 // Copy the channel's stage tables into the warp's slice of shared memory.
@@ -446,7 +470,22 @@ __device__ __forceinline__ void loadTables(float *dst, const float *tables, cons
 // Forward passes: AGG = from a zero state, write the unit aggregate of every stage;
 // OUT = from the checkpoints, write y.  ADJ_AGG: adjoint aggregates over the output
 // gradient (reverse time, stages in reverse order).
-enum UnitMode { UNIT_AGG = 0, UNIT_OUT = 1, UNIT_ADJ_AGG = 2 };
+enum UnitMode { UNIT_AGG = 0, UNIT_OUT = 1, UNIT_ADJ_AGG = 2, UNIT_OUT_MSE = 3 };
+
+// The adjoint's zero-entry pass over a unit (reverse time, stages in reverse order):
+// g holds the output gradient on entry, the unit aggregate of every stage goes to agg.
+__device__ __forceinline__ void adjointAggregates(float (&g)[kL], const float *sTab, int S, float2 *agg, int lane)
+{
+   for (int p = 0; p < S; p++) {
+      const float *tb = sTab + (S - 1 - p) * kBankTabFloats;
+      float w[kL];
+      float2 incl;
+      const float2 st =
+          chunkStateDown(zeroStatePassRev(g, w, tb[3], tb[4]), make_float2(0.0f, 0.0f), tb, lane, &incl);
+      correctAndOutputRev(w, g, tb, st.x, st.y);
+      if (lane == 0) agg[p] = incl;
+   }
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads) bank_unit_kernel(UnitArgs a)
@@ -462,30 +501,46 @@ __global__ void __launch_bounds__(kThreads) bank_unit_kernel(UnitArgs a)
    const int S = c.S, Lu = c.Lu, t0 = U.y * kUnit;
    const long long base = c.ckOff + (long long) U.y * S;
    loadTables(sTab, a.tables, c, lane);
+   constexpr bool OUT = MODE == UNIT_OUT || MODE == UNIT_OUT_MSE;
+   UnitStates ent = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+   if (OUT) ent = loadStates(a.ckpt + base, S, lane);
    float v[kL];
-   if (MODE == UNIT_ADJ_AGG) loadPacked(v, a.in + c.xOff, t0, Lu, sStage[warp], lane);
-   else loadChunk(v, a.in + c.pOff, t0 + lane * kL, Lu);
-   for (int p = 0; p < S; p++) {
-      const int s = MODE == UNIT_ADJ_AGG ? S - 1 - p : p;
-      const float *tb = sTab + s * kBankTabFloats;
-      float w[kL];
-      const float2 entry = MODE == UNIT_OUT ? a.ckpt[base + p] : make_float2(0.0f, 0.0f);
-      float2 incl;
-      if (MODE == UNIT_ADJ_AGG) {
-         const float2 st = chunkStateDown(zeroStatePassRev(v, w, tb[3], tb[4]), entry, tb, lane, &incl);
-         correctAndOutputRev(w, v, tb, st.x, st.y);
-         if (lane == 0) a.agg[base + p] = incl;
-      }
-      else {
-         const float2 st = chunkStateUp(zeroStatePass(v, w, tb[3], tb[4]), entry, tb, lane, &incl);
-         correctAndOutput(w, v, tb, st.x, st.y);
-         if (MODE == UNIT_AGG && lane == 31) a.agg[base + p] = incl;
-      }
+   if (MODE == UNIT_ADJ_AGG) {
+      loadPacked(v, a.in + c.xOff, t0, Lu, sStage[warp], lane);
+      adjointAggregates(v, sTab, S, a.agg + base, lane);
+      return;
    }
-   if (MODE == UNIT_OUT) {
+   loadChunk(v, a.in + c.pOff, t0 + lane * kL, Lu);
+   for (int p = 0; p < S; p++) {
+      const float *tb = sTab + p * kBankTabFloats;
+      float w[kL];
+      const float2 entry = OUT ? entryAt(ent, p) : make_float2(0.0f, 0.0f);
+      float2 incl;
+      const float2 st = chunkStateUp(zeroStatePass(v, w, tb[3], tb[4]), entry, tb, lane, &incl);
+      correctAndOutput(w, v, tb, st.x, st.y);
+      if (MODE == UNIT_AGG && lane == 31) a.agg[base + p] = incl;
+   }
+   if (OUT) {
       storePacked(v, a.out + c.xOff, t0, Lu, sStage[warp], lane);
       if (t0 + kUnit >= Lu)
          for (int t = Lu + lane; t < c.L; t += 32) a.out[c.xOff + t] = 0.0f;
+   }
+   if (MODE == UNIT_OUT_MSE) {
+      float tg[kL];
+      loadPacked(tg, a.target + c.xOff, t0, Lu, sStage[warp], lane);
+      double sq = 0.0;
+#pragma unroll
+      for (int i = 0; i < kL; i++) {
+         const bool valid = t0 + lane * kL + i < Lu;
+         const float d = v[i] - tg[i];
+         v[i] = valid ? a.scale * d : 0.0f;
+         if (valid) sq += (double) d * d;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+      if (lane == 0) a.lossPart[ui] = sq;
+      storePacked(v, a.gy + c.xOff, t0, Lu, sStage[warp], lane);
+      adjointAggregates(v, sTab, S, a.aggA + base, lane);
    }
 }
 
@@ -518,6 +573,7 @@ __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
    const RaggedChan c = a.chans[U.x];
    const int S = c.S, Lu = c.Lu, t0 = U.y * kUnit;
    const long long base = c.ckOff + (long long) U.y * S;
+   const UnitStates entF = loadStates(a.ckptF + base, S, lane), entA = loadStates(a.ckptA + base, S, lane);
    loadTables(sTab, a.tables, c, lane);
    float v[kL], w[kL];
    loadChunk(v, a.u + c.pOff, t0 + lane * kL, Lu);
@@ -525,7 +581,7 @@ __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
    for (int s = 0; s < S; s++) {
       const float *tb = sTab + s * kBankTabFloats;
       float2 incl;
-      const float2 st = chunkStateUp(zeroStatePass(v, w, tb[3], tb[4]), a.ckptF[base + s], tb, lane, &incl);
+      const float2 st = chunkStateUp(zeroStatePass(v, w, tb[3], tb[4]), entryAt(entF, s), tb, lane, &incl);
       correctAndOutput(w, v, tb, st.x, st.y);
       if (s + 1 < S) {
          float *Ws = W + s * kL * 32 + lane;
@@ -541,7 +597,7 @@ __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
       const float *tb = sTab + s * kBankTabFloats;
       float vz[kL], lam[kL];
       float2 incl;
-      const float2 st = chunkStateDown(zeroStatePassRev(g, vz, tb[3], tb[4]), a.ckptA[base + p], tb, lane, &incl);
+      const float2 st = chunkStateDown(zeroStatePassRev(g, vz, tb[3], tb[4]), entryAt(entA, p), tb, lane, &incl);
       correctAndOutputRev(vz, lam, tb, st.x, st.y);
       // forward sequence of this stage: wr[i + 2] = w[i]; w[-1], w[-2] are the previous
       // lane's last two samples (lane 0: the unit's checkpoint state)
@@ -557,10 +613,12 @@ __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
       }
       wr[1] = __shfl_up_sync(0xffffffffu, wr[kL + 1], 1);
       wr[0] = __shfl_up_sync(0xffffffffu, wr[kL], 1);
-      if (lane == 0) {
-         const float2 e = a.ckptF[base + s];
-         wr[1] = e.x;
-         wr[0] = e.y;
+      {
+         const float2 e = entryAt(entF, s);
+         if (lane == 0) {
+            wr[1] = e.x;
+            wr[0] = e.y;
+         }
       }
       float pr[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
@@ -651,15 +709,25 @@ cudaError_t launchBankForward(const BankLaunch &b, cudaStream_t s)
    }
    a.out = b.y;
    a.ckpt = b.ckptF;
+   if (b.target) {
+      a.target = b.target;
+      a.gy = b.gyOut;
+      a.lossPart = b.lossPart;
+      a.aggA = b.aggA;
+      a.scale = b.scale;
+      return launchUnits<UNIT_OUT_MSE>(a, s);
+   }
    return launchUnits<UNIT_OUT>(a, s);
 }
 
 cudaError_t launchBankBackward(const BankLaunch &b, cudaStream_t s)
 {
    if (b.nUnits <= 0) return cudaSuccess;
-   UnitArgs a{b.chans, b.units, b.nUnits, b.Smax, b.tables, b.gy, nullptr, b.aggA, nullptr};
-   cudaError_t e = launchUnits<UNIT_ADJ_AGG>(a, s);
-   if (e != cudaSuccess) return e;
+   cudaError_t e = cudaSuccess;
+   if (!b.aggReady) {
+      UnitArgs a{b.chans, b.units, b.nUnits, b.Smax, b.tables, b.gy, nullptr, b.aggA, nullptr};
+      if ((e = launchUnits<UNIT_ADJ_AGG>(a, s)) != cudaSuccess) return e;
+   }
    const size_t dynC = (size_t) (4 * b.Smax * (b.Smax + 1) / 2 + 2 * b.Smax) * sizeof(double);
    if ((e = cudaFuncSetAttribute(bank_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dynC)) !=
        cudaSuccess)

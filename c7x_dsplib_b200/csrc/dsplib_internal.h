@@ -272,6 +272,13 @@ struct BankLaunch {
    float2 *aggF, *ckptF, *aggA, *ckptA;
    float *part;       // adjoint: 5 coefficient-gradient sums per unit and stage
    float *gcoefs;
+   // forward with the loss fused (target != nullptr): gyOut = scale (y - target), unit
+   // sums of squares in lossPart, the adjoint's unit aggregates in aggA
+   const float *target;
+   float *gyOut;
+   double *lossPart;
+   float scale;
+   bool aggReady; // adjoint: aggA already computed by the fused forward
 };
 // Doubles of both unit transitions of a channel of S stages.
 long long bankTransitionDoubles(int S);

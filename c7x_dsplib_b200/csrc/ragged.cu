@@ -20,7 +20,6 @@
 //                          outputs; the adjoint the same in reverse time, with
 //                          each unit's forward recomputed from the checkpoints
 //                          (no stage output is stored).
-//   ragged_passthrough_kernel  channels without biquad stages: y = u, g = gy.
 //   fir_dh_bf16x3_kernel (fir_tc.cu) / fir_dh_reduce_kernel  taps gradient
 //                          dh[T-1-c] = sum_j gu[j] x[j+c] as split-BF16x3
 //                          tcgen05 contractions over runs of 8192-sample tiles,
@@ -49,7 +48,7 @@ struct RaggedPlan {
    int C = 0;
    long long totalLen = 0, totalTaps = 0, totalCoefs = 0, totalOut = 0;
    long long planeStride = 0; // floats of the FIR output plane: sum of round16(Lu)
-   int Smax = 0, Tmax = 0, totalStages = 0, noStage = 0;
+   int Smax = 0, Tmax = 0, totalStages = 0;
    int nFwdItems = 0, nFirFwdRuns = 0, nFirDxRuns = 0, nUnits = 0;
    long long nCk = 0;  // unit states (float2): sum over channels of units x stages
    long long nPhi = 0; // doubles of the unit transitions
@@ -65,7 +64,7 @@ struct RaggedPlan {
    // work buffer layout (float offsets)
    long long wCk = 0, wAgg = 0, wTab = 0, wPhi = 0, wTotal = 0;
    // scratch layout (float offsets)
-   long long sAgg = 0, sCk = 0, sPart = 0, sDh = 0, sTotal = 0;
+   long long sAgg = 0, sCk = 0, sPart = 0, sLoss = 0, sDh = 0, sTotal = 0;
 };
 
 namespace {
@@ -131,19 +130,6 @@ __global__ void __launch_bounds__(1024) mse_reduce_kernel(const double *part, in
       __syncthreads();
    }
    if (threadIdx.x == 0) loss[0] = (float) (red[0] * invCount);
-}
-
-// Channels without biquad stages: the cascade is the identity (forward y = u with the
-// T - 1 tail samples zero; adjoint g = gy).  One CTA per channel; others return.
-__global__ void __launch_bounds__(256) ragged_passthrough_kernel(const RaggedChan *chans, const float *in, float *out,
-                                                                 int fromPlane)
-{
-   const RaggedChan c = chans[blockIdx.x];
-   if (c.S != 0) return;
-   const float *src = in + (fromPlane ? c.pOff : c.xOff);
-   for (int t = threadIdx.x; t < c.Lu; t += 256) out[c.xOff + t] = src[t];
-   if (fromPlane)
-      for (int t = c.Lu + threadIdx.x; t < c.L; t += 256) out[c.xOff + t] = 0.0f;
 }
 
 template <typename T> cudaError_t upload(T **dst, const std::vector<T> &v)
@@ -241,7 +227,6 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
       co += 5LL * S;
       p->Smax = std::max(p->Smax, S);
       p->Tmax = std::max(p->Tmax, T);
-      if (S == 0) p->noStage++;
       start[c] = (int) dhRuns.size();
       for (int t = 0; t * kRTile < Lu; t++) fwd.push_back(make_int2(c, t));
       {
@@ -249,8 +234,7 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
          for (int t = 0; t < tiles; t += kFirBfRunTiles)
             dhRuns.push_back(make_int4(c, t, std::min(kFirBfRunTiles, tiles - t), (int) dhRuns.size()));
       }
-      if (S > 0)
-         for (int j = 0; j < nu; j++) units.push_back(make_int2(c, j));
+      for (int j = 0; j < nu; j++) units.push_back(make_int2(c, j));
       addRuns(firFwd, c, Lu);
       addRuns(firDx, c, L);
    }
@@ -287,7 +271,8 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    p->sAgg = align4(p->totalLen);
    p->sCk = p->sAgg + align4(2 * p->nCk);
    p->sPart = p->sCk + align4(2 * p->nCk);
-   p->sDh = p->sPart + align4(5 * p->nCk);
+   p->sLoss = p->sPart + align4(5 * p->nCk);
+   p->sDh = p->sLoss + align4(2LL * p->nUnits); // unit sums of squares (doubles) of the fused loss
    p->sTotal = p->sDh + align4(std::max((long long) p->nDhRuns * kDhMaxT, 2LL * p->nFwdItems));
    const bool ok = upload(&p->dChan, ch) == cudaSuccess && upload(&p->dFwdItems, fwd) == cudaSuccess &&
                    upload(&p->dFirFwdRuns, firFwd) == cudaSuccess && upload(&p->dFirDxRuns, firDx) == cudaSuccess &&
@@ -351,16 +336,11 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_fwd(DSPLIB_gpu_raggedPlan plan, const 
    b.y = y;
    if (launchFirBf16x3Ragged(p->dChan, p->dFirFwdRuns, p->nFirFwdRuns, x, taps, u, false, p->Tmax, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
-   if (p->nUnits > 0 &&
-       (launchBankTables(p->dChan, p->C, coefs, p->totalStages, p->Smax, work + p->wTab, (double *) (work + p->wPhi),
-                         s) != cudaSuccess ||
-        launchBankForward(b, s) != cudaSuccess))
+   if (launchBankTables(p->dChan, p->C, coefs, p->totalStages, p->Smax, work + p->wTab, (double *) (work + p->wPhi),
+                        s) != cudaSuccess ||
+       launchBankForward(b, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
-   if (p->noStage > 0) {
-      ragged_passthrough_kernel<<<p->C, 256, 0, s>>>(p->dChan, u, y, 1);
-      countLaunch();
-   }
-   return cudaGetLastError() == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
+   return DSPLIB_SUCCESS;
 }
 
 DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
@@ -382,17 +362,60 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
    b.ckptA = (float2 *) (scratch + p->sCk);
    b.part = scratch + p->sPart;
    b.gcoefs = gcoefs;
-   if (p->nUnits > 0 && launchBankBackward(b, s) != cudaSuccess) return DSPLIB_ERR_FAILURE;
-   if (p->noStage > 0) {
-      ragged_passthrough_kernel<<<p->C, 256, 0, s>>>(p->dChan, gy, g, 0);
-      countLaunch();
-   }
+   if (launchBankBackward(b, s) != cudaSuccess) return DSPLIB_ERR_FAILURE;
    if (launchFirBf16x3Ragged(p->dChan, p->dFirDxRuns, p->nFirDxRuns, g, taps, gx, true, p->Tmax, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
    if (launchFirDhBf16x3Ragged(p->dChan, p->dDhRuns, p->nDhRuns, x, g, part, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
    fir_dh_reduce_kernel<<<p->C, 256, 0, s>>>(p->dChan, p->dDhStart, part, gtaps);
    countLaunch(1);
+   return cudaGetLastError() == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
+}
+
+DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMse(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
+                                                  const float *coefs, const float *target, float *y, float *gy,
+                                                  float *loss, float *gx, float *gtaps, float *gcoefs, float *work,
+                                                  float *scratch, void *stream)
+{
+   RaggedPlan *p = (RaggedPlan *) plan;
+   if (!p || !x || !taps || ((!coefs || !gcoefs) && p->totalCoefs) || !target || !y || !gy || !loss || !gx ||
+       !gtaps || !work || !scratch)
+      return DSPLIB_ERR_NULL_POINTER;
+   if (p->totalOut <= 0) return DSPLIB_ERR_INVALID_DIMENSION;
+   PlanDevice dev(p);
+   if (!dev.ok()) return DSPLIB_ERR_FAILURE;
+   cudaStream_t s = (cudaStream_t) stream;
+   float *g = scratch;
+   BankLaunch b = bankLaunch(p, work);
+   b.y = y;
+   b.target = target;
+   b.gyOut = gy;
+   b.lossPart = (double *) (scratch + p->sLoss);
+   b.scale = (float) (2.0 / (double) p->totalOut);
+   b.aggA = (float2 *) (scratch + p->sAgg);
+   // forward, loss gradient and the adjoint's first pass in one sweep over the units
+   if (launchFirBf16x3Ragged(p->dChan, p->dFirFwdRuns, p->nFirFwdRuns, x, taps, work, false, p->Tmax, s) !=
+           cudaSuccess ||
+       launchBankTables(p->dChan, p->C, coefs, p->totalStages, p->Smax, work + p->wTab, (double *) (work + p->wPhi),
+                        s) != cudaSuccess ||
+       launchBankForward(b, s) != cudaSuccess)
+      return DSPLIB_ERR_FAILURE;
+   mse_reduce_kernel<<<1, 1024, 0, s>>>(b.lossPart, p->nUnits, 1.0 / (double) p->totalOut, loss);
+   countLaunch();
+   // adjoint
+   b.target = nullptr;
+   b.gy = gy;
+   b.g = g;
+   b.ckptA = (float2 *) (scratch + p->sCk);
+   b.part = scratch + p->sPart;
+   b.gcoefs = gcoefs;
+   b.aggReady = true;
+   if (launchBankBackward(b, s) != cudaSuccess ||
+       launchFirBf16x3Ragged(p->dChan, p->dFirDxRuns, p->nFirDxRuns, g, taps, gx, true, p->Tmax, s) != cudaSuccess ||
+       launchFirDhBf16x3Ragged(p->dChan, p->dDhRuns, p->nDhRuns, x, g, scratch + p->sDh, s) != cudaSuccess)
+      return DSPLIB_ERR_FAILURE;
+   fir_dh_reduce_kernel<<<p->C, 256, 0, s>>>(p->dChan, p->dDhStart, scratch + p->sDh, gtaps);
+   countLaunch();
    return cudaGetLastError() == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
 }
 

@@ -133,13 +133,32 @@ class RaggedFilterBank:
         if st != SUCCESS:
             raise DsplibError("DSPLIB_gpu_raggedMseGrad", st)
 
+    def step_mse_raw(self, x, taps, coefs, target, y, gy, loss, gx, gtaps, gcoefs, work, scratch):
+        """Forward + MSE loss + adjoint in one call (DSPLIB_gpu_firBiquadBatched_stepMse)."""
+        self._check(target, self.sizes[SAMPLES], "target")
+        self._check(y, self.sizes[SAMPLES], "y")
+        self._check(gy, self.sizes[SAMPLES], "gy")
+        self._check(loss, 1, "loss")
+        self._check(gx, self.sizes[SAMPLES], "gx")
+        self._check(gtaps, self.sizes[TAPS], "gtaps")
+        self._check(gcoefs, self.sizes[COEFS], "gcoefs")
+        self._check(work, self.sizes[WORK], "work")
+        self._check(scratch, self.sizes[SCRATCH], "scratch")
+        st = lib().DSPLIB_gpu_firBiquadBatched_stepMse(
+            self._plan, x.data_ptr(), taps.data_ptr(), coefs.data_ptr(), target.data_ptr(), y.data_ptr(),
+            gy.data_ptr(), loss.data_ptr(), gx.data_ptr(), gtaps.data_ptr(), gcoefs.data_ptr(), work.data_ptr(),
+            scratch.data_ptr(), _stream_ptr())
+        if st != SUCCESS:
+            raise DsplibError("DSPLIB_gpu_firBiquadBatched_stepMse", st)
+
     # ---------------------------------------------------------------- autograd
     def apply(self, x, taps, coefs):
         """Differentiable y = filterbank(x; taps, coefs) on packed tensors."""
         return _FirBiquadFn.apply(x, taps, coefs, self)
 
     def graph_step(self, x, taps, coefs, target):
-        """Capture forward + MSE loss (DSPLIB_gpu_raggedMseGrad) + backward for this plan in a CUDA graph.
+        """Capture one training step (forward, MSE loss, adjoint: DSPLIB_gpu_firBiquadBatched_stepMse)
+        for this plan in a CUDA graph.
 
         Returns ``(replay, outputs)``: ``replay()`` reruns the captured work on
         the same input tensors (refill them in place between replays);
@@ -157,9 +176,7 @@ class RaggedFilterBank:
         loss = torch.empty(1, device=dev)
 
         def body():
-            self.forward_raw(x, taps, coefs, y, work)
-            self.mse_grad_raw(y, target, gy, loss, scratch)
-            self.backward_raw(x, taps, coefs, work, gy, gx, gtaps, gcoefs, scratch)
+            self.step_mse_raw(x, taps, coefs, target, y, gy, loss, gx, gtaps, gcoefs, work, scratch)
 
         s = torch.cuda.Stream(device=dev)
         s.wait_stream(torch.cuda.current_stream(dev))

@@ -156,6 +156,17 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
 DSPLIB_STATUS DSPLIB_gpu_raggedMseGrad(DSPLIB_gpu_raggedPlan plan, const float *y, const float *target, float *gy,
                                        float *loss, float *scratch, void *stream);
 
+/** One training step: the forward, the mean squared error against target (as
+ *  DSPLIB_gpu_raggedMseGrad: loss[0], gy) and the adjoint (as
+ *  DSPLIB_gpu_firBiquadBatched_bwd with that gy) in one call, sharing passes: the
+ *  cascade's output pass also forms gy and runs the adjoint's first pass over it.
+ *  Results equal those of the three separate calls; y and gy are outputs too.
+ *  work and scratch as for the separate calls.  No counterpart in the reference. */
+DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMse(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
+                                                  const float *coefs, const float *target, float *y, float *gy,
+                                                  float *loss, float *gx, float *gtaps, float *gcoefs, float *work,
+                                                  float *scratch, void *stream);
+
 /** Size, in floats, of the scratch array built into the library for
  *  DSPLIB_gpu_firBiquadBatched_bwdStaticScratch (16 MiB per device). */
 #define DSPLIB_GPU_STATIC_SCRATCH_FLOATS (4u << 20)

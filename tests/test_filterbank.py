@@ -334,3 +334,37 @@ def test_bank_deep_cascades_beyond_shared_memory():
     lengths, taps, stages, x, h, c = _bank_case(8, 5, Lrange=(2000, 12000), Tmax=32, Smax=4,
                                                 force=[(9000, 16, 24), (3000, 3, 22)])
     _check_bank(lengths, taps, stages, x, h, c)
+
+
+@pytest.mark.gpu
+def test_fused_step_equals_separate_calls():
+    """DSPLIB_gpu_firBiquadBatched_stepMse against forward + MSE + adjoint as three calls:
+    y, gy and every gradient bitwise equal, the loss to FP64 summation order."""
+    import torch
+
+    from c7x_dsplib_b200.filterbank import RaggedFilterBank
+
+    lengths, taps, stages, x, h, c = _bank_case(13, 20, Lrange=(100, 30000), Tmax=96, Smax=6,
+                                                force=[(70000, 33, 4), (600, 1, 0)])
+    bank = RaggedFilterBank(lengths, taps, stages)
+    dev = "cuda"
+    xt, ht, ct = (torch.tensor(a, dtype=torch.float32, device=dev) for a in (x, h, c))
+    target = torch.randn(bank.sizes[0], device=dev, generator=torch.Generator(dev).manual_seed(3))
+    n = bank.sizes[0]
+    sep = {k: torch.empty(n, device=dev) for k in ("y", "gy", "gx")}
+    sep["gtaps"], sep["gcoefs"] = torch.empty_like(ht), torch.empty_like(ct)
+    sep["loss"] = torch.empty(1, device=dev)
+    work = torch.empty(bank.sizes[3], device=dev)
+    scratch = torch.empty(bank.sizes[4], device=dev)
+    bank.forward_raw(xt, ht, ct, sep["y"], work)
+    bank.mse_grad_raw(sep["y"], target, sep["gy"], sep["loss"], scratch)
+    bank.backward_raw(xt, ht, ct, work, sep["gy"], sep["gx"], sep["gtaps"], sep["gcoefs"], scratch)
+    fus = {k: torch.full_like(v, 7.0) for k, v in sep.items()}
+    work2 = torch.empty_like(work)
+    scratch2 = torch.empty_like(scratch)
+    bank.step_mse_raw(xt, ht, ct, target, fus["y"], fus["gy"], fus["loss"], fus["gx"], fus["gtaps"],
+                      fus["gcoefs"], work2, scratch2)
+    torch.cuda.synchronize()
+    for k in ("y", "gy", "gx", "gtaps", "gcoefs"):
+        assert torch.equal(fus[k], sep[k]), k
+    assert float(fus["loss"]) == pytest.approx(float(sep["loss"]), rel=1e-6)
