@@ -540,6 +540,8 @@ __global__ void __launch_bounds__(kThreads) bank_unit_kernel(UnitArgs a)
       for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
       if (lane == 0) a.lossPart[ui] = sq;
       storePacked(v, a.gy + c.xOff, t0, Lu, sStage[warp], lane);
+      if (t0 + kUnit >= Lu)
+         for (int t = Lu + lane; t < c.L; t += 32) a.gy[c.xOff + t] = 0.0f;
       adjointAggregates(v, sTab, S, a.aggA + base, lane);
    }
 }
