@@ -50,7 +50,6 @@ constexpr int kThreads = 32 * kWarps;
 constexpr int kOutPad = kL + 1; // padded shared row per chunk (conflict-free staging)
 constexpr int kUnitLog2 = 9;    // Phi = A_c^(2^9)
 constexpr int kChainFastStages = 16; // cascades the FP32 register chain takes
-constexpr int kChainWin = 64;         // unit aggregates staged per window of that chain
 
 static_assert(kUnit == kBankSpan, "unit size");
 
@@ -115,7 +114,8 @@ __host__ __device__ inline int blk(int p, int q) { return p * (p + 1) / 2 + q; }
 __device__ __forceinline__ int stageAt(int p, int S, bool adj) { return adj ? S - 1 - p : p; }
 
 // Phi = A_c^512 for one channel and direction, one CTA: A_c in shared memory, nine
-// squarings C(p,q) = sum_{m=q..p} B(p,m) B(m,q) between two shared buffers.
+// squarings C(p,q) = sum_{m=q..p} B(p,m) B(m,q) between two shared buffers; then
+// Phi^32.  Per channel: Phi forward, Phi adjoint, Phi^32 forward, Phi^32 adjoint.
 __global__ void __launch_bounds__(128) bank_transition_kernel(const RaggedChan *chans, const float *coefs,
                                                               double *phi)
 {
@@ -182,6 +182,33 @@ __global__ void __launch_bounds__(128) bank_transition_kernel(const RaggedChan *
    }
    double *dst = phi + c.phiOff + (adj ? 4LL * nb : 0);
    for (int i = threadIdx.x; i < 4 * nb; i += blockDim.x) dst[i] = B[i];
+   // five more squarings: Phi^32, the transition over a group of 32 units
+   for (int it = 0; it < 5; it++) {
+      for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+         int p = 0;
+         while (blk(p + 1, 0) <= b) p++;
+         const int q = b - blk(p, 0);
+         double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
+         for (int m = q; m <= p; m++) {
+            const double *x = B + 4 * blk(p, m), *y = B + 4 * blk(m, q);
+            r0 = fma(x[0], y[0], fma(x[1], y[2], r0));
+            r1 = fma(x[0], y[1], fma(x[1], y[3], r1));
+            r2 = fma(x[2], y[0], fma(x[3], y[2], r2));
+            r3 = fma(x[2], y[1], fma(x[3], y[3], r3));
+         }
+         double *o = C + 4 * b;
+         o[0] = r0;
+         o[1] = r1;
+         o[2] = r2;
+         o[3] = r3;
+      }
+      __syncthreads();
+      double *t = B;
+      B = C;
+      C = t;
+   }
+   dst = phi + c.phiOff + 8LL * nb + (adj ? 4LL * nb : 0);
+   for (int i = threadIdx.x; i < 4 * nb; i += blockDim.x) dst[i] = B[i];
 }
 
 // Per channel (one warp): z_0 = 0, checkpoint z_j, z_{j+1} = Phi z_j + e_j over the
@@ -229,21 +256,20 @@ __global__ void __launch_bounds__(32) bank_chain_kernel(const RaggedChan *chans,
    }
 }
 
-// The same chain for cascades of up to 16 stages (2S <= 32), in FP32 (Phi rounded once
-// from its FP64 product): lane r holds state component r and row r of Phi in registers;
-// each step broadcasts z by shuffles.  The unit aggregates are staged in shared memory
-// 64 units at a time (one coalesced read per window).
+// The same chain for cascades of up to 16 stages (2S <= 32), in FP32 (the transitions
+// rounded once from their FP64 products), in two levels so that its depth is about
+// 2 x 32 + units / 32 steps instead of one step per unit: each warp of the CTA runs
+// groups of 32 units from a zero state (group aggregates), warp 0 chains the groups
+// with Phi^32, then every group runs again from its true start and writes the
+// checkpoints.  In a step, lane r holds state component r and row r of the
+// transition in registers; z is broadcast by shuffles.  Group states sit in shared
+// memory for channels of up to 64 groups, in the caller's buffer beyond.
+constexpr int kChainWarps = 8;
+constexpr int kChainGroup = 32;
+constexpr int kChainSharedGroups = 64;
 
-__global__ void __launch_bounds__(32) bank_chain_fast_kernel(const RaggedChan *chans, const double *phi,
-                                                             const float2 *agg, float2 *ckpt, int adj)
+__device__ __forceinline__ void loadRow(float (&row)[2 * kChainFastStages], const double *P, int n2, int lane)
 {
-   __shared__ float sE[kChainWin * 2 * kChainFastStages];
-   const RaggedChan c = chans[blockIdx.x];
-   const int S = c.S, lane = threadIdx.x;
-   if (S == 0 || S > kChainFastStages) return;
-   const int n2 = 2 * S, nb = S * (S + 1) / 2;
-   const double *P = phi + c.phiOff + (adj ? 4LL * nb : 0);
-   float row[2 * kChainFastStages];
 #pragma unroll
    for (int k = 0; k < 2 * kChainFastStages; k++) row[k] = 0.0f;
    if (lane < n2) {
@@ -254,31 +280,79 @@ __global__ void __launch_bounds__(32) bank_chain_fast_kernel(const RaggedChan *c
          if (k < n2 && q <= p) row[k] = (float) P[4 * blk(p, q) + 2 * i + (k & 1)];
       }
    }
+}
+
+// z' = row . z + e (lane r: component r), z broadcast from lanes 0 .. n2 - 1.
+__device__ __forceinline__ float chainStep(const float (&row)[2 * kChainFastStages], float z, float e, int n2)
+{
+   float a0 = e, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+#pragma unroll
+   for (int q = 0; q < 2 * kChainFastStages; q += 4) {
+      if (q >= n2) break;
+      a0 = fmaf(row[q], __shfl_sync(0xffffffffu, z, q), a0);
+      a1 = fmaf(row[q + 1], __shfl_sync(0xffffffffu, z, q + 1), a1);
+      a2 = fmaf(row[q + 2], __shfl_sync(0xffffffffu, z, q + 2), a2);
+      a3 = fmaf(row[q + 3], __shfl_sync(0xffffffffu, z, q + 3), a3);
+   }
+   return (a0 + a1) + (a2 + a3);
+}
+
+__global__ void __launch_bounds__(kChainWarps * 32) bank_chain_fast_kernel(const RaggedChan *chans,
+                                                                           const double *phi, const float2 *agg,
+                                                                           float2 *ckpt, float *groupBuf, int adj)
+{
+   __shared__ float sE[kChainWarps][kChainGroup * 2 * kChainFastStages]; // a group's aggregates, per warp
+   __shared__ float sG[kChainSharedGroups * 2 * kChainFastStages];       // group states
+   const RaggedChan c = chans[blockIdx.x];
+   const int S = c.S, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   if (S == 0 || S > kChainFastStages) return;
+   const int n2 = 2 * S, nb = S * (S + 1) / 2;
+   const int units = (c.Lu + kUnit - 1) / kUnit, groups = (units + kChainGroup - 1) / kChainGroup;
+   float *G = groups <= kChainSharedGroups ? sG : groupBuf + c.grpOff;
    const float *ag = (const float *) (agg + c.ckOff);
    float *ck = (float *) (ckpt + c.ckOff);
-   const int units = (c.Lu + kUnit - 1) / kUnit;
-   float z = 0.0f;
-   for (int w0 = 0; w0 < units; w0 += kChainWin) {
-      const int wn = min(kChainWin, units - w0);
-      // units [j0, j0 + wn) of this window in memory order
-      const int j0 = adj ? units - w0 - wn : w0;
+   float row[2 * kChainFastStages];
+   // unit of step k of group g (processing order), and that group's units in memory order
+   auto unitOf = [&](int g, int k) { return adj ? units - 1 - (g * kChainGroup + k) : g * kChainGroup + k; };
+   auto stageGroup = [&](int g, int gn) {
+      const int j0 = adj ? units - g * kChainGroup - gn : g * kChainGroup;
       __syncwarp();
-      for (int q = lane; q < wn * n2; q += 32) sE[q] = ag[(long long) j0 * n2 + q];
+      for (int q = lane; q < gn * n2; q += 32) sE[warp][q] = ag[(long long) j0 * n2 + q];
       __syncwarp();
-      for (int k = 0; k < wn; k++) {
-         const int j = adj ? units - 1 - (w0 + k) : w0 + k;
+      return j0;
+   };
+   // 1. group aggregates from a zero state (the last group's is not needed)
+   loadRow(row, phi + c.phiOff + (adj ? 4LL * nb : 0), n2, lane);
+   for (int g = warp; g + 1 < groups; g += kChainWarps) {
+      const int j0 = stageGroup(g, kChainGroup);
+      float z = 0.0f;
+      for (int k = 0; k < kChainGroup; k++)
+         z = chainStep(row, z, lane < n2 ? sE[warp][(unitOf(g, k) - j0) * n2 + lane] : 0.0f, n2);
+      if (lane < n2) G[g * n2 + lane] = z;
+   }
+   __syncthreads();
+   // 2. true group starts: Z_0 = 0, Z_{g+1} = Phi^32 Z_g + E_g
+   if (warp == 0) {
+      float rowQ[2 * kChainFastStages];
+      loadRow(rowQ, phi + c.phiOff + 8LL * nb + (adj ? 4LL * nb : 0), n2, lane);
+      float Z = 0.0f;
+      for (int g = 0; g < groups; g++) {
+         const float E = (lane < n2 && g + 1 < groups) ? G[g * n2 + lane] : 0.0f;
+         __syncwarp();
+         if (lane < n2) G[g * n2 + lane] = Z;
+         if (g + 1 < groups) Z = chainStep(rowQ, Z, E, n2);
+      }
+   }
+   __syncthreads();
+   // 3. every group from its true start: the checkpoints
+   for (int g = warp; g < groups; g += kChainWarps) {
+      const int gn = min(kChainGroup, units - g * kChainGroup);
+      const int j0 = stageGroup(g, gn);
+      float z = lane < n2 ? G[g * n2 + lane] : 0.0f;
+      for (int k = 0; k < gn; k++) {
+         const int j = unitOf(g, k);
          if (lane < n2) ck[(long long) j * n2 + lane] = z;
-         if (w0 + k + 1 == units) break;
-         float a0 = lane < n2 ? sE[(j - j0) * n2 + lane] : 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
-#pragma unroll
-         for (int q = 0; q < 2 * kChainFastStages; q += 4) {
-            if (q >= n2) break;
-            a0 = fmaf(row[q], __shfl_sync(0xffffffffu, z, q), a0);
-            a1 = fmaf(row[q + 1], __shfl_sync(0xffffffffu, z, q + 1), a1);
-            a2 = fmaf(row[q + 2], __shfl_sync(0xffffffffu, z, q + 2), a2);
-            a3 = fmaf(row[q + 3], __shfl_sync(0xffffffffu, z, q + 3), a3);
-         }
-         z = (a0 + a1) + (a2 + a3);
+         if (k + 1 < gn) z = chainStep(row, z, lane < n2 ? sE[warp][(j - j0) * n2 + lane] : 0.0f, n2);
       }
    }
 }
@@ -662,7 +736,7 @@ __global__ void __launch_bounds__(32) bank_coef_kernel(const RaggedChan *chans, 
 
 } // namespace
 
-long long bankTransitionDoubles(int S) { return 4LL * S * (S + 1); } // both directions
+long long bankTransitionDoubles(int S) { return 8LL * S * (S + 1); } // Phi and Phi^32, both directions
 
 cudaError_t launchBankTables(const RaggedChan *chans, int C, const float *coefs, int totalStages, int Smax,
                              float *tables, double *phi, cudaStream_t s)
@@ -703,7 +777,7 @@ cudaError_t launchBankForward(const BankLaunch &b, cudaStream_t s)
    if ((e = cudaFuncSetAttribute(bank_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dynC)) !=
        cudaSuccess)
       return e;
-   bank_chain_fast_kernel<<<b.C, 32, 0, s>>>(b.chans, b.phi, b.aggF, b.ckptF, 0);
+   bank_chain_fast_kernel<<<b.C, kChainWarps * 32, 0, s>>>(b.chans, b.phi, b.aggF, b.ckptF, b.groupF, 0);
    countLaunch();
    if (b.Smax > kChainFastStages) {
       bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.phi, b.aggF, b.ckptF, 0);
@@ -734,7 +808,7 @@ cudaError_t launchBankBackward(const BankLaunch &b, cudaStream_t s)
    if ((e = cudaFuncSetAttribute(bank_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dynC)) !=
        cudaSuccess)
       return e;
-   bank_chain_fast_kernel<<<b.C, 32, 0, s>>>(b.chans, b.phi, b.aggA, b.ckptA, 1);
+   bank_chain_fast_kernel<<<b.C, kChainWarps * 32, 0, s>>>(b.chans, b.phi, b.aggA, b.ckptA, b.groupA, 1);
    countLaunch();
    if (b.Smax > kChainFastStages) {
       bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.phi, b.aggA, b.ckptA, 1);

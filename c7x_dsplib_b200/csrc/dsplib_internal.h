@@ -233,6 +233,7 @@ struct RaggedChan {
    int L, T, S, Lu;
    long long ckOff;  // first unit state (float2) of the channel: one per 512-sample unit and stage
    long long phiOff; // first double of the channel's unit transitions
+   long long grpOff; // first float of the channel's chain group states (2S per 32 units)
 };
 // Split-BF16x3 tensor-core FIR over a list of runs {channel, first tile, tiles, 0}
 // of kFirBfTile outputs: forward (valid correlation of the channel's x with its
@@ -270,6 +271,7 @@ struct BankLaunch {
    const float *gy;   // adjoint: output gradient
    float *g;          // adjoint: gradient w.r.t. the FIR output
    float2 *aggF, *ckptF, *aggA, *ckptA;
+   float *groupF, *groupA; // chain group states of channels beyond 64 groups of 32 units
    float *part;       // adjoint: 5 coefficient-gradient sums per unit and stage
    float *gcoefs;
    // forward with the loss fused (target != nullptr): gyOut = scale (y - target), unit

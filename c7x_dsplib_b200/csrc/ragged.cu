@@ -52,6 +52,7 @@ struct RaggedPlan {
    int nFwdItems = 0, nFirFwdRuns = 0, nFirDxRuns = 0, nUnits = 0;
    long long nCk = 0;  // unit states (float2): sum over channels of units x stages
    long long nPhi = 0; // doubles of the unit transitions
+   long long nGrp = 0; // floats of chain group states
    RaggedChan *dChan = nullptr;
    int2 *dFwdItems = nullptr;   // (channel, 2048-sample tile over Lu): taps-gradient partials, loss
    int4 *dFirFwdRuns = nullptr; // (channel, first tile, tiles): FIR forward, 8192-output tiles over Lu
@@ -62,9 +63,9 @@ struct RaggedPlan {
    int2 *dUnits = nullptr;      // cascade units (channel, unit index)
    int device = 0;
    // work buffer layout (float offsets)
-   long long wCk = 0, wAgg = 0, wTab = 0, wPhi = 0, wTotal = 0;
+   long long wCk = 0, wAgg = 0, wTab = 0, wPhi = 0, wGrp = 0, wTotal = 0;
    // scratch layout (float offsets)
-   long long sAgg = 0, sCk = 0, sPart = 0, sLoss = 0, sDh = 0, sTotal = 0;
+   long long sAgg = 0, sCk = 0, sGrp = 0, sPart = 0, sLoss = 0, sDh = 0, sTotal = 0;
 };
 
 namespace {
@@ -208,7 +209,7 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
       const int tiles = (outLen + kFirBfTile - 1) / kFirBfTile;
       for (int t = 0; t < tiles; t += kFirBfRunTiles) runs.push_back(make_int4(c, t, std::min(kFirBfRunTiles, tiles - t), 0));
    };
-   long long xo = 0, ho = 0, co = 0, po = 0, ck = 0, ph = 0;
+   long long xo = 0, ho = 0, co = 0, po = 0, ck = 0, ph = 0, gr = 0;
    for (int c = 0; c < numChannels; c++) {
       const int L = length[c], T = taps[c], S = stages[c];
       if (T < 1 || T > kFirBfMaxTaps || L < T || S < 0 || S > kRaggedMaxStages) {
@@ -217,7 +218,8 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
       }
       const int Lu = L - T + 1;
       const int nu = (Lu + kBankSpan - 1) / kBankSpan;
-      ch[c] = RaggedChan{xo, ho, co, po, L, T, S, Lu, ck, ph};
+      ch[c] = RaggedChan{xo, ho, co, po, L, T, S, Lu, ck, ph, gr};
+      gr += 2LL * S * ((nu + 31) / 32);
       po += (Lu + 15) & ~15;
       ck += (long long) nu * S;
       ph += bankTransitionDoubles(S);
@@ -255,6 +257,7 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    p->totalStages = (int) (co / 5);
    p->nCk = ck;
    p->nPhi = ph;
+   p->nGrp = gr;
    p->nFwdItems = (int) fwd.size();
    p->nFirFwdRuns = (int) firFwd.size();
    p->nFirDxRuns = (int) firDx.size();
@@ -266,11 +269,13 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    p->wAgg = p->wCk + align4(2 * p->nCk);
    p->wTab = p->wAgg + align4(2 * p->nCk);
    p->wPhi = p->wTab + (long long) kBankTabFloats * p->totalStages;
-   p->wTotal = p->wPhi + align4(2 * p->nPhi);
+   p->wGrp = p->wPhi + align4(2 * p->nPhi);
+   p->wTotal = p->wGrp + align4(p->nGrp);
    // scratch: g | adjoint aggregates | adjoint checkpoints | coefficient partials | taps partials
    p->sAgg = align4(p->totalLen);
    p->sCk = p->sAgg + align4(2 * p->nCk);
-   p->sPart = p->sCk + align4(2 * p->nCk);
+   p->sGrp = p->sCk + align4(2 * p->nCk);
+   p->sPart = p->sGrp + align4(p->nGrp);
    p->sLoss = p->sPart + align4(5 * p->nCk);
    p->sDh = p->sLoss + align4(2LL * p->nUnits); // unit sums of squares (doubles) of the fused loss
    p->sTotal = p->sDh + align4(std::max((long long) p->nDhRuns * kDhMaxT, 2LL * p->nFwdItems));
@@ -320,6 +325,7 @@ static BankLaunch bankLaunch(const RaggedPlan *p, const float *work)
    b.u = work;
    b.aggF = (float2 *) (work + p->wAgg);
    b.ckptF = (float2 *) (work + p->wCk);
+   b.groupF = (float *) (work + p->wGrp);
    return b;
 }
 
@@ -360,6 +366,7 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
    b.g = g;
    b.aggA = (float2 *) (scratch + p->sAgg);
    b.ckptA = (float2 *) (scratch + p->sCk);
+   b.groupA = scratch + p->sGrp;
    b.part = scratch + p->sPart;
    b.gcoefs = gcoefs;
    if (launchBankBackward(b, s) != cudaSuccess) return DSPLIB_ERR_FAILURE;
@@ -407,6 +414,7 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMse(DSPLIB_gpu_raggedPlan plan, co
    b.gy = gy;
    b.g = g;
    b.ckptA = (float2 *) (scratch + p->sCk);
+   b.groupA = scratch + p->sGrp;
    b.part = scratch + p->sPart;
    b.gcoefs = gcoefs;
    b.aggReady = true;
