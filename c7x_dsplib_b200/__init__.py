@@ -413,11 +413,13 @@ def q15tofl(x, dtype=np.float32, *, func_style=OPTIMIZED, out=None, handle=None,
 
 
 def fir_setup(dtype_code, batch, N, T, *, nch, func_style=OPTIMIZED, mma=False, shift=0, in_pitch=None,
-              out_pitch=None, filter_pitch=None):
-    """Descriptors + InitArgs for a FIR call, as the reference driver builds them."""
+              out_pitch=None, filter_pitch=None, float_q=None):
+    """Descriptors + InitArgs for a FIR call, as the reference driver builds them.
+    ``float_q``: FLOAT32 filters in float Q mode (InitArgs.enableQ = 1, Q = float_q)."""
     elt = _elt(dtype_code)
     args = FirInitArgs(funcStyle=func_style, dataSize=N, batchSize=batch, filterSize=T, shift=shift,
-                       enableNchCoefs=int(nch), enableMMA=int(mma), MMA_SIZE=MMA_SIZE[elt], enableQ=0, Q=0)
+                       enableNchCoefs=int(nch), enableMMA=int(mma), MMA_SIZE=MMA_SIZE[elt],
+                       enableQ=int(float_q is not None), Q=int(float_q or 0))
     out_size = N - T + 1
     pin = bp(dtype_code, N, batch, (in_pitch or N) * elt)
     pout = bp(dtype_code, (out_pitch or out_size), batch, (out_pitch or out_size) * elt)
@@ -429,7 +431,7 @@ def fir_setup(dtype_code, batch, N, T, *, nch, func_style=OPTIMIZED, mma=False, 
 
 
 def fir(x, h, T=None, *, nch=None, func_style=OPTIMIZED, precision=FIR_SIMT, qmode=False, shift=0, out=None,
-        handle=None, stream=None):
+        handle=None, stream=None, float_q=None):
     """y = FIR(x, h) over channel-major rows of ``x`` [batch, N] with stored
     taps ``h`` [1 or batch, T] (reference tap order).  numpy in -> numpy out
     (host staging inside the library); torch CUDA in -> torch CUDA out.
@@ -439,7 +441,8 @@ def fir(x, h, T=None, *, nch=None, func_style=OPTIMIZED, precision=FIR_SIMT, qmo
     if nch is None:
         nch = h.shape[0] > 1
     code = _dtype_code(x)
-    args, pin, pfilt, pout = fir_setup(code, batch, N, T, nch=nch, func_style=func_style, shift=shift)
+    args, pin, pfilt, pout = fir_setup(code, batch, N, T, nch=nch, func_style=func_style, shift=shift,
+                                       float_q=float_q)
     out_size = N - T + 1
     if out is None:
         if isinstance(x, np.ndarray):

@@ -182,11 +182,14 @@ enum FirKernelKind {
    FIR_F32_SIMT = 2,   // FP32 FMA register-tiled CUDA-core kernel
    FIR_F32_BF16X3 = 3, // tcgen05 split-BF16x3 tensor-core kernel
    FIR_INT_WRAP_TC = 4, // tcgen05 kind::i8 kernel, int8/int16, natural-C wrap output
-   FIR_INT_Q_TC = 5     // tcgen05 kind::i8 kernel, int8/int16, Q-mode output
+   FIR_INT_Q_TC = 5,    // tcgen05 kind::i8 kernel, int8/int16, Q-mode output
+   FIR_F32_Q = 6        // FLOAT32 in float Q mode (InitArgs.enableQ): int32 quantisation, exact sums
 };
 
 // Largest InitArgs.shift the Q-mode output stages accept.
 constexpr int kFirMaxQShift = 62;
+// Largest InitArgs.Q of the float Q mode (the reference scales by 1U << Q).
+constexpr int kFirMaxFloatQ = 31;
 
 cudaError_t launchFir(const FirLaunch &a, FirKernelKind kind, cudaStream_t s);
 

@@ -175,8 +175,16 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
       return DSPLIB_ERR_INVALID_VALUE;
    }
 
+   // Float Q mode: FLOAT32 filters quantised to int32 at scale 2^Q (InitArgs.enableQ / Q).
+   const bool floatQ = !natc && p->dtype == DSPLIB_FLOAT32 && ia.enableQ != 0;
+   if (floatQ && ia.Q > (uint32_t) kFirMaxFloatQ) {
+      setError(hc, "exec: float Q mode needs Q <= %d (got %u)", kFirMaxFloatQ, ia.Q);
+      return DSPLIB_ERR_INVALID_VALUE;
+   }
+
    FirKernelKind kind;
    if (natc) kind = FIR_NATC;
+   else if (floatQ) kind = FIR_F32_Q;
    else if (p->dtype == DSPLIB_FLOAT32)
       kind = hc->firPrecision == DSPLIB_GPU_FIR_BF16X3 ? FIR_F32_BF16X3 : FIR_F32_SIMT;
    else kind = hc->firQMode ? FIR_QMODE : FIR_NATC;
@@ -214,7 +222,7 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
    a.inPitch = p->inPitch;
    a.outPitch = p->outPitch;
    a.filtPitch = nch ? filtPitch : 0; // staging keeps the caller's row pitch
-   a.shift = (int) ia.shift;
+   a.shift = floatQ ? (int) ia.Q : (int) ia.shift;
    // Optimized 8/16-bit integers run on the tensor cores when the taps fit the band buffer.
    if (!natc && (p->dtype == DSPLIB_INT8 || p->dtype == DSPLIB_INT16) && firIntTcSupported(a))
       kind = hc->firQMode ? FIR_INT_Q_TC : FIR_INT_WRAP_TC;

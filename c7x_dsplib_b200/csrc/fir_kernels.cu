@@ -16,6 +16,8 @@
 // y[l*outPitch + j]; stored taps h[T-1-c] multiply x[j+c].
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include "dsplib_internal.h"
 
 namespace dsplib {
@@ -94,6 +96,59 @@ __global__ void __launch_bounds__(kDirThreads) fir_direct_kernel(FirLaunch a)
       for (int r = 0; r < kDirTile / kDirThreads; r++) {
          const int j = threadIdx.x + r * kDirThreads;
          if (j0 + j < a.outSize) y[j0 + j] = acc[r].out(a.shift);
+      }
+   }
+}
+
+// FLOAT32 filters in Q mode (InitArgs.enableQ): the C7x fixed-point MMA path of
+// src/DSPLIB_fir/DSPLIB_fir_ci.cpp:1559-1625.  Signal and taps are scaled by 2^Q and
+// converted to int32 (round to nearest even, saturating; NaN -> 0), the products are
+// summed exactly (128 bits), the sum is shifted right by Q with half-LSB rounding and
+// saturated to int32 (the MMA output stage, X_SHIFT = Q with rounding and saturation),
+// then converted to float and scaled by 2^-Q.
+__device__ __forceinline__ int quantQ(float v, float scale) { return __float2int_rn(v * scale); }
+
+__global__ void __launch_bounds__(kDirThreads) fir_floatq_kernel(FirLaunch a)
+{
+   __shared__ int xs[kDirTile + kDirTaps];
+   __shared__ int hs[kDirTaps];
+   const int j0 = blockIdx.x * kDirTile;
+   const long long inExtent = (long long) a.outSize + a.T - 1;
+   const int Q = a.shift;
+   const float scale = ldexpf(1.0f, Q), unscale = ldexpf(1.0f, -Q);
+   for (int l = blockIdx.y; l < a.batch; l += gridDim.y) {
+      const float *x = (const float *) a.x + (long long) l * a.inPitch;
+      const float *h = (const float *) a.h + (long long) l * a.filtPitch;
+      float *y = (float *) a.y + (long long) l * a.outPitch;
+      __int128 acc[kDirTile / kDirThreads];
+#pragma unroll
+      for (int r = 0; r < kDirTile / kDirThreads; r++) acc[r] = 0;
+      for (int cb = 0; cb < a.T; cb += kDirTaps) {
+         const int tb = min(kDirTaps, a.T - cb);
+         for (int k = threadIdx.x; k < kDirTile + tb - 1; k += kDirThreads) {
+            long long idx = (long long) j0 + cb + k;
+            xs[k] = idx < inExtent ? quantQ(x[idx], scale) : 0;
+         }
+         for (int k = threadIdx.x; k < tb; k += kDirThreads) hs[k] = quantQ(h[a.T - 1 - (cb + k)], scale);
+         __syncthreads();
+#pragma unroll
+         for (int r = 0; r < kDirTile / kDirThreads; r++) {
+            const int j = threadIdx.x + r * kDirThreads;
+            if (j0 + j < a.outSize)
+               for (int c = 0; c < tb; c++) acc[r] += (__int128) ((long long) xs[j + c] * (long long) hs[c]);
+         }
+         __syncthreads();
+      }
+#pragma unroll
+      for (int r = 0; r < kDirTile / kDirThreads; r++) {
+         const int j = threadIdx.x + r * kDirThreads;
+         if (j0 + j < a.outSize) {
+            __int128 v = acc[r];
+            if (Q > 0) v = (v + ((__int128) 1 << (Q - 1))) >> Q;
+            if (v < (__int128) INT32_MIN) v = INT32_MIN;
+            if (v > (__int128) INT32_MAX) v = INT32_MAX;
+            y[j0 + j] = (float) (int) v * unscale;
+         }
       }
    }
 }
@@ -187,6 +242,13 @@ cudaError_t launchFir(const FirLaunch &a, FirKernelKind kind, cudaStream_t s)
       if (a.dtype != DSPLIB_FLOAT32) return cudaErrorInvalidValue;
       dim3 grid((a.outSize + kSimtTile - 1) / kSimtTile, a.batch < 65535 ? a.batch : 65535);
       fir_f32_simt_kernel<<<grid, kSimtThreads, 0, s>>>(a);
+      countLaunch();
+      return cudaGetLastError();
+   }
+   case FIR_F32_Q: {
+      if (a.dtype != DSPLIB_FLOAT32 || a.shift < 0 || a.shift > kFirMaxFloatQ) return cudaErrorInvalidValue;
+      dim3 grid((a.outSize + kDirTile - 1) / kDirTile, a.batch < 65535 ? a.batch : 65535);
+      fir_floatq_kernel<<<grid, kDirThreads, 0, s>>>(a);
       countLaunch();
       return cudaGetLastError();
    }

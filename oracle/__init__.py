@@ -58,7 +58,7 @@ def port():
         if not os.path.exists(PORT_SO):
             build()
         _port = ctypes.CDLL(PORT_SO)
-        for name in ("oracle_fir_cn", "oracle_fir_q", "oracle_fir_f64", "oracle_biquad_df",
+        for name in ("oracle_fir_cn", "oracle_fir_q", "oracle_fir_floatq", "oracle_fir_f64", "oracle_biquad_df",
                      "oracle_biquad_df_f64", "oracle_biquad_tif", "oracle_tif_coefficients", "oracle_fltoq15",
                      "oracle_q15tofl", "oracle_transpose", "oracle_addnch"):
             getattr(_port, name).restype = None
@@ -114,6 +114,18 @@ def fir_q(x, h, T, shift, *, nch):
     y = np.zeros((batch, out_size), dtype=x.dtype)
     port().oracle_fir_q(DT[x.dtype], _ptr(x), _ptr(h), _ptr(y), batch, T, out_size, in_pitch, out_size,
                         h.shape[1] if nch else 0, int(shift))
+    return y
+
+
+def fir_floatq(x, h, T, Q, *, nch):
+    """FLOAT32 FIR in float Q mode (quantised to int32 at scale 2^Q, exact sums, rounding shift)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    h = np.ascontiguousarray(h, dtype=np.float32)
+    batch, in_pitch = x.shape
+    out_size = in_pitch - T + 1
+    y = np.zeros((batch, out_size), dtype=np.float32)
+    port().oracle_fir_floatq(_ptr(x), _ptr(h), _ptr(y), batch, T, out_size, in_pitch, out_size,
+                             h.shape[1] if nch else 0, int(Q))
     return y
 
 

@@ -102,6 +102,41 @@ void oracle_fir_q(int dtype, const void *x, const void *h, void *y, int batch, i
    }
 }
 
+/* FLOAT32 FIR in float Q mode (src/DSPLIB_fir/DSPLIB_fir_ci.cpp:1559-1625 with the
+ * helpers src/common/c71/DSPLIB_UTIL_Q_*.h): signal and taps times 2^Q converted to
+ * int32 (__float_to_int: round to nearest even, saturating; NaN taken as 0), an exact
+ * integer sum, the MMA output stage with X_SHIFT = Q (round half up, arithmetic shift,
+ * saturate to int32, src/DSPLIB_fir/DSPLIB_fir_ci.cpp:229-233), then int to float and
+ * times 2^-Q (the reciprocal of the scale, exact). */
+static int32_t quant_q(float v, float scale)
+{
+   float p = v * scale; /* one rounding, as the vector multiply */
+   if (p != p) return 0;
+   double r = nearbyint((double) p); /* the default rounding mode: nearest even */
+   if (r >= 2147483647.0) return INT32_MAX;
+   if (r <= -2147483648.0) return INT32_MIN;
+   return (int32_t) r;
+}
+
+void oracle_fir_floatq(const float *x, const float *h, float *y, int batch, int T, int outSize, int inPitch,
+                       int outPitch, int filtPitch, int Q)
+{
+   const float scale = ldexpf(1.0f, Q), unscale = ldexpf(1.0f, -Q);
+   for (int l = 0; l < batch; l++) {
+      for (int j = 0; j < outSize; j++) {
+         size_t xo = (size_t) l * inPitch + j;
+         size_t ho = (size_t) l * filtPitch;
+         __int128 acc = 0;
+         for (int c = 0; c < T; c++)
+            acc += (__int128) ((int64_t) quant_q(x[xo + c], scale) * (int64_t) quant_q(h[ho + T - 1 - c], scale));
+         if (Q > 0) acc = (acc + ((__int128) 1 << (Q - 1))) >> Q;
+         if (acc < INT32_MIN) acc = INT32_MIN;
+         if (acc > INT32_MAX) acc = INT32_MAX;
+         y[(size_t) l * outPitch + j] = (float) (int32_t) acc * unscale;
+      }
+   }
+}
+
 void oracle_fir_f64(const float *x, const float *h, double *y, int batch, int T, int outSize, int inPitch,
                     int outPitch, int filtPitch)
 {

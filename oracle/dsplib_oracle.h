@@ -35,6 +35,8 @@ void oracle_fir_cn(int dtype, const void *x, const void *h, void *y, int batch, 
  *   acc = exact sum;  y = sat_T((acc + 2^(s-1)) >> s)  (s > 0),  y = sat_T(acc)  (s == 0)
  * Rounding/saturation follow src/common/c7504/DSPLIB_configurations.cpp:94-160
  * (X_RE = 1: add half an LSB; X_SAT = 1: saturate to the output type). */
+void oracle_fir_floatq(const float *x, const float *h, float *y, int batch, int T, int outSize, int inPitch,
+                       int outPitch, int filtPitch, int Q);
 void oracle_fir_q(int dtype, const void *x, const void *h, void *y, int batch, int T, int outSize,
                   int inPitch, int outPitch, int filtPitch, int shift);
 

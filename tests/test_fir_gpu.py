@@ -408,3 +408,38 @@ def test_handles_on_concurrent_host_threads():
         want = oracle.fir(x, h, 33, nch=True)
         for y in ys:
             assert np.array_equal(y, want)
+
+
+# ------------------------------------------------------------------ float Q mode
+
+
+@pytest.mark.parametrize("Q", [0, 8, 15, 24, 31])
+@pytest.mark.parametrize("nch", [0, 1])
+def test_float_q_mode_bitexact(Q, nch):
+    """FLOAT32 with InitArgs.enableQ: quantised to int32 at scale 2^Q, exact integer sums,
+    rounding shift and saturation (the C7x fixed-point MMA path), bit-exact to the
+    restatement; the saturation at large Q included (|x| 2^31 overflows int32)."""
+    rng = np.random.default_rng(40 + Q + nch)
+    for (B, N, T) in [(1, 17, 17), (3, 2000, 64), (2, 5000, 1500)]:
+        x = rng.standard_normal((B, N)).astype(np.float32)
+        h = (rng.standard_normal((B if nch else 1, T)) / np.sqrt(T)).astype(np.float32)
+        x[0, :3] = [np.inf, -np.inf, np.nan]
+        got = host(D.fir(dev(x), dev(h), T, nch=nch, float_q=Q))
+        want = oracle.fir_floatq(x, h, T, Q, nch=nch)
+        assert np.array_equal(got, want, equal_nan=True), (B, N, T)
+
+
+def test_float_q_mode_tracks_fp64_and_rejects_large_q():
+    rng = np.random.default_rng(44)
+    x = rng.uniform(-1, 1, (2, 4096)).astype(np.float32)
+    h = (rng.standard_normal((1, 128)) / 16).astype(np.float32)
+    got = host(D.fir(dev(x), dev(h), 128, nch=0, float_q=20)).astype(np.float64)
+    w = oracle.fir_f64(x, h, 128, nch=0)
+    # each operand carries at most 2^-21 of quantisation error: |err| <= T 2^-20 max|x| max|h| roughly
+    assert np.abs(got - w).max() <= 128 * 2.0 ** -20 * float(np.abs(h).max() + 1)
+    args, pin, pf, po = D.fir_setup(D.FLOAT32, 2, 4096, 128, nch=0, float_q=32)
+    hd = D.FirHandle()
+    assert hd.init(args, pin, pf, po) == D.SUCCESS
+    out = dev(np.zeros((2, 4096 - 127), np.float32))
+    assert hd.exec(dev(x), dev(h), out) == D.ERR_INVALID_VALUE
+    assert "Q" in hd.last_error()

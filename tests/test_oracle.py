@@ -133,3 +133,22 @@ def test_q_mode_rounding_and_saturation():
     x = np.array([[100, 100]], np.int8)
     assert oracle.fir_q(x, h, 2, 0, nch=0).tolist() == [[127]]
     assert oracle.fir_q(-x, h, 2, 0, nch=0).tolist() == [[-128]]
+
+
+def test_float_q_mode_restatement_rules():
+    """Float Q mode (no reference test covers it; restated from the C7x MMA path):
+    x 2^Q and h 2^Q rounded to the nearest int32 (ties to even, saturating), exact sum,
+    sum rounded half up and shifted by Q, saturated to int32, scaled back by 2^-Q."""
+    Q = 2
+    # taps [1.0] -> hq = 4; x values at scale 4: 0.125 -> 0.5 -> 0 (tie to even), 0.375 -> 1.5 -> 2,
+    # 0.625 -> 2.5 -> 2, -0.375 -> -1.5 -> -2;  y = round_half_up(xq * 4 / 4) / 4 = xq / 4
+    x = np.array([[0.125, 0.375, 0.625, -0.375, 1e12]], np.float32)
+    h = np.array([[1.0]], np.float32)
+    y = oracle.fir_floatq(x, h, 1, Q, nch=0)
+    assert y[0, :4].tolist() == [0.0, 0.5, 0.5, -0.5]
+    # 1e12 * 4 saturates to 2^31 - 1; times hq = 4, shifted by 2: 2^31 - 1 again; / 4
+    assert y[0, 4] == np.float32(2147483647) / 4
+    # sums wider than 64 bits stay exact: 4 products of (2^31 - 1)^2 at Q = 0
+    x = np.full((1, 4), 3e9, np.float32)
+    h = np.full((1, 4), 3e9, np.float32)
+    assert oracle.fir_floatq(x, h, 4, 0, nch=0)[0, 0] == np.float32(2147483647)
