@@ -150,6 +150,9 @@ SIGNATURES = {
                                                    _P(ctypes.c_int32), _P(ctypes.c_int32)]),
     "DSPLIB_gpu_raggedPlanSize": (ctypes.c_int64, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_raggedPlanDestroy": (ctypes.c_int, [_VP]),
+    "DSPLIB_gpu_raggedPlanStatus": (ctypes.c_int, [_VP]),
+    "DSPLIB_gpu_status": (ctypes.c_int, [_VP]),
+    "DSPLIB_gpu_injectFault": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_firBiquadBatched_fwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_gpu_firBiquadBatched_bwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_gpu_raggedMseGrad": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
@@ -213,6 +216,12 @@ class _Handle:
         L = lib()
         self.buf = ctypes.create_string_buffer(int(getattr(L, self.size_fn)(None)))
         self.h = ctypes.cast(self.buf, ctypes.c_void_p)
+
+    def status(self) -> int:
+        return lib().DSPLIB_gpu_status(self.h)
+
+    def inject_fault(self, operation: int) -> int:
+        return lib().DSPLIB_gpu_injectFault(self.h, int(operation))
 
     def last_error(self) -> str:
         s = lib().DSPLIB_gpu_lastError(self.h)

@@ -124,6 +124,18 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_get_coefficients(uint32_t biquadForm,
 
    const uint32_t S = pIn->dim_x / DSPLIB_NUM_BIQUAD_COEFS;
    const uint32_t C = enableNChCoeffs ? pIn->dim_y : 1;
+   // Both buffers in device memory: the transform runs on the GPU, in place (the call
+   // returns once it is done, as the host form does).
+   if (isDevicePtr(pFilterCoeff) && isDevicePtr(pFilterCoeffOpt)) {
+      const long long pitch = enableNChCoeffs ? (long long) pOpt->stride_y / 4 : 0;
+      if (enableNChCoeffs && pitch < (long long) C) return DSPLIB_ERR_INVALID_DIMENSION;
+      if (launchBiquadCoefTransform(biquadForm == DSPLIB_BIQUAD_TIF, (int) enableNChCoeffs,
+                                    (const float *) pFilterCoeff, (float *) pFilterCoeffOpt, (int) S, (int) C, pitch,
+                                    0) != cudaSuccess ||
+          cudaStreamSynchronize(0) != cudaSuccess)
+         return DSPLIB_ERR_FAILURE;
+      return DSPLIB_SUCCESS;
+   }
    // Natural coefficients are read densely, [ch][stage][5] (utils.cpp:340-360).
    std::vector<float> nat((size_t) C * S * DSPLIB_NUM_BIQUAD_COEFS);
    if (!fetch(pFilterCoeff, nat.data(), nat.size() * 4)) return DSPLIB_ERR_FAILURE;
@@ -328,20 +340,24 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_exec(DSPLIB_kernelHandle handle,
    Region rc{pFilterCoeff, nullptr, cw, ch, cp, false, true};
    cudaStream_t sIn = pc ? pc->in : s;
    cudaError_t e;
+   injectArm(hc);
+   struct Disarm {
+      ~Disarm() { injectDisarm(); }
+   } disarm;
    if (pc) {
       // after whatever the caller queued on the handle's stream
       if ((e = cudaEventRecord(pc->start, s)) != cudaSuccess || (e = cudaStreamWaitEvent(pc->in, pc->start, 0)) ||
           (e = cudaStreamWaitEvent(pc->comp, pc->start, 0)) || (e = cudaStreamWaitEvent(pc->out, pc->start, 0)))
          return cudaFail(hc, e, "pipeline set-up");
    }
-   if ((e = regionIn(rin, 0, pc == nullptr, sIn)) != cudaSuccess) return cudaFail(hc, e, "stage input");
-   if ((e = regionIn(rc, 1, true, sIn)) != cudaSuccess) return cudaFail(hc, e, "stage coefficients");
-   if ((e = regionIn(rst, 3, true, sIn)) != cudaSuccess) return cudaFail(hc, e, "stage state");
+   if ((e = injectCheck(regionIn(rin, 0, pc == nullptr, sIn))) != cudaSuccess) return pipeFail(hc, pc, e, "stage input");
+   if ((e = injectCheck(regionIn(rc, 1, true, sIn))) != cudaSuccess) return pipeFail(hc, pc, e, "stage coefficients");
+   if ((e = injectCheck(regionIn(rst, 3, true, sIn))) != cudaSuccess) return pipeFail(hc, pc, e, "stage state");
    if (pOut == pIn && rin.staged) {
       rout = rin; // in-place on a host buffer: the staged copy is both input and output
    }
-   else if ((e = regionIn(rout, 2, false, sIn)) != cudaSuccess) {
-      return cudaFail(hc, e, "stage output");
+   else if ((e = injectCheck(regionIn(rout, 2, false, sIn))) != cudaSuccess) {
+      return pipeFail(hc, pc, e, "stage output");
    }
 
    BiquadLaunch a;
@@ -364,8 +380,8 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_exec(DSPLIB_kernelHandle handle,
       return natc ? launchBiquadSequential(l, st) : launchBiquadScan(l, st);
    };
    if (!pc) {
-      if ((e = launch(a, s)) != cudaSuccess) return cudaFail(hc, e, "biquad kernel launch");
-      if ((e = regionOut(rout, s)) != cudaSuccess) return cudaFail(hc, e, "copy output");
+      if ((e = injectCheck(launch(a, s))) != cudaSuccess) return cudaFail(hc, e, "biquad kernel launch");
+      if ((e = injectCheck(regionOut(rout, s))) != cudaSuccess) return cudaFail(hc, e, "copy output");
    }
    else {
       int nblk = (int) (rin.bytes() / kBqPipeBlockBytes);
@@ -375,8 +391,8 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_exec(DSPLIB_kernelHandle handle,
       for (int b = 0; b * rowsPer < N; b++) {
          const int r0 = b * rowsPer, rows = (N - r0) < rowsPer ? (N - r0) : rowsPer;
          const size_t inOff = (size_t) r0 * rin.pitch, outOff = (size_t) r0 * rout.pitch;
-         if ((e = copyRows((char *) rin.dev + inOff, (const char *) rin.host + inOff, rin.width, rows, rin.pitch,
-                           cudaMemcpyHostToDevice, pc->in)) != cudaSuccess ||
+         if ((e = injectCheck(copyRows((char *) rin.dev + inOff, (const char *) rin.host + inOff, rin.width, rows,
+                                       rin.pitch, cudaMemcpyHostToDevice, pc->in))) != cudaSuccess ||
              (e = cudaEventRecord(pc->copied[b], pc->in)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->comp, pc->copied[b], 0)) != cudaSuccess)
             return pipeFail(hc, pc, e, "copy input block");
@@ -384,18 +400,18 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_exec(DSPLIB_kernelHandle handle,
          blk.x = a.x + (size_t) r0 * a.inPitch;
          blk.y = a.y + (size_t) r0 * a.outPitch;
          blk.N = rows;
-         if ((e = launch(blk, pc->comp)) != cudaSuccess) return pipeFail(hc, pc, e, "biquad kernel launch");
+         if ((e = injectCheck(launch(blk, pc->comp))) != cudaSuccess) return pipeFail(hc, pc, e, "biquad kernel launch");
          if ((e = cudaEventRecord(pc->computed[b], pc->comp)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->out, pc->computed[b], 0)) != cudaSuccess ||
-             (e = copyRows((char *) rout.host + outOff, (const char *) rout.dev + outOff, rout.width, rows,
-                           rout.pitch, cudaMemcpyDeviceToHost, pc->out)) != cudaSuccess)
+             (e = injectCheck(copyRows((char *) rout.host + outOff, (const char *) rout.dev + outOff, rout.width,
+                                       rows, rout.pitch, cudaMemcpyDeviceToHost, pc->out))) != cudaSuccess)
             return pipeFail(hc, pc, e, "copy output block");
       }
       // the state is final once the last block's kernel has run (the out stream waited for it)
       if ((e = cudaEventRecord(pc->done, pc->out)) != cudaSuccess || (e = cudaStreamWaitEvent(s, pc->done, 0)))
          return pipeFail(hc, pc, e, "pipeline join");
    }
-   if ((e = regionOut(rst, s)) != cudaSuccess) return cudaFail(hc, e, "copy state");
+   if ((e = injectCheck(regionOut(rst, s))) != cudaSuccess) return pipeFail(hc, pc, e, "copy state");
    if (mustSync(hc, rin.staged || rout.staged || rst.staged || rc.staged,
                 rin.onHost || rout.onHost || rst.onHost || rc.onHost)) {
       if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, "biquad execution");

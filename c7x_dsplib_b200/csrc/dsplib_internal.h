@@ -30,6 +30,8 @@ struct HandleCommon {
    int32_t firPrecision;
    int32_t firQMode;
    char err[200];
+   int32_t errSlot;  // 1 + this handle's slot in the error-word pool (0: none yet)
+   int32_t injectAt; // testing: the n-th CUDA operation of the next exec reports failure (0: off)
 };
 
 struct FirPriv {
@@ -88,6 +90,24 @@ struct AddNChPriv {
 // ---------------------------------------------------------------- runtime
 
 void setError(HandleCommon *h, const char *fmt, ...);
+
+// Error words written by kernels when a bounded wait gives up: one per handle, in
+// mapped page-locked host memory (kernels store to it, the host reads it after the
+// stream has synchronized; no copy).  errorWord never returns null.
+int *errorWord(HandleCommon *h);
+void releaseErrorWord(HandleCommon *h);
+// The word's value, cleared when set.
+int takeErrorWord(HandleCommon *h);
+// Process-wide words for callers without a handle (filter-bank plans).
+int *allocErrorWord();
+void freeErrorWord(int *w);
+
+// Fault injection for tests (DSPLIB_gpu_injectFault): armed from the handle at the start
+// of an exec on this thread; injectCheck passes e through, except that the armed
+// operation (counted over the calls of injectCheck) reports cudaErrorUnknown.
+void injectArm(HandleCommon *h);
+void injectDisarm();
+cudaError_t injectCheck(cudaError_t e);
 DSPLIB_STATUS cudaFail(HandleCommon *h, cudaError_t e, const char *what);
 void countLaunch(int n = 1);
 
@@ -174,6 +194,7 @@ struct FirLaunch {
    long long outPitch;  // elements
    long long filtPitch; // elements between tap rows, 0 = shared
    int shift;
+   int *err = nullptr; // tensor-core kernels: error word for an expired bounded wait
 };
 
 enum FirKernelKind {
@@ -223,9 +244,6 @@ cudaError_t launchAddNCh(const AddNChLaunch &a, cudaStream_t s);
 bool firIntTcSupported(const FirLaunch &a);
 bool firBf16x3Supported(const FirLaunch &a);
 cudaError_t launchFirIntTc(const FirLaunch &a, bool qmode, cudaStream_t s);
-// Error word written by the tensor-core kernels when a bounded wait gives up
-// (-1: could not be read).
-int firTcErrorFlag(bool clear);
 
 // One channel of the batched filter bank: samples at xOff (length L; the FIR
 // output and the biquad signals use the first Lu = L - T + 1), T taps at hOff,
@@ -250,9 +268,9 @@ int raggedPlanDevice(DSPLIB_gpu_raggedPlan plan);
 // tiles, partial slot} of 8192 samples of the gradient at the FIR output:
 // part[slot * 512 + c] = sum over the run of gu[j] x[j + c], c < T.
 cudaError_t launchFirDhBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *x,
-                                    const float *gu, float *part, cudaStream_t s);
+                                    const float *gu, float *part, int *err, cudaStream_t s);
 cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *in,
-                                  const float *taps, float *out, bool dx, int Tmax, cudaStream_t s);
+                                  const float *taps, float *out, bool dx, int Tmax, int *err, cudaStream_t s);
 
 // Cascade of the filter bank split along time (bank_scan.cu): units of kBankSpan
 // samples (one warp each), chained per channel through the 2S-dimensional cascade
@@ -304,6 +322,12 @@ struct BiquadLaunch {
    long long inPitch, outPitch, varPitch, coefPitch; // elements
    int prefetch = 0; // x is device memory: the scan kernel may fetch the next window early (cp.async)
 };
+
+// DSPLIB_cascadeBiquad_get_coefficients for device buffers (coef_kernels.cu): TIF transform
+// (tif != 0) or the per-channel coefficient-major reorder of the DF forms; pitch in floats
+// between the rows of per-channel layouts.
+cudaError_t launchBiquadCoefTransform(int tif, int nch, const float *nat, float *opt, int S, int C, long long pitch,
+                                      cudaStream_t s);
 
 // NATC: sequential recursion per channel, bit-exact to the reference _cn kernels.
 cudaError_t launchBiquadSequential(const BiquadLaunch &a, cudaStream_t s);

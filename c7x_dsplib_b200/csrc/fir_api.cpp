@@ -201,15 +201,19 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
       pc = pipeContext();
    cudaStream_t sIn = pc ? pc->in : s;
    cudaError_t e;
+   injectArm(hc);
+   struct Disarm {
+      ~Disarm() { injectDisarm(); }
+   } disarm;
    if (pc) {
       // after whatever the caller queued on the handle's stream
       if ((e = cudaEventRecord(pc->start, s)) != cudaSuccess || (e = cudaStreamWaitEvent(pc->in, pc->start, 0)) ||
           (e = cudaStreamWaitEvent(pc->comp, pc->start, 0)) || (e = cudaStreamWaitEvent(pc->out, pc->start, 0)))
          return cudaFail(hc, e, "pipeline set-up");
    }
-   if ((e = regionIn(rin, 0, pc == nullptr, sIn)) != cudaSuccess) return cudaFail(hc, e, "stage input");
-   if ((e = regionIn(rf, 1, true, sIn)) != cudaSuccess) return cudaFail(hc, e, "stage filter");
-   if ((e = regionIn(rout, 2, false, sIn)) != cudaSuccess) return cudaFail(hc, e, "stage output");
+   if ((e = injectCheck(regionIn(rin, 0, pc == nullptr, sIn))) != cudaSuccess) return pipeFail(hc, pc, e, "stage input");
+   if ((e = injectCheck(regionIn(rf, 1, true, sIn))) != cudaSuccess) return pipeFail(hc, pc, e, "stage filter");
+   if ((e = injectCheck(regionIn(rout, 2, false, sIn))) != cudaSuccess) return pipeFail(hc, pc, e, "stage output");
 
    FirLaunch a;
    a.x = rin.dev;
@@ -223,14 +227,15 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
    a.outPitch = p->outPitch;
    a.filtPitch = nch ? filtPitch : 0; // staging keeps the caller's row pitch
    a.shift = floatQ ? (int) ia.Q : (int) ia.shift;
+   a.err = errorWord(hc);
    // Optimized 8/16-bit integers run on the tensor cores when the taps fit the band buffer.
    if (!natc && (p->dtype == DSPLIB_INT8 || p->dtype == DSPLIB_INT16) && firIntTcSupported(a))
       kind = hc->firQMode ? FIR_INT_Q_TC : FIR_INT_WRAP_TC;
    // Split-BF16x3 covers up to 512 taps; longer filters run the FP32 CUDA-core kernel.
    if (kind == FIR_F32_BF16X3 && !firBf16x3Supported(a)) kind = FIR_F32_SIMT;
    if (!pc) {
-      if ((e = launchFir(a, kind, s)) != cudaSuccess) return cudaFail(hc, e, "FIR kernel launch");
-      if ((e = regionOut(rout, s)) != cudaSuccess) return cudaFail(hc, e, "copy output");
+      if ((e = injectCheck(launchFir(a, kind, s))) != cudaSuccess) return cudaFail(hc, e, "FIR kernel launch");
+      if ((e = injectCheck(regionOut(rout, s))) != cudaSuccess) return cudaFail(hc, e, "copy output");
    }
    else {
       const size_t total = rin.bytes() + rout.bytes();
@@ -240,8 +245,8 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
       for (int b = 0; b * rowsPer < batch; b++) {
          const int r0 = b * rowsPer, rows = (batch - r0) < rowsPer ? (batch - r0) : rowsPer;
          const size_t inOff = (size_t) r0 * rin.pitch, outOff = (size_t) r0 * rout.pitch;
-         if ((e = copyRows((char *) rin.dev + inOff, (const char *) rin.host + inOff, rin.width, rows, rin.pitch,
-                           cudaMemcpyHostToDevice, pc->in)) != cudaSuccess ||
+         if ((e = injectCheck(copyRows((char *) rin.dev + inOff, (const char *) rin.host + inOff, rin.width, rows,
+                                       rin.pitch, cudaMemcpyHostToDevice, pc->in))) != cudaSuccess ||
              (e = cudaEventRecord(pc->copied[b], pc->in)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->comp, pc->copied[b], 0)) != cudaSuccess)
             return pipeFail(hc, pc, e, "copy input block");
@@ -250,11 +255,12 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
          blk.y = (char *) a.y + outOff;
          blk.h = (const char *) a.h + (nch ? (size_t) r0 * filtPitch * elt : 0);
          blk.batch = rows;
-         if ((e = launchFir(blk, kind, pc->comp)) != cudaSuccess) return pipeFail(hc, pc, e, "FIR kernel launch");
+         if ((e = injectCheck(launchFir(blk, kind, pc->comp))) != cudaSuccess)
+            return pipeFail(hc, pc, e, "FIR kernel launch");
          if ((e = cudaEventRecord(pc->computed[b], pc->comp)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->out, pc->computed[b], 0)) != cudaSuccess ||
-             (e = copyRows((char *) rout.host + outOff, (const char *) rout.dev + outOff, rout.width, rows,
-                           rout.pitch, cudaMemcpyDeviceToHost, pc->out)) != cudaSuccess)
+             (e = injectCheck(copyRows((char *) rout.host + outOff, (const char *) rout.dev + outOff, rout.width,
+                                       rows, rout.pitch, cudaMemcpyDeviceToHost, pc->out))) != cudaSuccess)
             return pipeFail(hc, pc, e, "copy output block");
       }
       if ((e = cudaEventRecord(pc->done, pc->out)) != cudaSuccess || (e = cudaStreamWaitEvent(s, pc->done, 0)))
@@ -262,7 +268,7 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
    }
    if (mustSync(hc, rin.staged || rf.staged || rout.staged, rin.onHost || rf.onHost || rout.onHost)) {
       if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, "FIR execution");
-      if ((kind == FIR_INT_WRAP_TC || kind == FIR_INT_Q_TC || kind == FIR_F32_BF16X3) && firTcErrorFlag(true) != 0) {
+      if ((kind == FIR_INT_WRAP_TC || kind == FIR_INT_Q_TC || kind == FIR_F32_BF16X3) && takeErrorWord(hc) != 0) {
          setError(hc, "tensor-core FIR: a bounded wait for MMA completion expired; outputs are incomplete");
          return DSPLIB_ERR_FAILURE;
       }

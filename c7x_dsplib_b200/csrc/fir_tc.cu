@@ -37,8 +37,8 @@
 // one.  The integer kernel is persistent: one wave of CTAs strides over the
 // (channel, tile range) work items, keeps a band of shared taps for all of them
 // and fetches each item's first segment during the previous item's last tile.
-// All waits on the tensor core are bounded; on expiry the kernel raises
-// g_firTcError, frees its TMEM and exits.
+// All waits on the tensor core are bounded; on expiry the kernel sets the error word it
+// was given (the calling handle's or plan's), frees its TMEM and exits.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -47,7 +47,12 @@
 
 namespace dsplib {
 
-__device__ int g_firTcError; // set when a bounded wait for the tensor core gives up
+// Set the error word of the call (mapped page-locked host memory; a plain store, since
+// atomics on host memory are not available on every system).
+__device__ __forceinline__ void raiseError(int *err)
+{
+   if (err) *(volatile int *) err = 1;
+}
 
 namespace {
 
@@ -367,7 +372,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 2 ? 6 : 8) fir_int_tc_k
             }
          }
          const bool done = tc::mbarWait(mbar, iter & 1);
-         if (!done && tid == 0) atomicExch(&g_firTcError, 1);
+         if (!done && tid == 0) raiseError(a.err);
          failed = __syncthreads_or(!done) != 0;
          iter++;
          tc::fenceAfterSync();
@@ -592,6 +597,7 @@ struct BfRun {
    float *y;
    long long inShift, inLen;
    int outLen, T, reverse, t0, t1;
+   int *err; // error word for an expired bounded wait
 };
 
 // Shared memory for taps up to Tmax: the hi/lo signal planes of the current
@@ -653,7 +659,7 @@ __device__ __forceinline__ bool bfDrain(const BfRun &r, const BfSmem &L, uint32_
    const int warp = tid >> 5, lane = tid & 31;
    const bool done = tid == 0 ? tc::mbarWait(L.mbar, pp.iter & 1) : true; // the barrier releases the rest
    pp.iter++;
-   if (!done && tid == 0) atomicExch(&g_firTcError, 1);
+   if (!done && tid == 0) raiseError(r.err);
    if (__syncthreads_or(!done)) return false;
    tc::fenceAfterSync();
    const long long j0 = (long long) t * kBfTile;
@@ -768,7 +774,7 @@ __device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint3
          pp.par ^= 1u << k;
          pp.pending &= ~(1u << k);
       }
-      if (!ok && tid == 0) atomicExch(&g_firTcError, 1);
+      if (!ok && tid == 0) raiseError(r.err);
       // raw tile landed; the previous tile's outputs have left the planes
       if (__syncthreads_or(!ok)) return false;
       if (viaBulk) bfSplit(L.slot(k), nb, L.hi, L.lo, tid);
@@ -849,6 +855,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) fir_bf16x3_tc_kernel(FirLaunch 
       r.reverse = 1;
       r.t0 = blockIdx.x * tilesPerCta;
       r.t1 = min(nt, r.t0 + tilesPerCta);
+      r.err = a.err;
       if (!bfProcess(r, L, tmem, pp, tid)) break;
    }
    bfEnd(L, pp, tmem, tid);
@@ -860,7 +867,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) fir_bf16x3_tc_kernel(FirLaunch 
 // of the output gradient with the taps.
 __global__ void __launch_bounds__(kBfThreads, 1)
     fir_bf16x3_ragged_kernel(const RaggedChan *chans, const int4 *runs, const float *in, const float *taps,
-                             float *out, int dx, int Tmax)
+                             float *out, int dx, int Tmax, int *err)
 {
    extern __shared__ __align__(16) unsigned char smraw[];
    const BfSmem L = bfSmemLayout(smraw, Tmax);
@@ -879,6 +886,7 @@ __global__ void __launch_bounds__(kBfThreads, 1)
    r.reverse = dx ? 0 : 1;
    r.t0 = it.y;
    r.t1 = it.y + it.z;
+   r.err = err;
    BfPipe pp;
    bfProcess(r, L, tmem, pp, tid);
    bfEnd(L, pp, tmem, tid);
@@ -925,7 +933,8 @@ __device__ __forceinline__ uint64_t descSw128Mn(uint32_t saddr, uint32_t lbo, ui
 }
 
 __global__ void __launch_bounds__(kBfThreads, 1)
-    fir_dh_bf16x3_kernel(const RaggedChan *chans, const int4 *runs, const float *x, const float *gu, float *part)
+    fir_dh_bf16x3_kernel(const RaggedChan *chans, const int4 *runs, const float *x, const float *gu, float *part,
+                         int *err)
 {
    extern __shared__ __align__(16) unsigned char smraw[];
    unsigned char *sm = (unsigned char *) (((uintptr_t) smraw + 1023) & ~(uintptr_t) 1023);
@@ -987,7 +996,7 @@ __global__ void __launch_bounds__(kBfThreads, 1)
          if (k >= 1) {
             const bool done = tid == 0 ? tc::mbarWait(mbar + (1 - b), (par >> (1 - b)) & 1) : true;
             par ^= 1u << (1 - b);
-            if (!done && tid == 0) atomicExch(&g_firTcError, 1);
+            if (!done && tid == 0) raiseError(err);
             ok = !__syncthreads_or(!done);
             if (!ok) break;
          }
@@ -1005,7 +1014,7 @@ __global__ void __launch_bounds__(kBfThreads, 1)
       const bool done = tid == 0 ? tc::mbarWait(mbar + b, (par >> b) & 1) : true;
       par ^= 1u << b;
       if (!done && tid == 0) {
-         atomicExch(&g_firTcError, 1);
+         raiseError(err);
          fail = true;
       }
    }
@@ -1071,7 +1080,7 @@ cudaError_t launchFirBf16x3(const FirLaunch &a, cudaStream_t s)
 }
 
 cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *in,
-                                  const float *taps, float *out, bool dx, int Tmax, cudaStream_t s)
+                                  const float *taps, float *out, bool dx, int Tmax, int *err, cudaStream_t s)
 {
    if (Tmax < 1 || Tmax > kBfMaxTaps) return cudaErrorNotSupported;
    if (nRuns <= 0) return cudaSuccess;
@@ -1079,32 +1088,22 @@ cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int
    cudaError_t e =
        cudaFuncSetAttribute(fir_bf16x3_ragged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
    if (e != cudaSuccess) return e;
-   fir_bf16x3_ragged_kernel<<<nRuns, kBfThreads, smem, s>>>(chans, runs, in, taps, out, dx ? 1 : 0, Tmax);
+   fir_bf16x3_ragged_kernel<<<nRuns, kBfThreads, smem, s>>>(chans, runs, in, taps, out, dx ? 1 : 0, Tmax, err);
    countLaunch();
    return cudaGetLastError();
 }
 
 cudaError_t launchFirDhBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *x,
-                                    const float *gu, float *part, cudaStream_t s)
+                                    const float *gu, float *part, int *err, cudaStream_t s)
 {
    if (nRuns <= 0) return cudaSuccess;
    cudaError_t e =
        cudaFuncSetAttribute(fir_dh_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kDhSmem);
    if (e != cudaSuccess) return e;
-   fir_dh_bf16x3_kernel<<<nRuns, kBfThreads, kDhSmem, s>>>(chans, runs, x, gu, part);
+   fir_dh_bf16x3_kernel<<<nRuns, kBfThreads, kDhSmem, s>>>(chans, runs, x, gu, part, err);
    countLaunch();
    return cudaGetLastError();
 }
 
-int firTcErrorFlag(bool clear)
-{
-   int v = 0;
-   if (cudaMemcpyFromSymbol(&v, g_firTcError, sizeof(int)) != cudaSuccess) return -1;
-   if (clear && v) {
-      int z = 0;
-      cudaMemcpyToSymbol(g_firTcError, &z, sizeof(int));
-   }
-   return v;
-}
 
 } // namespace dsplib

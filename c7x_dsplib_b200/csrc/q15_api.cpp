@@ -68,8 +68,12 @@ DSPLIB_STATUS convertExec(HandleCommon *hc, void *pIn, size_t eltIn, void *pOut,
    prepare(in);
    prepare(out);
    cudaError_t e;
+   injectArm(hc);
+   struct Disarm {
+      ~Disarm() { injectDisarm(); }
+   } disarm;
    if (!in.staged && !out.staged) {
-      if ((e = launch(in.dev, out.dev, n, s)) != cudaSuccess) return cudaFail(hc, e, what);
+      if ((e = injectCheck(launch(in.dev, out.dev, n, s))) != cudaSuccess) return cudaFail(hc, e, what);
       const bool hostSide = in.dev != in.host || out.dev != out.host;
       if (mustSync(hc, false, hostSide) && (e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(hc, e, what);
       return DSPLIB_SUCCESS;
@@ -81,10 +85,12 @@ DSPLIB_STATUS convertExec(HandleCommon *hc, void *pIn, size_t eltIn, void *pOut,
    const size_t staged = (in.staged ? inBytes : 0) + (out.staged ? outBytes : 0);
    PipeContext *pc = staged >= kConvPipeMinBytes ? pipeContext() : nullptr;
    if (!pc) {
-      if (in.staged && (e = cudaMemcpyAsync(in.dev, in.host, inBytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      if (in.staged &&
+          (e = injectCheck(cudaMemcpyAsync(in.dev, in.host, inBytes, cudaMemcpyHostToDevice, s))) != cudaSuccess)
          return cudaFail(hc, e, "copy input");
-      if ((e = launch(in.dev, out.dev, n, s)) != cudaSuccess) return cudaFail(hc, e, what);
-      if (out.staged && (e = cudaMemcpyAsync(out.host, out.dev, outBytes, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      if ((e = injectCheck(launch(in.dev, out.dev, n, s))) != cudaSuccess) return cudaFail(hc, e, what);
+      if (out.staged &&
+          (e = injectCheck(cudaMemcpyAsync(out.host, out.dev, outBytes, cudaMemcpyDeviceToHost, s))) != cudaSuccess)
          return cudaFail(hc, e, "copy output");
    }
    else {
@@ -99,18 +105,18 @@ DSPLIB_STATUS convertExec(HandleCommon *hc, void *pIn, size_t eltIn, void *pOut,
       for (int b = 0; (long long) b * per < n; b++) {
          const long long e0 = (long long) b * per, cnt = (n - e0) < per ? (n - e0) : per;
          char *di = (char *) in.dev + e0 * eltIn, *dout = (char *) out.dev + e0 * eltOut;
-         if (in.staged &&
-             (e = cudaMemcpyAsync(di, (char *) in.host + e0 * eltIn, cnt * eltIn, cudaMemcpyHostToDevice, pc->in)))
+         if (in.staged && (e = injectCheck(cudaMemcpyAsync(di, (char *) in.host + e0 * eltIn, cnt * eltIn,
+                                                           cudaMemcpyHostToDevice, pc->in))))
             return pipeFail(hc, pc, e, "copy input block");
          if ((e = cudaEventRecord(pc->copied[b], pc->in)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->comp, pc->copied[b], 0)) != cudaSuccess)
             return pipeFail(hc, pc, e, "pipeline");
-         if ((e = launch(di, dout, cnt, pc->comp)) != cudaSuccess) return pipeFail(hc, pc, e, what);
+         if ((e = injectCheck(launch(di, dout, cnt, pc->comp))) != cudaSuccess) return pipeFail(hc, pc, e, what);
          if ((e = cudaEventRecord(pc->computed[b], pc->comp)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(pc->out, pc->computed[b], 0)) != cudaSuccess)
             return pipeFail(hc, pc, e, "pipeline");
-         if (out.staged && (e = cudaMemcpyAsync((char *) out.host + e0 * eltOut, dout, cnt * eltOut,
-                                                cudaMemcpyDeviceToHost, pc->out)))
+         if (out.staged && (e = injectCheck(cudaMemcpyAsync((char *) out.host + e0 * eltOut, dout, cnt * eltOut,
+                                                            cudaMemcpyDeviceToHost, pc->out))))
             return pipeFail(hc, pc, e, "copy output block");
       }
       if ((e = cudaEventRecord(pc->done, pc->out)) != cudaSuccess || (e = cudaStreamWaitEvent(s, pc->done, 0)))

@@ -61,6 +61,7 @@ struct RaggedPlan {
    int4 *dDhRuns = nullptr;     // (channel, first tile, tiles, slot): taps gradient, longest first
    int nDhRuns = 0;
    int2 *dUnits = nullptr;      // cascade units (channel, unit index)
+   int *err = nullptr;          // error word of the tensor-core kernels (mapped page-locked)
    int device = 0;
    // work buffer layout (float offsets)
    long long wCk = 0, wAgg = 0, wTab = 0, wPhi = 0, wGrp = 0, wTotal = 0;
@@ -153,6 +154,7 @@ static void freePlan(RaggedPlan *p)
    cudaFree(p->dDhStart);
    cudaFree(p->dDhRuns);
    cudaFree(p->dUnits);
+   freeErrorWord(p->err);
    delete p;
 }
 
@@ -264,6 +266,7 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    p->nUnits = (int) units.size();
    p->nDhRuns = (int) dhRuns.size();
    cudaGetDevice(&p->device);
+   p->err = allocErrorWord();
    // work buffer: u | forward checkpoints | forward aggregates | stage tables | unit transitions
    p->wCk = align4(p->planeStride);
    p->wAgg = p->wCk + align4(2 * p->nCk);
@@ -306,6 +309,17 @@ int64_t DSPLIB_gpu_raggedPlanSize(DSPLIB_gpu_raggedPlan plan, int32_t what)
    }
 }
 
+DSPLIB_STATUS DSPLIB_gpu_raggedPlanStatus(DSPLIB_gpu_raggedPlan plan)
+{
+   RaggedPlan *p = (RaggedPlan *) plan;
+   if (!p) return DSPLIB_ERR_NULL_POINTER;
+   if (p->err && *(volatile int *) p->err != 0) {
+      *(volatile int *) p->err = 0;
+      return DSPLIB_ERR_FAILURE;
+   }
+   return DSPLIB_SUCCESS;
+}
+
 DSPLIB_STATUS DSPLIB_gpu_raggedPlanDestroy(DSPLIB_gpu_raggedPlan plan)
 {
    freePlan((RaggedPlan *) plan);
@@ -340,7 +354,7 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_fwd(DSPLIB_gpu_raggedPlan plan, const 
    float *u = work;
    BankLaunch b = bankLaunch(p, work);
    b.y = y;
-   if (launchFirBf16x3Ragged(p->dChan, p->dFirFwdRuns, p->nFirFwdRuns, x, taps, u, false, p->Tmax, s) != cudaSuccess)
+   if (launchFirBf16x3Ragged(p->dChan, p->dFirFwdRuns, p->nFirFwdRuns, x, taps, u, false, p->Tmax, p->err, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
    if (launchBankTables(p->dChan, p->C, coefs, p->totalStages, p->Smax, work + p->wTab, (double *) (work + p->wPhi),
                         s) != cudaSuccess ||
@@ -370,9 +384,9 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
    b.part = scratch + p->sPart;
    b.gcoefs = gcoefs;
    if (launchBankBackward(b, s) != cudaSuccess) return DSPLIB_ERR_FAILURE;
-   if (launchFirBf16x3Ragged(p->dChan, p->dFirDxRuns, p->nFirDxRuns, g, taps, gx, true, p->Tmax, s) != cudaSuccess)
+   if (launchFirBf16x3Ragged(p->dChan, p->dFirDxRuns, p->nFirDxRuns, g, taps, gx, true, p->Tmax, p->err, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
-   if (launchFirDhBf16x3Ragged(p->dChan, p->dDhRuns, p->nDhRuns, x, g, part, s) != cudaSuccess)
+   if (launchFirDhBf16x3Ragged(p->dChan, p->dDhRuns, p->nDhRuns, x, g, part, p->err, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
    fir_dh_reduce_kernel<<<p->C, 256, 0, s>>>(p->dChan, p->dDhStart, part, gtaps);
    countLaunch(1);
@@ -401,7 +415,7 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMse(DSPLIB_gpu_raggedPlan plan, co
    b.scale = (float) (2.0 / (double) p->totalOut);
    b.aggA = (float2 *) (scratch + p->sAgg);
    // forward, loss gradient and the adjoint's first pass in one sweep over the units
-   if (launchFirBf16x3Ragged(p->dChan, p->dFirFwdRuns, p->nFirFwdRuns, x, taps, work, false, p->Tmax, s) !=
+   if (launchFirBf16x3Ragged(p->dChan, p->dFirFwdRuns, p->nFirFwdRuns, x, taps, work, false, p->Tmax, p->err, s) !=
            cudaSuccess ||
        launchBankTables(p->dChan, p->C, coefs, p->totalStages, p->Smax, work + p->wTab, (double *) (work + p->wPhi),
                         s) != cudaSuccess ||
@@ -419,8 +433,8 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMse(DSPLIB_gpu_raggedPlan plan, co
    b.gcoefs = gcoefs;
    b.aggReady = true;
    if (launchBankBackward(b, s) != cudaSuccess ||
-       launchFirBf16x3Ragged(p->dChan, p->dFirDxRuns, p->nFirDxRuns, g, taps, gx, true, p->Tmax, s) != cudaSuccess ||
-       launchFirDhBf16x3Ragged(p->dChan, p->dDhRuns, p->nDhRuns, x, g, scratch + p->sDh, s) != cudaSuccess)
+       launchFirBf16x3Ragged(p->dChan, p->dFirDxRuns, p->nFirDxRuns, g, taps, gx, true, p->Tmax, p->err, s) != cudaSuccess ||
+       launchFirDhBf16x3Ragged(p->dChan, p->dDhRuns, p->nDhRuns, x, g, scratch + p->sDh, p->err, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
    fir_dh_reduce_kernel<<<p->C, 256, 0, s>>>(p->dChan, p->dDhStart, scratch + p->sDh, gtaps);
    countLaunch();

@@ -4,6 +4,8 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "dsplib_internal.h"
 
@@ -20,6 +22,101 @@ void setError(HandleCommon *h, const char *fmt, ...)
    va_start(ap, fmt);
    vsnprintf(h->err, sizeof(h->err), fmt, ap);
    va_end(ap);
+}
+
+// ---------------------------------------------------------------- error words
+
+namespace {
+constexpr int kErrWords = 4096;
+std::mutex g_errMutex;
+int *g_errPool = nullptr;  // mapped, portable page-locked words
+std::vector<int> g_errFree; // free slots
+int g_errNext = 1;          // slot 0 is shared by handles once the pool is exhausted
+
+bool errPool()
+{
+   if (g_errPool) return true;
+   void *p = nullptr;
+   if (cudaHostAlloc(&p, kErrWords * sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+      (void) cudaGetLastError();
+      return false;
+   }
+   std::memset(p, 0, kErrWords * sizeof(int));
+   g_errPool = (int *) p;
+   return true;
+}
+
+int takeSlot()
+{
+   if (!g_errFree.empty()) {
+      const int k = g_errFree.back();
+      g_errFree.pop_back();
+      return k;
+   }
+   return g_errNext < kErrWords ? g_errNext++ : 0;
+}
+} // namespace
+
+int *errorWord(HandleCommon *h)
+{
+   std::lock_guard<std::mutex> lock(g_errMutex);
+   if (!errPool()) return nullptr;
+   if (h->errSlot == 0) {
+      h->errSlot = 1 + takeSlot();
+      g_errPool[h->errSlot - 1] = 0;
+   }
+   return g_errPool + (h->errSlot - 1);
+}
+
+void releaseErrorWord(HandleCommon *h)
+{
+   std::lock_guard<std::mutex> lock(g_errMutex);
+   if (h->errSlot > 1) g_errFree.push_back(h->errSlot - 1);
+   h->errSlot = 0;
+}
+
+int takeErrorWord(HandleCommon *h)
+{
+   if (h->errSlot == 0 || !g_errPool) return 0;
+   volatile int *w = g_errPool + (h->errSlot - 1);
+   const int v = *w;
+   if (v) *w = 0;
+   return v;
+}
+
+int *allocErrorWord()
+{
+   std::lock_guard<std::mutex> lock(g_errMutex);
+   if (!errPool()) return nullptr;
+   const int k = takeSlot();
+   g_errPool[k] = 0;
+   return g_errPool + k;
+}
+
+void freeErrorWord(int *w)
+{
+   std::lock_guard<std::mutex> lock(g_errMutex);
+   if (w && g_errPool && w > g_errPool && w < g_errPool + kErrWords) g_errFree.push_back((int) (w - g_errPool));
+}
+
+// ---------------------------------------------------------------- fault injection
+
+namespace {
+thread_local int t_injectLeft = 0;
+}
+
+void injectArm(HandleCommon *h)
+{
+   t_injectLeft = h ? h->injectAt : 0;
+   if (h) h->injectAt = 0; // one call
+}
+
+void injectDisarm() { t_injectLeft = 0; }
+
+cudaError_t injectCheck(cudaError_t e)
+{
+   if (e != cudaSuccess || t_injectLeft <= 0) return e;
+   return --t_injectLeft == 0 ? cudaErrorUnknown : cudaSuccess;
 }
 
 // Wait for what is already queued on s (copies into or out of the caller's host
@@ -286,8 +383,29 @@ DSPLIB_STATUS DSPLIB_gpu_releaseHandle(DSPLIB_kernelHandle handle)
    if (!c) return DSPLIB_ERR_NULL_POINTER;
    // Work queued by an asynchronous exec may still read buffers the caller is about to free.
    const cudaError_t e = c->async ? cudaStreamSynchronize(c->stream) : cudaSuccess;
+   releaseErrorWord(c);
    c->magic = 0;
    return e == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
+}
+
+DSPLIB_STATUS DSPLIB_gpu_status(DSPLIB_kernelHandle handle)
+{
+   HandleCommon *c = common(handle);
+   if (!c) return DSPLIB_ERR_NULL_POINTER;
+   if (takeErrorWord(c) != 0) {
+      setError(c, "a bounded wait for the tensor core expired in an earlier call; its outputs are incomplete");
+      return DSPLIB_ERR_FAILURE;
+   }
+   return DSPLIB_SUCCESS;
+}
+
+DSPLIB_STATUS DSPLIB_gpu_injectFault(DSPLIB_kernelHandle handle, int32_t operation)
+{
+   HandleCommon *c = common(handle);
+   if (!c) return DSPLIB_ERR_NULL_POINTER;
+   if (operation < 0) return DSPLIB_ERR_INVALID_VALUE;
+   c->injectAt = operation;
+   return DSPLIB_SUCCESS;
 }
 
 } // extern "C"

@@ -53,6 +53,20 @@ DSPLIB_STATUS DSPLIB_gpu_firSetPrecision(DSPLIB_kernelHandle handle, int32_t pre
  *      accumulator and InitArgs.shift (shift = 0: saturate(acc)). */
 DSPLIB_STATUS DSPLIB_gpu_firSetQMode(DSPLIB_kernelHandle handle, int32_t enable);
 
+/** After asynchronous calls on this handle (DSPLIB_gpu_setAsync) and a synchronisation of
+ *  its stream: DSPLIB_ERR_FAILURE (reason in DSPLIB_gpu_lastError) if a bounded wait of a
+ *  tensor-core kernel expired in any of them since the last check, else DSPLIB_SUCCESS.
+ *  Synchronous calls check this themselves.  Each handle has its own error word (in
+ *  page-locked host memory shared by the library's handles; DSPLIB_gpu_releaseHandle
+ *  returns it). */
+DSPLIB_STATUS DSPLIB_gpu_status(DSPLIB_kernelHandle handle);
+
+/** Testing hook: the n-th CUDA operation (staging copy, kernel launch or pipeline block
+ *  copy) that the next exec on this handle queues reports a failure after it was queued,
+ *  so the call takes its error path (DSPLIB_ERR_FAILURE, reason in DSPLIB_gpu_lastError,
+ *  work already queued drained before returning).  Applies to one exec; 0 disables. */
+DSPLIB_STATUS DSPLIB_gpu_injectFault(DSPLIB_kernelHandle handle, int32_t operation);
+
 /** Number of CUDA kernels this library has launched in this process. */
 int64_t DSPLIB_gpu_kernelLaunchCount(void);
 
@@ -166,6 +180,11 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMse(DSPLIB_gpu_raggedPlan plan, co
                                                   const float *coefs, const float *target, float *y, float *gy,
                                                   float *loss, float *gx, float *gtaps, float *gcoefs, float *work,
                                                   float *scratch, void *stream);
+
+/** After the calls queued on this plan were synchronised: DSPLIB_ERR_FAILURE if a bounded
+ *  wait of one of its tensor-core kernels expired since the last check (the outputs of
+ *  that call are incomplete), else DSPLIB_SUCCESS; the check clears the plan's word. */
+DSPLIB_STATUS DSPLIB_gpu_raggedPlanStatus(DSPLIB_gpu_raggedPlan plan);
 
 /** Size, in floats, of the scratch array built into the library for
  *  DSPLIB_gpu_firBiquadBatched_bwdStaticScratch (16 MiB per device). */

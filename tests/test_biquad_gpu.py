@@ -457,3 +457,33 @@ def test_opt_async_level2_pinned_calls_overlap():
         stream.synchronize()
         assert np.array_equal(hy.numpy(), want)
         assert np.array_equal(hs.numpy(), st_want)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("nch", [0, 1])
+def test_get_coefficients_on_device_buffers_matches_host(form, nch):
+    """get_coefficients with device buffers runs the transform on the GPU: bit for bit the
+    host function's result (TIF transform with its 7-stage group gains, per-channel
+    reorder), the padding between channel columns left untouched."""
+    import ctypes
+
+    from c7x_dsplib_b200 import BufParams2D, bp, lib
+
+    if form != D.TIF and not nch:
+        pytest.skip("DF forms with shared coefficients have no optimized layout (INVALID_VALUE)")
+    rng = np.random.default_rng(70 + form * 2 + nch)
+    for S, C in [(1, 1), (4, 33), (7, 5), (8, 17), (15, 3), (22, 40)]:
+        nat = stable_sections(rng, C if nch else 1, S)
+        nat[0, 0] = 0.0  # b0 = 0: the reciprocal is taken as 0
+        want, popt = D.opt_coefficients(nat, form, nch, C)
+        pcn = bp(D.FLOAT32, S * 5, C if nch else 1, S * 5 * 4)
+        opt_d = torch.full((popt.dim_y * popt.stride_y // 4,), 3.0, device="cuda")
+        st = lib().DSPLIB_cascadeBiquad_get_coefficients(form, int(nch), ctypes.byref(pcn), ctypes.byref(popt),
+                                                         dev(nat).data_ptr(), opt_d.data_ptr())
+        assert st == D.SUCCESS
+        got = host(opt_d)
+        if nch:  # columns beyond C keep what the caller had there
+            got2 = got.reshape(popt.dim_y, popt.stride_y // 4)
+            assert np.all(got2[:, C:] == 3.0)
+            got2[:, C:] = want.reshape(popt.dim_y, -1)[:, C:]
+        assert np.array_equal(got, want), (S, C)
