@@ -92,3 +92,115 @@ def q15tofl(x: torch.Tensor, dtype: torch.dtype) -> torch.Tensor:
 @q15tofl.register_fake
 def _(x, dtype):
     return x.new_empty(x.numel(), dtype=dtype)
+
+
+# ---------------------------------------------------------------- autograd
+
+def _fir_setup(ctx, inputs, output):
+    x, h, nch, precision, qmode, shift = inputs
+    ctx.save_for_backward(x, h)
+    ctx.nch = nch
+
+
+def _fir_backward(ctx, gy):
+    """y[l, j] = sum_c x[l, j + c] h[T - 1 - c]  (FLOAT32 only):
+    dx = FIR of gy zero-padded by T - 1 on both sides with the taps flipped (a full
+    convolution with the taps), dh[T - 1 - c] = sum_j gy[j] x[j + c], the FIR of x
+    with each channel's flipped gradient as its taps.  Both on the library's kernels."""
+    x, h = ctx.saved_tensors
+    if x.dtype != torch.float32:
+        raise RuntimeError("dsplib_gpu::fir is differentiable for FLOAT32 only")
+    T = h.shape[1]
+    gy = gy.contiguous()
+    gx = gh = None
+    if ctx.needs_input_grad[0]:
+        pad = torch.nn.functional.pad(gy, (T - 1, T - 1))
+        hf = torch.flip(h, dims=[1]).contiguous()
+        gx = torch.ops.dsplib_gpu.fir(pad, hf, bool(ctx.nch), 0, False, 0)
+    if ctx.needs_input_grad[1]:
+        lag = torch.ops.dsplib_gpu.fir(x.contiguous(), torch.flip(gy, dims=[1]).contiguous(), True, 0, False, 0)
+        gh = torch.flip(lag, dims=[1])
+        if not ctx.nch:
+            gh = gh.sum(dim=0, keepdim=True)
+    return gx, gh, None, None, None, None
+
+
+fir.register_autograd(_fir_backward, setup_context=_fir_setup)
+
+
+_PLANS = {}
+
+
+def _bank_plan(C, N, S, device):
+    """A filter-bank plan of C channels of N samples, one tap, S stages: the cascade alone."""
+    from .filterbank import RaggedFilterBank
+
+    key = (C, N, S, str(device))
+    if key not in _PLANS:
+        _PLANS[key] = RaggedFilterBank([N] * C, [1] * C, [S] * C, device=device)
+    return _PLANS[key]
+
+
+@torch.library.custom_op(f"{_LIB}::cascade_biquad_natural", mutates_args=())
+def cascade_biquad_natural(x: torch.Tensor, coef: torch.Tensor, form: int) -> torch.Tensor:
+    """Differentiable DSPLIB_cascadeBiquad (OPTIMIZED) from a zero state over time-major
+    x [N, C] (FLOAT32) with natural coefficients coef [1 or C, 5 S] ([b0 b1 b2 a1 a2] per
+    stage); the optimized buffer comes from DSPLIB_cascadeBiquad_get_coefficients on the
+    device.  Gradients w.r.t. x and coef (every form has the transfer function of the
+    natural coefficients; the adjoint is the filter-bank adjoint)."""
+    _cuda(x, coef)
+    x, coef = x.contiguous(), coef.contiguous()
+    N, C = x.shape
+    S = coef.shape[1] // 5
+    nch = coef.shape[0] > 1
+    nv = 4 if form == D.DF1 else 2
+    state = torch.zeros((S * nv, C), device=x.device)
+    if form == D.TIF or nch:
+        import ctypes
+
+        args, pin, pout, pvar, pcn, popt = D.biquad_descs(C, N, S, form, nch)
+        opt = torch.zeros(popt.dim_y * popt.stride_y // 4, device=x.device)
+        st = D.lib().DSPLIB_cascadeBiquad_get_coefficients(form, int(nch), ctypes.byref(pcn), ctypes.byref(popt),
+                                                           coef.data_ptr(), opt.data_ptr())
+        if st != D.SUCCESS:
+            raise D.DsplibError("DSPLIB_cascadeBiquad_get_coefficients", st)
+    else:
+        opt = coef
+    out = torch.empty_like(x)
+    D.cascade_biquad(x, opt, state, form=form, nch=nch, out=out, stream=torch.cuda.current_stream())
+    return out
+
+
+@cascade_biquad_natural.register_fake
+def _(x, coef, form):
+    return torch.empty_like(x)
+
+
+def _bq_setup(ctx, inputs, output):
+    x, coef, form = inputs
+    ctx.save_for_backward(x, coef)
+
+
+def _bq_backward(ctx, gy):
+    x, coef = ctx.saved_tensors
+    N, C = x.shape
+    S = coef.shape[1] // 5
+    bank = _bank_plan(C, N, S, x.device)
+    coefs = (coef if coef.shape[0] == C else coef.expand(C, -1)).contiguous().view(-1)
+    xp = x.t().contiguous().view(-1)
+    taps = torch.ones(C, device=x.device)
+    y = torch.empty(bank.sizes[0], device=x.device)
+    work = torch.empty(bank.sizes[3], device=x.device)
+    bank.forward_raw(xp, taps, coefs, y, work)
+    gx = torch.empty_like(xp)
+    gt = torch.empty_like(taps)
+    gc = torch.empty_like(coefs)
+    scratch = torch.empty(bank.sizes[4], device=x.device)
+    bank.backward_raw(xp, taps, coefs, work, gy.t().contiguous().view(-1), gx, gt, gc, scratch)
+    gc = gc.view(C, 5 * S)
+    if coef.shape[0] == 1:
+        gc = gc.sum(dim=0, keepdim=True)
+    return gx.view(C, N).t().contiguous(), gc, None
+
+
+cascade_biquad_natural.register_autograd(_bq_backward, setup_context=_bq_setup)

@@ -77,3 +77,60 @@ def test_ops_capture_in_cuda_graph():
     torch.cuda.synchronize()
     assert torch.allclose(yg, 2.0 * y0, rtol=1e-5, atol=1e-5)
     del D
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nch", [False, True])
+def test_fir_operator_gradients_match_fp64(nch):
+    """dx and dh of torch.ops.dsplib_gpu.fir (FLOAT32) against float64 autograd of the same
+    correlation (y[j] = sum_c x[j + c] h[T - 1 - c])."""
+    import c7x_dsplib_b200.torch_ops  # noqa: F401
+
+    g = torch.Generator().manual_seed(5)
+    B, N, T = 3, 400, 23
+    x = torch.randn(B, N, generator=g)
+    h = torch.randn(B if nch else 1, T, generator=g) / 5
+    w = torch.randn(B, N - T + 1, generator=g)
+    xd, hd = x.cuda().requires_grad_(), h.cuda().requires_grad_()
+    (torch.ops.dsplib_gpu.fir(xd, hd, nch, 0, False, 0) * w.cuda()).sum().backward()
+    x64, h64 = x.double().requires_grad_(), h.double().requires_grad_()
+    hh = h64 if nch else h64.expand(B, T)
+    y64 = torch.stack([torch.nn.functional.conv1d(x64[l].view(1, 1, -1), hh[l].flip(0).view(1, 1, -1)).view(-1)
+                       for l in range(B)])
+    (y64 * w.double()).sum().backward()
+    for got, want in ((xd.grad, x64.grad), (hd.grad, h64.grad)):
+        err = (got.double().cpu() - want).abs().max() / want.abs().max()
+        assert err <= 1e-5, float(err)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", [0, 1, 2, 3])
+@pytest.mark.parametrize("nch", [False, True])
+def test_cascade_operator_gradients_match_fp64(form, nch):
+    """torch.ops.dsplib_gpu.cascade_biquad_natural: output and the gradients w.r.t. the
+    input and the natural coefficients against the FP64 restatement of the adjoint."""
+    import c7x_dsplib_b200.torch_ops  # noqa: F401
+    from oracle.filterbank64 import channel_adjoint, channel_forward, stable_sections
+
+    rng = np.random.default_rng(30 + form + 4 * nch)
+    N, C, S = 3000, 6, 3
+    x = rng.standard_normal((N, C)).astype(np.float32)
+    rows = C if nch else 1
+    nat = np.stack([stable_sections(rng, S).reshape(-1) for _ in range(rows)]).astype(np.float32)
+    gy = rng.standard_normal((N, C)).astype(np.float32)
+    xd = torch.from_numpy(x).cuda().requires_grad_()
+    cd = torch.from_numpy(nat).cuda().requires_grad_()
+    y = torch.ops.dsplib_gpu.cascade_biquad_natural(xd, cd, form)
+    (y * torch.from_numpy(gy).cuda()).sum().backward()
+    gc64 = np.zeros((C, 5 * S))
+    for ch in range(C):
+        c64 = nat[ch if nch else 0].astype(np.float64)
+        y64, _ = channel_forward(x[:, ch].astype(np.float64), np.ones(1), c64)
+        assert np.abs(y.detach().cpu().numpy()[:, ch] - y64).max() <= 1e-4 * np.abs(y64).max()
+        gx64, _, gcc = channel_adjoint(x[:, ch].astype(np.float64), np.ones(1), c64, gy[:, ch].astype(np.float64))
+        got = xd.grad.cpu().numpy()[:, ch]
+        assert np.abs(got - gx64).max() <= 1e-4 * np.abs(gx64).max()
+        gc64[ch] = gcc.reshape(-1)
+    want = gc64 if nch else gc64.sum(axis=0, keepdims=True)
+    got = cd.grad.cpu().numpy()
+    assert np.abs(got - want).max() <= 1e-4 * np.abs(want).max()
