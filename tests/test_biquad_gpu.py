@@ -487,3 +487,44 @@ def test_get_coefficients_on_device_buffers_matches_host(form, nch):
             assert np.all(got2[:, C:] == 3.0)
             got2[:, C:] = want.reshape(popt.dim_y, -1)[:, C:]
         assert np.array_equal(got, want), (S, C)
+
+
+def sections_at_radius(rng, rows, S, r):
+    """Natural [rows, S*5]: every pole pair at radius r (angle U[0.05, pi - 0.05]), zeros on
+    the unit circle, each section scaled to unit gain at its pole angle."""
+    out = np.zeros((rows, S, 5))
+    for r_ in range(rows):
+        for s in range(S):
+            th, ph = rng.uniform(0.05, np.pi - 0.05), rng.uniform(0, np.pi)
+            b = np.array([1.0, -2 * np.cos(ph), 1.0])
+            a = np.array([1.0, -2 * r * np.cos(th), r * r])
+            z = np.exp(-1j * th * np.arange(3))
+            g = 1.0 / max(abs(np.dot(b, z) / np.dot(a, z)), 1e-12)
+            out[r_, s] = [g * b[0], g * b[1], g * b[2], a[1], a[2]]
+    return out.reshape(rows, S * 5).astype(np.float32)
+
+
+@pytest.mark.parametrize("radius", [0.99, 0.995, 0.999])
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("C", [4, 64])
+def test_opt_scan_poles_near_unit_circle(radius, form, C):
+    """Poles at radius 0.99 / 0.995 / 0.999, where the transition powers are formed in FP64:
+    the per-channel scan (4 channels) and the lane scan (64 channels, clustered CTAs) over
+    signals of several windows, outputs and final states against FP64.  Bound: the one of
+    check_accuracy (1e-4, or 4x the sequential FP32 recursion's own error, which grows like
+    1 / (1 - r) here)."""
+    rng = np.random.default_rng(int(radius * 1e4) + form * 10 + C)
+    N, S = 20000, 3
+    x = rng.standard_normal((N, C)).astype(np.float32)
+    nat = sections_at_radius(rng, 1, S, radius)
+    st = np.zeros((S * nv(form), C), np.float32)
+    opt, _ = D.opt_coefficients(nat, form, 0, C)
+    sd = dev(st)
+    y = host(D.cascade_biquad(dev(x), dev(opt), sd, form=form, nch=0))
+    y32, st32, y64, s64 = oracle_run(form, x, nat, st, 0)
+    check_accuracy(y, y32, y64, (radius, form, C))
+    if form != D.TIF:  # TIF keeps its own state variables (no FP64 counterpart)
+        sgot = host(sd).astype(np.float64)
+        seq = np.abs(st32 - s64).max() / max(np.abs(s64).max(), 1e-30)
+        err = np.abs(sgot - s64).max() / max(np.abs(s64).max(), 1e-30)
+        assert err <= max(1e-4, 4 * seq), (err, seq)
