@@ -157,6 +157,7 @@ SIGNATURES = {
     "DSPLIB_gpu_firBiquadBatched_bwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_gpu_raggedMseGrad": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "DSPLIB_gpu_firBiquadBatched_stepMse": (ctypes.c_int, [_VP] * 14),
+    "DSPLIB_gpu_firBiquadBatched_stepMseHost": (ctypes.c_int, [_VP] * 12),
     "DSPLIB_gpu_firBiquadBatched_bwdStaticScratch": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                                                                     _VP]),
 }

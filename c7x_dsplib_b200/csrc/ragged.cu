@@ -67,6 +67,18 @@ struct RaggedPlan {
    long long wCk = 0, wAgg = 0, wTab = 0, wPhi = 0, wGrp = 0, wTotal = 0;
    // scratch layout (float offsets)
    long long sAgg = 0, sCk = 0, sGrp = 0, sPart = 0, sLoss = 0, sDh = 0, sTotal = 0;
+   // host-buffer steps: the channel table, and contiguous channel segments (each with a
+   // plan of its own) that are copied in, filtered and copied out as a pipeline
+   std::vector<int> hLen, hTaps, hStages;
+   struct Segment {
+      int c0, c1;            // channels [c0, c1)
+      long long x0, x1;      // samples
+      long long h0, h1;      // taps
+      long long k0, k1;      // coefficients
+      RaggedPlan *plan;
+   };
+   std::vector<Segment> segs;
+   long long segWork = 0, segScratch = 0; // largest work / scratch of one segment
 };
 
 namespace {
@@ -120,7 +132,10 @@ __global__ void __launch_bounds__(256) mse_partial_kernel(const RaggedChan *chan
    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
-__global__ void __launch_bounds__(1024) mse_reduce_kernel(const double *part, int n, double invCount, float *loss)
+// loss[0] = invCount * the sum of the partials (in a fixed order); with `sum`, the
+// FP64 sum itself goes to sum[0] instead (one segment of a host-buffer step).
+__global__ void __launch_bounds__(1024) mse_reduce_kernel(const double *part, int n, double invCount, float *loss,
+                                                          double *sum)
 {
    __shared__ double red[1024];
    double s = 0.0;
@@ -131,7 +146,20 @@ __global__ void __launch_bounds__(1024) mse_reduce_kernel(const double *part, in
       if ((int) threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
       __syncthreads();
    }
-   if (threadIdx.x == 0) loss[0] = (float) (red[0] * invCount);
+   if (threadIdx.x == 0) {
+      if (sum)
+         sum[0] = red[0];
+      else
+         loss[0] = (float) (red[0] * invCount);
+   }
+}
+
+// The segments' sums of squares, added in segment order.
+__global__ void mse_segments_kernel(const double *sums, int n, double invCount, float *loss)
+{
+   double s = 0.0;
+   for (int i = 0; i < n; i++) s += sums[i];
+   loss[0] = (float) (s * invCount);
 }
 
 template <typename T> cudaError_t upload(T **dst, const std::vector<T> &v)
@@ -155,6 +183,7 @@ static void freePlan(RaggedPlan *p)
    cudaFree(p->dDhRuns);
    cudaFree(p->dUnits);
    freeErrorWord(p->err);
+   for (RaggedPlan::Segment &g : p->segs) freePlan(g.plan);
    delete p;
 }
 
@@ -265,6 +294,9 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    p->nFirDxRuns = (int) firDx.size();
    p->nUnits = (int) units.size();
    p->nDhRuns = (int) dhRuns.size();
+   p->hLen.assign(length, length + numChannels);
+   p->hTaps.assign(taps, taps + numChannels);
+   p->hStages.assign(stages, stages + numChannels);
    cudaGetDevice(&p->device);
    p->err = allocErrorWord();
    // work buffer: u | forward checkpoints | forward aggregates | stage tables | unit transitions
@@ -393,26 +425,24 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
    return cudaGetLastError() == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
 }
 
-DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMse(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
-                                                  const float *coefs, const float *target, float *y, float *gy,
-                                                  float *loss, float *gx, float *gtaps, float *gcoefs, float *work,
-                                                  float *scratch, void *stream)
+} // extern "C"
+
+namespace dsplib {
+
+// The training step on device buffers: gy = scale (y - target); the loss goes to
+// loss[0] (times invCount) or, with lossSum, as the plain FP64 sum to lossSum[0].
+static DSPLIB_STATUS stepMseCore(RaggedPlan *p, const float *x, const float *taps, const float *coefs,
+                                 const float *target, float *y, float *gy, float *loss, double *lossSum, float *gx,
+                                 float *gtaps, float *gcoefs, float *work, float *scratch, float scale,
+                                 double invCount, cudaStream_t s)
 {
-   RaggedPlan *p = (RaggedPlan *) plan;
-   if (!p || !x || !taps || ((!coefs || !gcoefs) && p->totalCoefs) || !target || !y || !gy || !loss || !gx ||
-       !gtaps || !work || !scratch)
-      return DSPLIB_ERR_NULL_POINTER;
-   if (p->totalOut <= 0) return DSPLIB_ERR_INVALID_DIMENSION;
-   PlanDevice dev(p);
-   if (!dev.ok()) return DSPLIB_ERR_FAILURE;
-   cudaStream_t s = (cudaStream_t) stream;
    float *g = scratch;
    BankLaunch b = bankLaunch(p, work);
    b.y = y;
    b.target = target;
    b.gyOut = gy;
    b.lossPart = (double *) (scratch + p->sLoss);
-   b.scale = (float) (2.0 / (double) p->totalOut);
+   b.scale = scale;
    b.aggA = (float2 *) (scratch + p->sAgg);
    // forward, loss gradient and the adjoint's first pass in one sweep over the units
    if (launchFirBf16x3Ragged(p->dChan, p->dFirFwdRuns, p->nFirFwdRuns, x, taps, work, false, p->Tmax, p->err, s) !=
@@ -421,7 +451,7 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMse(DSPLIB_gpu_raggedPlan plan, co
                         s) != cudaSuccess ||
        launchBankForward(b, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
-   mse_reduce_kernel<<<1, 1024, 0, s>>>(b.lossPart, p->nUnits, 1.0 / (double) p->totalOut, loss);
+   mse_reduce_kernel<<<1, 1024, 0, s>>>(b.lossPart, p->nUnits, invCount, loss, lossSum);
    countLaunch();
    // adjoint
    b.target = nullptr;
@@ -441,6 +471,180 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMse(DSPLIB_gpu_raggedPlan plan, co
    return cudaGetLastError() == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
 }
 
+// Input bytes (x and target) per segment of a host-buffer step.
+constexpr long long kStepSegmentBytes = 16LL << 20;
+
+// Split the channels into up to kPipeMaxBlocks contiguous segments of about equal
+// samples, each with a plan of its own (on the plan's device, which is current).
+static bool buildSegments(RaggedPlan *p)
+{
+   if (!p->segs.empty()) return true;
+   const long long bytes = 8LL * p->totalLen;
+   int G = (int) std::min<long long>(kPipeMaxBlocks, std::max<long long>(1, (bytes + kStepSegmentBytes - 1) /
+                                                                              kStepSegmentBytes));
+   G = std::min(G, p->C);
+   std::vector<RaggedPlan::Segment> segs;
+   long long x = 0, h = 0, k = 0;
+   int c = 0;
+   for (int g = 0; g < G; g++) {
+      RaggedPlan::Segment sg{};
+      sg.c0 = c;
+      sg.x0 = x;
+      sg.h0 = h;
+      sg.k0 = k;
+      const long long goal = p->totalLen * (g + 1) / G;
+      // at least one channel, and one left for each later segment
+      do {
+         x += p->hLen[c];
+         h += p->hTaps[c];
+         k += 5LL * p->hStages[c];
+         c++;
+      } while (c < p->C - (G - 1 - g) && x < goal);
+      if (g + 1 == G)
+         for (; c < p->C; c++) {
+            x += p->hLen[c];
+            h += p->hTaps[c];
+            k += 5LL * p->hStages[c];
+         }
+      sg.c1 = c;
+      sg.x1 = x;
+      sg.h1 = h;
+      sg.k1 = k;
+      DSPLIB_gpu_raggedPlan sub = nullptr;
+      if (DSPLIB_gpu_raggedPlanCreate(&sub, sg.c1 - sg.c0, &p->hLen[sg.c0], &p->hTaps[sg.c0], &p->hStages[sg.c0]) !=
+          DSPLIB_SUCCESS) {
+         for (RaggedPlan::Segment &o : segs) freePlan(o.plan);
+         return false;
+      }
+      sg.plan = (RaggedPlan *) sub;
+      segs.push_back(sg);
+   }
+   p->segWork = p->segScratch = 0;
+   for (const RaggedPlan::Segment &sg : segs) {
+      p->segWork = std::max(p->segWork, sg.plan->wTotal);
+      p->segScratch = std::max(p->segScratch, sg.plan->sTotal);
+   }
+   p->segs = std::move(segs);
+   return true;
+}
+
+// A device view of one array of a host-buffer step: the caller's pointer when it is
+// device memory, else a slice of the staging block.
+struct StepArray {
+   const void *host;
+   float *dev;
+   bool staged;
+};
+
+} // namespace dsplib
+
+extern "C" {
+
+DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMse(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
+                                                  const float *coefs, const float *target, float *y, float *gy,
+                                                  float *loss, float *gx, float *gtaps, float *gcoefs, float *work,
+                                                  float *scratch, void *stream)
+{
+   RaggedPlan *p = (RaggedPlan *) plan;
+   if (!p || !x || !taps || ((!coefs || !gcoefs) && p->totalCoefs) || !target || !y || !gy || !loss || !gx ||
+       !gtaps || !work || !scratch)
+      return DSPLIB_ERR_NULL_POINTER;
+   if (p->totalOut <= 0) return DSPLIB_ERR_INVALID_DIMENSION;
+   PlanDevice dev(p);
+   if (!dev.ok()) return DSPLIB_ERR_FAILURE;
+   return stepMseCore(p, x, taps, coefs, target, y, gy, loss, nullptr, gx, gtaps, gcoefs, work, scratch,
+                      (float) (2.0 / (double) p->totalOut), 1.0 / (double) p->totalOut, (cudaStream_t) stream);
+}
+
+DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMseHost(DSPLIB_gpu_raggedPlan plan, const float *x, const float *taps,
+                                                      const float *coefs, const float *target, float *y, float *gy,
+                                                      float *loss, float *gx, float *gtaps, float *gcoefs,
+                                                      void *stream)
+{
+   RaggedPlan *p = (RaggedPlan *) plan;
+   if (!p || !x || !taps || ((!coefs || !gcoefs) && p->totalCoefs) || !target || !y || !loss || !gx || !gtaps)
+      return DSPLIB_ERR_NULL_POINTER;
+   if (p->totalOut <= 0) return DSPLIB_ERR_INVALID_DIMENSION;
+   PlanDevice dev(p);
+   if (!dev.ok() || !buildSegments(p)) return DSPLIB_ERR_FAILURE;
+   PipeContext *pc = pipeContext();
+   if (!pc) return DSPLIB_ERR_FAILURE;
+   cudaStream_t s = (cudaStream_t) stream;
+   const int G = (int) p->segs.size();
+   const long long nx = align4(p->totalLen), nh = align4(p->totalTaps), nk = align4(p->totalCoefs);
+   // staging block: x | target | y | gy | gx | taps | gtaps | coefs | gcoefs | loss sums | loss
+   StepArray arr[9] = {{x, nullptr, false},      {target, nullptr, false}, {y, nullptr, false},
+                       {gy, nullptr, false},     {gx, nullptr, false},     {taps, nullptr, false},
+                       {gtaps, nullptr, false},  {coefs, nullptr, false},  {gcoefs, nullptr, false}};
+   const long long len[9] = {nx, nx, nx, nx, nx, nh, nh, nk, nk};
+   const long long stagedFloats = 5 * nx + 2 * nh + 2 * nk + 2 * kPipeMaxBlocks + 4;
+   float *blk = (float *) stagingBuffer(0, (size_t) stagedFloats * sizeof(float), s);
+   float *work = (float *) stagingBuffer(1, (size_t) p->segWork * sizeof(float), s);
+   float *scratch = (float *) stagingBuffer(2, (size_t) p->segScratch * sizeof(float), s);
+   if (!blk || !work || !scratch) return DSPLIB_ERR_FAILURE;
+   long long off = 0;
+   for (int i = 0; i < 9; i++) {
+      arr[i].staged = arr[i].host == nullptr || !isDevicePtr(arr[i].host);
+      arr[i].dev = arr[i].staged ? blk + off : (float *) arr[i].host;
+      off += len[i];
+   }
+   double *sums = (double *) (blk + off);
+   float *lossDev = blk + off + 2 * kPipeMaxBlocks;
+   const bool lossStaged = !isDevicePtr(loss);
+   if (!lossStaged) lossDev = loss;
+   auto h2d = [&](const StepArray &a, long long o, long long n) {
+      if (!a.staged || n == 0) return cudaSuccess;
+      return cudaMemcpyAsync(a.dev + o, (const float *) a.host + o, n * sizeof(float), cudaMemcpyHostToDevice, pc->in);
+   };
+   auto d2h = [&](const StepArray &a, long long o, long long n) {
+      if (!a.staged || !a.host || n == 0) return cudaSuccess;
+      return cudaMemcpyAsync((float *) a.host + o, a.dev + o, n * sizeof(float), cudaMemcpyDeviceToHost, pc->out);
+   };
+   cudaError_t e = cudaEventRecord(pc->start, s);
+   if (e == cudaSuccess) e = cudaStreamWaitEvent(pc->in, pc->start, 0);
+   if (e == cudaSuccess) e = cudaStreamWaitEvent(pc->comp, pc->start, 0);
+   if (e == cudaSuccess) e = cudaStreamWaitEvent(pc->out, pc->start, 0);
+   if (e != cudaSuccess) return pipeFail(nullptr, pc, e, "pipeline start");
+   const float scale = (float) (2.0 / (double) p->totalOut);
+   for (int g = 0; g < G; g++) {
+      const RaggedPlan::Segment &sg = p->segs[g];
+      const long long xo = sg.x0, xn = sg.x1 - sg.x0, ho = sg.h0, hn = sg.h1 - sg.h0, ko = sg.k0, kn = sg.k1 - sg.k0;
+      if ((e = h2d(arr[0], xo, xn)) != cudaSuccess || (e = h2d(arr[1], xo, xn)) != cudaSuccess ||
+          (e = h2d(arr[5], ho, hn)) != cudaSuccess || (e = h2d(arr[7], ko, kn)) != cudaSuccess ||
+          (e = cudaEventRecord(pc->copied[g], pc->in)) != cudaSuccess ||
+          (e = cudaStreamWaitEvent(pc->comp, pc->copied[g], 0)) != cudaSuccess)
+         return pipeFail(nullptr, pc, e, "copy segment in");
+      float *gyDev = arr[3].dev + xo;
+      if (stepMseCore(sg.plan, arr[0].dev + xo, arr[5].dev + ho, arr[7].dev + ko, arr[1].dev + xo, arr[2].dev + xo,
+                      gyDev, nullptr, sums + g, arr[4].dev + xo, arr[6].dev + ho, arr[8].dev + ko, work, scratch,
+                      scale, 0.0, pc->comp) != DSPLIB_SUCCESS)
+         return pipeFail(nullptr, pc, cudaErrorLaunchFailure, "segment step");
+      if ((e = cudaEventRecord(pc->computed[g], pc->comp)) != cudaSuccess ||
+          (e = cudaStreamWaitEvent(pc->out, pc->computed[g], 0)) != cudaSuccess ||
+          (e = d2h(arr[2], xo, xn)) != cudaSuccess || (e = d2h(arr[3], xo, xn)) != cudaSuccess ||
+          (e = d2h(arr[4], xo, xn)) != cudaSuccess || (e = d2h(arr[6], ho, hn)) != cudaSuccess ||
+          (e = d2h(arr[8], ko, kn)) != cudaSuccess)
+         return pipeFail(nullptr, pc, e, "copy segment out");
+   }
+   mse_segments_kernel<<<1, 1, 0, pc->comp>>>(sums, G, 1.0 / (double) p->totalOut, lossDev);
+   countLaunch();
+   if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaEventRecord(pc->done, pc->comp)) != cudaSuccess ||
+       (e = cudaStreamWaitEvent(pc->out, pc->done, 0)) != cudaSuccess)
+      return pipeFail(nullptr, pc, e, "loss");
+   if (lossStaged && (e = cudaMemcpyAsync(loss, lossDev, sizeof(float), cudaMemcpyDeviceToHost, pc->out)) != cudaSuccess)
+      return pipeFail(nullptr, pc, e, "copy loss");
+   if ((e = cudaEventRecord(pc->done, pc->out)) != cudaSuccess || (e = cudaStreamWaitEvent(s, pc->done, 0)) != cudaSuccess ||
+       (e = cudaStreamSynchronize(s)) != cudaSuccess)
+      return pipeFail(nullptr, pc, e, "pipeline join");
+   bool expired = false;
+   for (const RaggedPlan::Segment &sg : p->segs)
+      if (sg.plan->err && *(volatile int *) sg.plan->err != 0) {
+         *(volatile int *) sg.plan->err = 0;
+         expired = true;
+      }
+   return expired ? DSPLIB_ERR_FAILURE : DSPLIB_SUCCESS;
+}
+
 DSPLIB_STATUS DSPLIB_gpu_raggedMseGrad(DSPLIB_gpu_raggedPlan plan, const float *y, const float *target, float *gy,
                                        float *loss, float *scratch, void *stream)
 {
@@ -453,7 +657,7 @@ DSPLIB_STATUS DSPLIB_gpu_raggedMseGrad(DSPLIB_gpu_raggedPlan plan, const float *
    double *part = (double *) (scratch + p->sDh);
    mse_partial_kernel<<<p->nFwdItems, 256, 0, s>>>(p->dChan, p->dFwdItems, y, target, gy, part,
                                                    (float) (2.0 / (double) p->totalOut));
-   mse_reduce_kernel<<<1, 1024, 0, s>>>(part, p->nFwdItems, 1.0 / (double) p->totalOut, loss);
+   mse_reduce_kernel<<<1, 1024, 0, s>>>(part, p->nFwdItems, 1.0 / (double) p->totalOut, loss, nullptr);
    countLaunch(2);
    return cudaGetLastError() == cudaSuccess ? DSPLIB_SUCCESS : DSPLIB_ERR_FAILURE;
 }

@@ -151,6 +151,31 @@ class RaggedFilterBank:
         if st != SUCCESS:
             raise DsplibError("DSPLIB_gpu_firBiquadBatched_stepMse", st)
 
+    def step_mse_host(self, x, taps, coefs, target, y, gy, loss, gx, gtaps, gcoefs):
+        """The training step on host tensors (DSPLIB_gpu_firBiquadBatched_stepMseHost):
+        inputs copied in and results copied out by the library, channel segments
+        pipelined over three streams; returns once the results are in host memory.
+        Page-locked tensors let the copies overlap; gy may be None."""
+        def check(t, n, name):
+            import torch
+
+            if not (t.dtype == torch.float32 and t.is_contiguous() and t.numel() == n):
+                raise ValueError(f"{name}: need a contiguous float32 tensor of {n} elements")
+
+        n, nh, nk = self.sizes[SAMPLES], self.sizes[TAPS], self.sizes[COEFS]
+        for t, m, name in ((x, n, "x"), (taps, nh, "taps"), (coefs, nk, "coefs"), (target, n, "target"),
+                           (y, n, "y"), (loss, 1, "loss"), (gx, n, "gx"), (gtaps, nh, "gtaps"),
+                           (gcoefs, nk, "gcoefs")):
+            check(t, m, name)
+        if gy is not None:
+            check(gy, n, "gy")
+        st = lib().DSPLIB_gpu_firBiquadBatched_stepMseHost(
+            self._plan, x.data_ptr(), taps.data_ptr(), coefs.data_ptr(), target.data_ptr(), y.data_ptr(),
+            None if gy is None else gy.data_ptr(), loss.data_ptr(), gx.data_ptr(), gtaps.data_ptr(),
+            gcoefs.data_ptr(), _stream_ptr())
+        if st != SUCCESS:
+            raise DsplibError("DSPLIB_gpu_firBiquadBatched_stepMseHost", st)
+
     # ---------------------------------------------------------------- autograd
     def apply(self, x, taps, coefs):
         """Differentiable y = filterbank(x; taps, coefs) on packed tensors."""

@@ -368,3 +368,48 @@ def test_fused_step_equals_separate_calls():
     for k in ("y", "gy", "gx", "gtaps", "gcoefs"):
         assert torch.equal(fus[k], sep[k]), k
     assert float(fus["loss"]) == pytest.approx(float(sep["loss"]), rel=1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pinned", [True, False])
+def test_host_step_equals_device_step(pinned):
+    """DSPLIB_gpu_firBiquadBatched_stepMseHost on host tensors (several pipelined channel
+    segments: 7.3 M samples at 2 M samples per segment) against the device call:
+    y, gy and every gradient bitwise equal, the loss to FP64 summation order; twice in a
+    row, then with gy omitted and the taps / coefficients left on the device."""
+    import torch
+
+    from c7x_dsplib_b200.filterbank import RaggedFilterBank
+
+    lengths, taps, stages, x, h, c = _bank_case(21, 60, Lrange=(1000, 240000), Tmax=300, Smax=8,
+                                                force=[(262144, 512, 8), (300, 300, 0)])
+    bank = RaggedFilterBank(lengths, taps, stages)
+    assert bank.sizes[0] > 6_000_000
+    dev = "cuda"
+    xt, ht, ct = (torch.tensor(a, dtype=torch.float32, device=dev) for a in (x, h, c))
+    target = torch.randn(bank.sizes[0], device=dev, generator=torch.Generator(dev).manual_seed(5))
+    n = bank.sizes[0]
+    ref = {k: torch.empty(n, device=dev) for k in ("y", "gy", "gx")}
+    ref["gtaps"], ref["gcoefs"], ref["loss"] = torch.empty_like(ht), torch.empty_like(ct), torch.empty(1, device=dev)
+    bank.step_mse_raw(xt, ht, ct, target, ref["y"], ref["gy"], ref["loss"], ref["gx"], ref["gtaps"], ref["gcoefs"],
+                      torch.empty(bank.sizes[3], device=dev), torch.empty(bank.sizes[4], device=dev))
+    torch.cuda.synchronize()
+    ref = {k: v.cpu() for k, v in ref.items()}
+
+    def host(t):
+        t = t.cpu()
+        return t.pin_memory() if pinned else t.clone()
+
+    hx, hh, hc, ht_ = host(xt), host(ht), host(ct), host(target)
+    for rep in range(3):
+        out = {k: host(torch.full_like(v, 7.0)) for k, v in ref.items()}
+        taps_in, coefs_in, gy_out = (hh, hc, out["gy"]) if rep < 2 else (ht, ct, None)
+        if rep == 2:
+            out["gtaps"], out["gcoefs"] = torch.full_like(ht, 7.0), torch.full_like(ct, 7.0)
+        bank.step_mse_host(hx, taps_in, coefs_in, ht_, out["y"], gy_out, out["loss"], out["gx"], out["gtaps"],
+                           out["gcoefs"])
+        for k in ("y", "gy", "gx", "gtaps", "gcoefs"):
+            if k == "gy" and gy_out is None:
+                continue
+            assert torch.equal(out[k].cpu(), ref[k]), (rep, k)
+        assert float(out["loss"]) == pytest.approx(float(ref["loss"]), rel=1e-6)
