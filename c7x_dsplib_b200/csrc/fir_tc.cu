@@ -503,7 +503,7 @@ __host__ __device__ constexpr int bfK(int T) { return ((63 + T + 15) / 16) * 16;
 __host__ __device__ constexpr int bfBlocks(int T) { return kRows + (bfK(T) + 63) / 64; }
 // 16-byte plane chunks staged per thread by bfStage
 constexpr int kBfChunksPerThread = (bfBlocks(kBfMaxTaps) * 8 + kBfThreads - 1) / kBfThreads;
-__host__ __device__ inline int bfTapSlots(int T) { return kBfPadLeft + bfK(T) + 8; }
+__host__ __device__ constexpr int bfTapSlots(int T) { return kBfPadLeft + bfK(T) + 8; }
 
 __device__ __forceinline__ void splitBf16(float v, uint16_t &hi, uint16_t &lo)
 {
@@ -600,30 +600,51 @@ struct BfRun {
    int *err; // error word for an expired bounded wait
 };
 
-// Shared memory for taps up to Tmax: the hi/lo signal planes of the current
-// tile (also the output staging area once its MMAs completed), a ring of raw
-// FP32 tiles in flight (two when they fit beside the band, else one), the taps
-// band and the split taps.
+// Shared memory for taps up to Tmax: two sets of hi/lo signal planes (tile t is
+// split into set t % 2 while the tensor core reads the other; a drained tile's set
+// also stages its output), a ring of raw FP32 tiles fetched by the TMA engine ahead
+// of their split (up to two when they fit beside the band, none for the longest
+// taps: those tiles are staged by the threads straight from global memory), the
+// taps band and the split taps.  Two accumulators of 128 TMEM columns each.
+//
+// Warp roles: warps 0-15 (the workers) build the band, split tiles into the planes
+// and drain the accumulators; warp 16 issues the MMAs.  The issuing thread may stall
+// in tcgen05.mma while the tensor core is busy, so it has a warp of its own.
+// Handshakes: planesFull[b] (a worker arrives once plane set b holds a tile and
+// accumulator b is free) and mmaDone[b] (tcgen05.commit once the MMAs reading set b
+// and writing accumulator b completed); the workers synchronise among themselves on
+// named barrier 1.
 constexpr size_t kBfSmemLimit = 227 * 1024;
-__host__ __device__ inline size_t bfPlaneBytes(int Tmax) { return (size_t) ((bfBlocks(Tmax) * 128 + 1023) & ~1023); }
-__host__ __device__ inline size_t bfRawBytes(int Tmax) { return (size_t) bfBlocks(Tmax) * 256; }
-__host__ __device__ inline size_t bfSmemBytesFor(int Tmax, int stages)
+constexpr uint32_t kBfTmemCols = 256;
+constexpr int kBfWorkers = kBfThreads;         // worker threads (16 warps)
+constexpr int kBfBlock = kBfWorkers + 32;      // + the MMA warp
+constexpr uint32_t kBfBar = 1;                 // the workers' named barrier
+__host__ __device__ constexpr size_t bfPlaneBytes(int Tmax) { return (size_t) ((bfBlocks(Tmax) * 128 + 1023) & ~1023); }
+__host__ __device__ constexpr size_t bfRawBytes(int Tmax) { return (size_t) bfBlocks(Tmax) * 256; }
+__host__ __device__ constexpr size_t bfSmemBytesFor(int Tmax, int stages)
 {
-   return 1024 + 2 * bfPlaneBytes(Tmax) + stages * bfRawBytes(Tmax) + (size_t) bfK(Tmax) * 256 +
-          4 * (size_t) bfTapSlots(Tmax) + 64;
+   return 1024 + 4 * bfPlaneBytes(Tmax) + stages * bfRawBytes(Tmax) + (size_t) bfK(Tmax) * 256 +
+          4 * (size_t) bfTapSlots(Tmax) + 128;
 }
-__host__ __device__ inline int bfStages(int Tmax) { return bfSmemBytesFor(Tmax, 2) <= kBfSmemLimit ? 2 : 1; }
+__host__ __device__ inline int bfStages(int Tmax)
+{
+   return bfSmemBytesFor(Tmax, 2) <= kBfSmemLimit ? 2 : (bfSmemBytesFor(Tmax, 1) <= kBfSmemLimit ? 1 : 0);
+}
 __host__ __device__ inline size_t bfSmemBytes(int Tmax) { return bfSmemBytesFor(Tmax, bfStages(Tmax)); }
+static_assert(bfSmemBytesFor(kBfMaxTaps, 0) <= kBfSmemLimit, "two plane sets and the longest band fit");
 
 struct BfSmem {
-   unsigned char *hi, *lo; // planes, each on a 1024-byte swizzle atom
-   float *raw;             // stages x bfBlocks(Tmax) * 64 floats
+   unsigned char *sets; // plane set b: hi at sets + 2 b planeBytes, lo planeBytes further (1024-byte aligned)
+   size_t planeBytes;
+   float *raw;          // stages x bfBlocks(Tmax) * 64 floats
    int rawFloats, stages;
    unsigned char *Bt;
    uint16_t *gHi, *gLo;
-   uint64_t *mbar, *full; // MMA completion; raw-tile arrival per stage
+   uint64_t *mbar, *planesFull, *full; // MMA completion and plane-set readiness per accumulator; raw tiles
    uint32_t *tslot;
    __device__ float *slot(int k) const { return raw + (size_t) k * rawFloats; }
+   __device__ unsigned char *hi(int b) const { return sets + (size_t) (2 * b) * planeBytes; }
+   __device__ unsigned char *lo(int b) const { return sets + (size_t) (2 * b + 1) * planeBytes; }
 };
 
 __device__ __forceinline__ BfSmem bfSmemLayout(unsigned char *smraw, int Tmax)
@@ -632,77 +653,92 @@ __device__ __forceinline__ BfSmem bfSmemLayout(unsigned char *smraw, int Tmax)
    unsigned char *sm = (unsigned char *) (((uintptr_t) smraw + 1023) & ~(uintptr_t) 1023);
    const size_t pb = bfPlaneBytes(Tmax);
    L.stages = bfStages(Tmax);
-   L.hi = sm;
-   L.lo = sm + pb;
-   L.raw = (float *) (sm + 2 * pb);
+   L.planeBytes = pb;
+   L.sets = sm;
+   L.raw = (float *) (sm + 4 * pb);
    L.rawFloats = bfBlocks(Tmax) * 64;
    L.Bt = (unsigned char *) L.raw + (size_t) L.stages * bfRawBytes(Tmax);
    L.gHi = (uint16_t *) (L.Bt + (size_t) bfK(Tmax) * 256); // split taps with zero padding
    L.gLo = L.gHi + bfTapSlots(Tmax);
    L.mbar = (uint64_t *) (((uintptr_t) (L.gLo + bfTapSlots(Tmax)) + 15) & ~(uintptr_t) 15);
-   L.full = L.mbar + 1;
+   L.planesFull = L.mbar + 2;
+   L.full = L.planesFull + 2;
    L.tslot = (uint32_t *) (L.full + 2);
    return L;
 }
 
-// Barrier phases and copies in flight, carried across the runs of one CTA.
+// The workers' barrier phases and copies in flight, carried across the runs of one CTA.
 struct BfPipe {
-   uint32_t iter = 0;    // MMA barrier phase
+   uint32_t tiles = 0;   // tiles split so far: tile n uses plane set and accumulator n % 2
+   uint32_t mmaPar = 0;  // mmaDone phase, one bit per accumulator
    uint32_t par = 0;     // raw-tile barrier phase, one bit per stage
    uint32_t pending = 0; // stages with a bulk copy issued and not yet waited for
 };
 
-// Drain the accumulator (the MMAs of output tile t) through the planes into y.
-// Returns false when the bounded wait gave up.
-__device__ __forceinline__ bool bfDrain(const BfRun &r, const BfSmem &L, uint32_t tmem, BfPipe &pp, int t, int tid)
+// The MMA thread's state.
+struct BfIssuer {
+   uint32_t tiles = 0;
+   uint32_t pfPar = 0;          // planesFull phase, one bit per accumulator
+   uint32_t commits0 = 0, commits1 = 0; // commits per accumulator
+};
+
+// Workers: wait for the MMAs of accumulator b (bounded; thread 0 waits, the barrier
+// releases the rest).
+__device__ __forceinline__ bool bfWaitMma(const BfSmem &L, BfPipe &pp, int b, int *err, int tid)
+{
+   const bool done = tid == 0 ? tc::mbarWait(L.mbar + b, (pp.mmaPar >> b) & 1) : true;
+   pp.mmaPar ^= 1u << b;
+   if (!done && tid == 0) raiseError(err);
+   return !tc::namedSyncOr(kBfBar, kBfWorkers, !done);
+}
+
+// Workers: drain accumulator b (output tile t of run r, its MMAs complete) through
+// plane set b into y.
+__device__ __forceinline__ void bfDrain(const BfRun &r, const BfSmem &L, uint32_t tmem, int b, int t, int tid)
 {
    const int warp = tid >> 5, lane = tid & 31;
-   const bool done = tid == 0 ? tc::mbarWait(L.mbar, pp.iter & 1) : true; // the barrier releases the rest
-   pp.iter++;
-   if (!done && tid == 0) raiseError(r.err);
-   if (__syncthreads_or(!done)) return false;
    tc::fenceAfterSync();
    const long long j0 = (long long) t * kBfTile;
+   unsigned char *stage = L.hi(b); // the set spans both planes: 2 * planeBytes >= 32 KB
    {
       // Warp w drains TMEM lane quadrant w % 4 (rows a) and output quarter qt = w / 4
       // (16 phases): y[j0 + 64a + 16*qt + b] = D[a][16*qt + b] + D[a][64 + 16*qt + b].
       const int quad = warp & 3, qt = warp >> 2, half = qt >> 1;
-      const uint32_t acc = tmem + ((uint32_t) (quad * 32) << 16);
+      const uint32_t acc = tmem + (uint32_t) b * 128 + ((uint32_t) (quad * 32) << 16);
       const int row = quad * 32 + lane;
-      uint32_t a[16], b[16];
+      uint32_t a[16], c[16];
       tc::tmemLoad16(acc + qt * 16, a);
-      tc::tmemLoad16(acc + 64 + qt * 16, b);
+      tc::tmemLoad16(acc + 64 + qt * 16, c);
       tc::tmemWaitLoad();
-      // The planes are free once the MMAs completed: they hold the output tile,
-      // 16-byte chunk v4 of row half (row, half) rotated to slot (v4 + row) & 7 so
-      // that eight consecutive rows store to distinct banks.
-      float *os = (float *) L.hi + row * kBfPhases + half * 32;
+      // 16-byte chunk v4 of row half (row, half) rotated to slot (v4 + row) & 7 so that
+      // eight consecutive rows store to distinct banks.
+      float *os = (float *) stage + row * kBfPhases + half * 32;
 #pragma unroll
       for (int v = 0; v < 4; v++) {
          const int v4 = (qt & 1) * 4 + v;
          float4 o;
-         o.x = __uint_as_float(a[4 * v + 0]) + __uint_as_float(b[4 * v + 0]);
-         o.y = __uint_as_float(a[4 * v + 1]) + __uint_as_float(b[4 * v + 1]);
-         o.z = __uint_as_float(a[4 * v + 2]) + __uint_as_float(b[4 * v + 2]);
-         o.w = __uint_as_float(a[4 * v + 3]) + __uint_as_float(b[4 * v + 3]);
+         o.x = __uint_as_float(a[4 * v + 0]) + __uint_as_float(c[4 * v + 0]);
+         o.y = __uint_as_float(a[4 * v + 1]) + __uint_as_float(c[4 * v + 1]);
+         o.z = __uint_as_float(a[4 * v + 2]) + __uint_as_float(c[4 * v + 2]);
+         o.w = __uint_as_float(a[4 * v + 3]) + __uint_as_float(c[4 * v + 3]);
          *(float4 *) (os + (((v4 + row) & 7) << 2)) = o;
       }
    }
    tc::fenceBeforeSync();
-   __syncthreads(); // the output tile is complete in shared memory; the accumulator is free
-   storeTile<float>(r.y + j0, (int) min((long long) kBfTile, (long long) r.outLen - j0),
-                    (const unsigned char *) L.hi,
+   tc::namedSync(kBfBar, kBfWorkers); // the output tile is complete in shared memory; the accumulator is free
+   storeTile<float>(r.y + j0, (int) min((long long) kBfTile, (long long) r.outLen - j0), (const unsigned char *) stage,
                     [](int ci) {
                        const int row = ci >> 4, half = (ci >> 3) & 1, v4 = ci & 7;
                        return (row * kBfPhases + half * 32 + (((v4 + row) & 7) << 2)) * 4;
                     },
-                    tid, kBfThreads);
-   return true;
+                    tid, kBfWorkers);
+   tc::namedSync(kBfBar, kBfWorkers); // the staged output has left plane set b: it may be split into again
 }
 
-// Build the taps band of run r, then stream its tiles through the tensor core.
+// Workers: build the taps band of run r, then split its tiles into alternate plane
+// sets (handing each to the MMA warp) and drain tile t - 1 while tile t's MMAs run.
 // Returns false when a bounded wait gave up.
-__device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint32_t tmem, BfPipe &pp, int tid)
+__device__ __forceinline__ bool bfWork(const BfRun &r, const BfSmem &L, uint32_t tmem, BfPipe &pp, int tid)
 {
    const int T_ = r.T;
    const int Kt = bfK(T_);
@@ -713,9 +749,10 @@ __device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint3
    auto q0 = [&](int t) { return r.inShift + (long long) t * kBfTile; };
    auto bulkOk = [&](int t) {
       const long long q = q0(t);
-      return q >= 0 && q + (long long) nb * 64 <= r.inLen && ((((uintptr_t) (r.x + q)) & 15) == 0);
+      return S > 0 && q >= 0 && q + (long long) nb * 64 <= r.inLen && ((((uintptr_t) (r.x + q)) & 15) == 0);
    };
-   // The first raw tiles are fetched while the taps band is built.
+   // The first raw tiles are fetched while the taps band is built.  (Every MMA of the
+   // previous run completed: its last tile was drained.)
    if (tid == 0)
       for (int k = 0; k < S && r.t0 + k < r.t1; k++)
          if (bulkOk(r.t0 + k)) {
@@ -725,25 +762,25 @@ __device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint3
    for (int k = 0; k < S && r.t0 + k < r.t1; k++)
       if (bulkOk(r.t0 + k)) pp.pending |= 1u << k;
    // g[c] split into hi/lo, stored at slot c + kBfPadLeft; zero elsewhere.
-   for (int sl = tid; sl < slots; sl += kBfThreads) {
+   for (int sl = tid; sl < slots; sl += kBfWorkers) {
       const int c = sl - kBfPadLeft;
       uint16_t hi = 0, lo = 0;
       if (c >= 0 && c < T_) splitBf16(r.reverse ? r.h[T_ - 1 - c] : r.h[c], hi, lo);
       L.gHi[sl] = hi;
       L.gLo[sl] = lo;
    }
-   __syncthreads();
+   tc::namedSync(kBfBar, kBfWorkers);
    // Taps band, K-major no swizzle: 16-byte chunk (q, n) at q*2048 + (n/8)*128 + (n%8)*16 holds
    // B[8q .. 8q+7][n]; rows n < 64: g_hi[m - n], rows n >= 64: g_lo[m - (n - 64)].
    // Each chunk is 8 consecutive split taps from an arbitrary element offset o: the two
    // aligned 16-byte vectors around it, shifted into place (funnel shifts by 16 bits for
    // odd offsets), instead of 8 scalar reads.
-   for (int cidx = tid; cidx < (Kt / 8) * 128; cidx += kBfThreads) {
+   for (int cidx = tid; cidx < (Kt / 8) * 128; cidx += kBfWorkers) {
       const int q = cidx >> 7, n = cidx & 127;
       const int o = kBfPadLeft + 8 * q - (n & 63);
       const uint4 *base = (const uint4 *) (n < 64 ? L.gHi : L.gLo) + (o >> 3);
       const uint4 lo4 = base[0], hi4 = base[1];
-      const int r = o & 7, h = r >> 1;
+      const int rr = o & 7, h = rr >> 1;
       // words h .. h + 4 of the 8 (selects, not an indexed array: it stays in registers)
       const uint32_t w0 = h == 0 ? lo4.x : h == 1 ? lo4.y : h == 2 ? lo4.z : lo4.w;
       const uint32_t w1 = h == 0 ? lo4.y : h == 1 ? lo4.z : h == 2 ? lo4.w : hi4.x;
@@ -751,7 +788,7 @@ __device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint3
       const uint32_t w3 = h == 0 ? lo4.w : h == 1 ? hi4.x : h == 2 ? hi4.y : hi4.z;
       const uint32_t w4 = h == 0 ? hi4.x : h == 1 ? hi4.y : h == 2 ? hi4.z : hi4.w;
       uint4 v;
-      if (r & 1) {
+      if (rr & 1) {
          v.x = __funnelshift_r(w0, w1, 16);
          v.y = __funnelshift_r(w1, w2, 16);
          v.z = __funnelshift_r(w2, w3, 16);
@@ -765,58 +802,86 @@ __device__ __forceinline__ bool bfProcess(const BfRun &r, const BfSmem &L, uint3
       }
       *(uint4 *) (L.Bt + q * 2048 + (n >> 3) * 128 + (n & 7) * 16) = v;
    }
-   for (int t = r.t0; t < r.t1; t++) {
-      const int k = (t - r.t0) % S;
-      bool ok = true;
-      const bool viaBulk = bulkOk(t);
-      if (viaBulk) {
-         ok = tid == 0 ? tc::mbarWait(L.full + k, (pp.par >> k) & 1) : true; // the barrier below releases the rest
-         pp.par ^= 1u << k;
-         pp.pending &= ~(1u << k);
-      }
-      if (!ok && tid == 0) raiseError(r.err);
-      // raw tile landed; the previous tile's outputs have left the planes
-      if (__syncthreads_or(!ok)) return false;
-      if (viaBulk) bfSplit(L.slot(k), nb, L.hi, L.lo, tid);
-      else bfStage(r.x, q0(t), r.inLen, nb, L.hi, L.lo, tid); // straight from global memory
-      tc::fenceProxyAsync();
-      __syncthreads(); // planes and band written; the raw stage is free again
-      if (t + S < r.t1 && bulkOk(t + S)) {
-         if (tid == 0) {
-            tc::mbarExpectTx(L.full + k, rawBytes);
-            tc::bulkLoad(L.slot(k), r.x + q0(t + S), rawBytes, L.full + k);
+   for (int t = r.t0; t <= r.t1; t++) {
+      const int cur = (int) (pp.tiles & 1), prev = cur ^ 1;
+      if (t < r.t1) {
+         // plane set and accumulator cur are free: tile t - 2 was drained
+         const int k = S > 0 ? (t - r.t0) % S : 0;
+         bool ok = true;
+         const bool viaBulk = bulkOk(t);
+         if (viaBulk) {
+            ok = tid == 0 ? tc::mbarWait(L.full + k, (pp.par >> k) & 1) : true; // the barrier below releases the rest
+            pp.par ^= 1u << k;
+            pp.pending &= ~(1u << k);
          }
-         pp.pending |= 1u << k;
-      }
-      if (tid == 0) {
-         tc::fenceAfterSync();
-         const uint32_t ahi = tc::smemAddr(L.hi), alo = tc::smemAddr(L.lo), bt = tc::smemAddr(L.Bt);
-         const uint32_t id128 = tc::idesc(1, 1, 1, kRows, 128);
-         const uint32_t d = tmem;
-         for (int k16 = 0; k16 < Kt / 16; k16++) {
-            const int blk = k16 >> 2, sub = k16 & 3;
-            // The swizzle is applied on absolute shared-memory address bits, so a start
-            // that is not atom-aligned (block blk of the plane) keeps base offset 0.
-            const uint64_t dHi = tc::descSw128(ahi + blk * 128 + sub * 32, 1024, 0);
-            const uint64_t dLo = tc::descSw128(alo + blk * 128 + sub * 32, 1024, 0);
-            const uint64_t dB = tc::descNoSwizzle(bt + k16 * 4096, 2048, 128);
-            tc::mmaF16(d, dHi, dB, id128, k16 > 0);
-            tc::mmaF16(d, dLo, dB, id128, true);
+         if (!ok && tid == 0) raiseError(r.err);
+         if (tc::namedSyncOr(kBfBar, kBfWorkers, !ok)) return false; // the raw tile landed (and the band is built)
+         if (viaBulk) bfSplit(L.slot(k), nb, L.hi(cur), L.lo(cur), tid);
+         else bfStage(r.x, q0(t), r.inLen, nb, L.hi(cur), L.lo(cur), tid); // straight from global memory
+         tc::fenceProxyAsync();
+         tc::fenceBeforeSync();
+         tc::namedSync(kBfBar, kBfWorkers); // planes (and band) written; the raw stage is free again
+         if (tid == 0) tc::mbarArrive(L.planesFull + cur);
+         if (t + S < r.t1 && bulkOk(t + S)) {
+            if (tid == 0) {
+               tc::mbarExpectTx(L.full + k, rawBytes);
+               tc::bulkLoad(L.slot(k), r.x + q0(t + S), rawBytes, L.full + k);
+            }
+            pp.pending |= 1u << k;
          }
-         tc::commit(L.mbar);
+         pp.tiles++;
       }
-      if (!bfDrain(r, L, tmem, pp, t, tid)) return false;
+      if (t > r.t0) {
+         // tile t - 1 (accumulator and plane set prev) while tile t's MMAs run
+         if (!bfWaitMma(L, pp, prev, r.err, tid)) return false;
+         bfDrain(r, L, tmem, prev, t - 1, tid);
+      }
    }
-   __syncthreads(); // before the taps band of the next run is rebuilt
+   return true;
+}
+
+// MMA thread: for each tile of run r, once its plane set is full, the Toeplitz
+// contraction into the tile's accumulator and a commit to its mmaDone barrier.
+__device__ __forceinline__ bool bfIssue(const BfRun &r, const BfSmem &L, uint32_t tmem, BfIssuer &mi)
+{
+   const int Kt = bfK(r.T);
+   const uint32_t bt = tc::smemAddr(L.Bt);
+   const uint32_t id128 = tc::idesc(1, 1, 1, kRows, 128);
+   for (int t = r.t0; t < r.t1; t++) {
+      const int b = (int) (mi.tiles & 1);
+      if (!tc::mbarWait(L.planesFull + b, (mi.pfPar >> b) & 1)) {
+         raiseError(r.err);
+         return false;
+      }
+      mi.pfPar ^= 1u << b;
+      tc::fenceAfterSync();
+      const uint32_t ahi = tc::smemAddr(L.hi(b)), alo = tc::smemAddr(L.lo(b));
+      const uint32_t d = tmem + (uint32_t) b * 128;
+      for (int k16 = 0; k16 < Kt / 16; k16++) {
+         const int blk = k16 >> 2, sub = k16 & 3;
+         // The swizzle is applied on absolute shared-memory address bits, so a start
+         // that is not atom-aligned (block blk of the plane) keeps base offset 0.
+         const uint64_t dHi = tc::descSw128(ahi + blk * 128 + sub * 32, 1024, 0);
+         const uint64_t dLo = tc::descSw128(alo + blk * 128 + sub * 32, 1024, 0);
+         const uint64_t dB = tc::descNoSwizzle(bt + k16 * 4096, 2048, 128);
+         tc::mmaF16(d, dHi, dB, id128, k16 > 0);
+         tc::mmaF16(d, dLo, dB, id128, true);
+      }
+      tc::commit(L.mbar + b);
+      if (b) mi.commits1++;
+      else mi.commits0++;
+      mi.tiles++;
+   }
    return true;
 }
 
 // Set-up and tear-down shared by the bf16x3 kernels.
 __device__ __forceinline__ uint32_t bfBegin(const BfSmem &L, int tid)
 {
-   if ((tid >> 5) == 0) tc::tmemAlloc(L.tslot, 128);
+   if ((tid >> 5) == 0) tc::tmemAlloc(L.tslot, kBfTmemCols);
    if (tid == 0) {
-      tc::mbarInit(L.mbar, 1);
+      for (int k = 0; k < 2; k++) tc::mbarInit(L.mbar + k, 1);
+      for (int k = 0; k < 2; k++) tc::mbarInit(L.planesFull + k, 1);
       for (int k = 0; k < 2; k++) tc::mbarInit(L.full + k, 1);
       tc::fenceMbarInit();
    }
@@ -826,16 +891,25 @@ __device__ __forceinline__ uint32_t bfBegin(const BfSmem &L, int tid)
    return *L.tslot;
 }
 
-__device__ __forceinline__ void bfEnd(const BfSmem &L, const BfPipe &pp, uint32_t tmem, int tid)
+// After the roles' loops (also after a failure): the MMA thread waits (bounded) for its
+// last commit on each accumulator, worker 0 for the bulk copies still in flight; then
+// the accumulators are released.
+__device__ __forceinline__ void bfEnd(const BfSmem &L, const BfPipe &pp, const BfIssuer &mi, uint32_t tmem, int tid)
 {
-   // After a failure, let the copies still in flight land before the shared memory is released.
-   for (int k = 0; k < 2; k++)
-      if (tid == 0 && ((pp.pending >> k) & 1)) (void) tc::mbarWait(L.full + k, (pp.par >> k) & 1);
+   if (tid == kBfWorkers) {
+      if (mi.commits0) (void) tc::mbarWait(L.mbar, (mi.commits0 - 1) & 1);
+      if (mi.commits1) (void) tc::mbarWait(L.mbar + 1, (mi.commits1 - 1) & 1);
+   }
+   if (tid == 0)
+      for (int k = 0; k < 2; k++)
+         if ((pp.pending >> k) & 1) (void) tc::mbarWait(L.full + k, (pp.par >> k) & 1);
+   tc::fenceBeforeSync();
    __syncthreads();
-   if ((tid >> 5) == 0) tc::tmemFree(tmem, 128);
+   tc::fenceAfterSync();
+   if ((tid >> 5) == 0) tc::tmemFree(tmem, kBfTmemCols);
 }
 
-__global__ void __launch_bounds__(kBfThreads, 1) fir_bf16x3_tc_kernel(FirLaunch a, int tilesPerCta)
+__global__ void __launch_bounds__(kBfBlock, 1) fir_bf16x3_tc_kernel(FirLaunch a, int tilesPerCta)
 {
    extern __shared__ __align__(16) unsigned char smraw[];
    const BfSmem L = bfSmemLayout(smraw, a.T);
@@ -843,53 +917,59 @@ __global__ void __launch_bounds__(kBfThreads, 1) fir_bf16x3_tc_kernel(FirLaunch 
    const uint32_t tmem = bfBegin(L, tid);
    const int nt = (a.outSize + kBfTile - 1) / kBfTile;
    BfPipe pp;
-   for (int l = blockIdx.y; l < a.batch; l += gridDim.y) {
-      BfRun r;
-      r.x = (const float *) a.x + (long long) l * a.inPitch;
-      r.h = (const float *) a.h + (long long) l * a.filtPitch;
-      r.y = (float *) a.y + (long long) l * a.outPitch;
-      r.inShift = 0;
-      r.inLen = (long long) a.outSize + a.T - 1;
-      r.outLen = a.outSize;
-      r.T = a.T;
-      r.reverse = 1;
-      r.t0 = blockIdx.x * tilesPerCta;
-      r.t1 = min(nt, r.t0 + tilesPerCta);
-      r.err = a.err;
-      if (!bfProcess(r, L, tmem, pp, tid)) break;
-   }
-   bfEnd(L, pp, tmem, tid);
+   BfIssuer mi;
+   if (tid < kBfWorkers || tid == kBfWorkers)
+      for (int l = blockIdx.y; l < a.batch; l += gridDim.y) {
+         BfRun r;
+         r.x = (const float *) a.x + (long long) l * a.inPitch;
+         r.h = (const float *) a.h + (long long) l * a.filtPitch;
+         r.y = (float *) a.y + (long long) l * a.outPitch;
+         r.inShift = 0;
+         r.inLen = (long long) a.outSize + a.T - 1;
+         r.outLen = a.outSize;
+         r.T = a.T;
+         r.reverse = 1;
+         r.t0 = blockIdx.x * tilesPerCta;
+         r.t1 = min(nt, r.t0 + tilesPerCta);
+         r.err = a.err;
+         if (!(tid < kBfWorkers ? bfWork(r, L, tmem, pp, tid) : bfIssue(r, L, tmem, mi))) break;
+      }
+   bfEnd(L, pp, mi, tmem, tid);
 }
 
-// Work lists of the batched filter bank: one run of up to kFirBfRunTiles tiles of
-// one channel per CTA.  DX = false: forward, y = valid correlation of x with
-// the taps (DSPLIB_fir order); DX = true: input gradient, the full convolution
-// of the output gradient with the taps.
-__global__ void __launch_bounds__(kBfThreads, 1)
-    fir_bf16x3_ragged_kernel(const RaggedChan *chans, const int4 *runs, const float *in, const float *taps,
-                             float *out, int dx, int Tmax, int *err)
+// Work lists of the batched filter bank: runs of up to kFirBfRunTiles tiles of one
+// channel, longest first, taken in turn by one persistent CTA per SM.  DX = false:
+// forward, y = valid correlation of x with the taps (DSPLIB_fir order); DX = true:
+// input gradient, the full convolution of the output gradient with the taps.
+__global__ void __launch_bounds__(kBfBlock, 1)
+    fir_bf16x3_ragged_kernel(const RaggedChan *chans, const int4 *runs, int nRuns, const float *in,
+                             const float *taps, float *out, int dx, int Tmax, int *err)
 {
    extern __shared__ __align__(16) unsigned char smraw[];
    const BfSmem L = bfSmemLayout(smraw, Tmax);
    const int tid = threadIdx.x;
    const uint32_t tmem = bfBegin(L, tid);
-   const int4 it = runs[blockIdx.x];
-   const RaggedChan c = chans[it.x];
-   BfRun r;
-   r.x = in + c.xOff;
-   r.h = taps + c.hOff;
-   r.y = out + (dx ? c.xOff : c.pOff); // forward: plane 0 of the work buffer
-   r.T = c.T;
-   r.inShift = dx ? -(long long) (c.T - 1) : 0;
-   r.inLen = dx ? c.L - c.T + 1 : c.L;
-   r.outLen = dx ? c.L : c.L - c.T + 1;
-   r.reverse = dx ? 0 : 1;
-   r.t0 = it.y;
-   r.t1 = it.y + it.z;
-   r.err = err;
    BfPipe pp;
-   bfProcess(r, L, tmem, pp, tid);
-   bfEnd(L, pp, tmem, tid);
+   BfIssuer mi;
+   if (tid < kBfWorkers || tid == kBfWorkers)
+      for (int i = blockIdx.x; i < nRuns; i += gridDim.x) {
+         const int4 it = runs[i];
+         const RaggedChan c = chans[it.x];
+         BfRun r;
+         r.x = in + c.xOff;
+         r.h = taps + c.hOff;
+         r.y = out + (dx ? c.xOff : c.pOff); // forward: plane 0 of the work buffer
+         r.T = c.T;
+         r.inShift = dx ? -(long long) (c.T - 1) : 0;
+         r.inLen = dx ? c.L - c.T + 1 : c.L;
+         r.outLen = dx ? c.L : c.L - c.T + 1;
+         r.reverse = dx ? 0 : 1;
+         r.t0 = it.y;
+         r.t1 = it.y + it.z;
+         r.err = err;
+         if (!(tid < kBfWorkers ? bfWork(r, L, tmem, pp, tid) : bfIssue(r, L, tmem, mi))) break;
+      }
+   bfEnd(L, pp, mi, tmem, tid);
 }
 
 
@@ -1074,7 +1154,7 @@ cudaError_t launchFirBf16x3(const FirLaunch &a, cudaStream_t s)
    const int nt = (a.outSize + kBfTile - 1) / kBfTile;
    const int tpc = tilesPerCtaFor(nt, a.batch, 1);
    dim3 grid((nt + tpc - 1) / tpc, a.batch < 65535 ? a.batch : 65535);
-   fir_bf16x3_tc_kernel<<<grid, kBfThreads, smem, s>>>(a, tpc);
+   fir_bf16x3_tc_kernel<<<grid, kBfBlock, smem, s>>>(a, tpc);
    countLaunch();
    return cudaGetLastError();
 }
@@ -1088,7 +1168,10 @@ cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int
    cudaError_t e =
        cudaFuncSetAttribute(fir_bf16x3_ragged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
    if (e != cudaSuccess) return e;
-   fir_bf16x3_ragged_kernel<<<nRuns, kBfThreads, smem, s>>>(chans, runs, in, taps, out, dx ? 1 : 0, Tmax, err);
+   int sms = 148, dev = 0;
+   if (cudaGetDevice(&dev) == cudaSuccess) (void) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+   const int grid = nRuns < sms ? nRuns : sms;
+   fir_bf16x3_ragged_kernel<<<grid, kBfBlock, smem, s>>>(chans, runs, nRuns, in, taps, out, dx ? 1 : 0, Tmax, err);
    countLaunch();
    return cudaGetLastError();
 }

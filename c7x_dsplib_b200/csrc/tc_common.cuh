@@ -107,12 +107,37 @@ __device__ __forceinline__ bool mbarWait(uint64_t *mbar, uint32_t parity, uint32
    return false;
 }
 
-// TMEM allocation by one full warp; the base address is written to *slot (shared memory).
 // Announce `bytes` of transaction traffic on mbar (this thread's arrival included).
 __device__ __forceinline__ void mbarExpectTx(uint64_t *mbar, uint32_t bytes)
 {
    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(mbar)), "r"(bytes)
                 : "memory");
+}
+
+// Plain arrival of this thread on mbar (release: its earlier shared-memory writes are
+// visible to a thread whose wait on mbar completes).
+__device__ __forceinline__ void mbarArrive(uint64_t *mbar)
+{
+   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(mbar)) : "memory");
+}
+
+// Named barrier `id` over the first `n` threads of the CTA (n a multiple of 32), and the
+// same with an OR over a predicate of the participating threads.
+__device__ __forceinline__ void namedSync(uint32_t id, uint32_t n)
+{
+   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+__device__ __forceinline__ bool namedSyncOr(uint32_t id, uint32_t n, bool v)
+{
+   uint32_t r;
+   asm volatile("{\n\t.reg .pred p, q;\n\t"
+                "setp.ne.u32 q, %2, 0;\n\t"
+                "bar.red.or.pred p, %1, %3, q;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}\n"
+                : "=r"(r)
+                : "r"(id), "r"((uint32_t) v), "r"(n)
+                : "memory");
+   return r != 0;
 }
 
 // Bulk copy (TMA engine, no tensor map) of `bytes` from global memory to this
@@ -134,6 +159,7 @@ __device__ __forceinline__ void cpAsync16(void *dst, const void *src)
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// TMEM allocation by one full warp; the base address is written to *slot (shared memory).
 __device__ __forceinline__ void tmemAlloc(uint32_t *slot, uint32_t ncols)
 {
    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(slot)),
