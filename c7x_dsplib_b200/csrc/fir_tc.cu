@@ -513,6 +513,16 @@ __device__ __forceinline__ void splitBf16(float v, uint16_t &hi, uint16_t &lo)
    lo = __bfloat16_as_ushort(l);
 }
 
+// The same for two values at once, packed (a in the low half): one paired conversion
+// per plane, rounding each value exactly as splitBf16 does.
+__device__ __forceinline__ void splitBf16x2(float a, float b, uint32_t &hi, uint32_t &lo)
+{
+   const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+   const __nv_bfloat162 l = __floats2bfloat162_rn(a - __low2float(h), b - __high2float(h));
+   hi = *(const uint32_t *) &h;
+   lo = *(const uint32_t *) &l;
+}
+
 // Stage one tile's signal planes: sample i of the tile (64 per 128-byte block
 // k = i / 64) goes to block k, 16-byte chunk c = (i % 64) / 8 stored at
 // k*128 + ((c ^ (k & 7)) * 16), as hi and lo BF16.  Sample i is input index
@@ -553,12 +563,14 @@ __device__ __forceinline__ void bfStage(const float *x, long long q0, long long 
       const int cidx = tid + u * kBfThreads;
       if (cidx < nb * 8) {
          const int k = cidx >> 3, c = cidx & 7;
-         uint16_t hv[8], lv[8];
-#pragma unroll
-         for (int e = 0; e < 8; e++) splitBf16(f[u][e], hv[e], lv[e]);
+         uint4 hv, lv;
+         splitBf16x2(f[u][0], f[u][1], hv.x, lv.x);
+         splitBf16x2(f[u][2], f[u][3], hv.y, lv.y);
+         splitBf16x2(f[u][4], f[u][5], hv.z, lv.z);
+         splitBf16x2(f[u][6], f[u][7], hv.w, lv.w);
          const int off = k * 128 + ((c ^ (k & 7)) << 4);
-         *(uint4 *) (Ahi + off) = *(uint4 *) hv;
-         *(uint4 *) (Alo + off) = *(uint4 *) lv;
+         *(uint4 *) (Ahi + off) = hv;
+         *(uint4 *) (Alo + off) = lv;
       }
    }
 }
@@ -569,22 +581,27 @@ __device__ __forceinline__ void bfStage(const float *x, long long q0, long long 
 // threads straight into the planes (bfStage).
 // Split a raw tile into the signal planes: sample i (64 per 128-byte block
 // k = i / 64) goes to block k, 16-byte chunk c = (i % 64) / 8 stored at
-// k*128 + ((c ^ (k & 7)) * 16), as hi and lo BF16.  A thread takes 4 samples
-// (one 16-byte read; consecutive lanes, consecutive addresses) and writes half
-// a chunk of each plane.
-__device__ __forceinline__ void bfSplit(const float *raw, int nb, unsigned char *Ahi, unsigned char *Alo, int tid)
+// k*128 + ((c ^ (k & 7)) * 16), as hi and lo BF16.  Sample i is raw[mis + i]
+// (mis < 4: the bulk copy started at the 16-byte boundary below the tile).  A
+// thread takes 4 samples (consecutive lanes, consecutive addresses) and writes
+// half a chunk of each plane.
+__device__ __forceinline__ void bfSplit(const float *raw, int mis, int nb, unsigned char *Ahi, unsigned char *Alo,
+                                        int tid)
 {
    for (int f = tid; f < nb * 16; f += kBfThreads) {
-      const float4 v = ((const float4 *) raw)[f];
+      float4 v;
+      if (mis == 0) v = ((const float4 *) raw)[f];
+      else {
+         const float *p = raw + mis + 4 * f;
+         v = make_float4(p[0], p[1], p[2], p[3]);
+      }
       const int k = f >> 4, c = (f >> 1) & 7, half = f & 1;
-      uint16_t hv[4], lv[4];
-      splitBf16(v.x, hv[0], lv[0]);
-      splitBf16(v.y, hv[1], lv[1]);
-      splitBf16(v.z, hv[2], lv[2]);
-      splitBf16(v.w, hv[3], lv[3]);
+      uint2 hv, lv;
+      splitBf16x2(v.x, v.y, hv.x, lv.x);
+      splitBf16x2(v.z, v.w, hv.y, lv.y);
       const int off = k * 128 + ((c ^ (k & 7)) << 4) + half * 8;
-      *(uint2 *) (Ahi + off) = *(uint2 *) hv;
-      *(uint2 *) (Alo + off) = *(uint2 *) lv;
+      *(uint2 *) (Ahi + off) = hv;
+      *(uint2 *) (Alo + off) = lv;
    }
 }
 
@@ -619,24 +636,28 @@ constexpr uint32_t kBfTmemCols = 256;
 constexpr int kBfWorkers = kBfThreads;         // worker threads (16 warps)
 constexpr int kBfBlock = kBfWorkers + 32;      // + the MMA warp
 constexpr uint32_t kBfBar = 1;                 // the workers' named barrier
-__host__ __device__ constexpr size_t bfPlaneBytes(int Tmax) { return (size_t) ((bfBlocks(Tmax) * 128 + 1023) & ~1023); }
-__host__ __device__ constexpr size_t bfRawBytes(int Tmax) { return (size_t) bfBlocks(Tmax) * 256; }
-__host__ __device__ constexpr size_t bfSmemBytesFor(int Tmax, int stages)
+// Layout for taps up to T (the batched kernels lay out shared memory per run, for that
+// run's taps, in an allocation of kBfSmemLimit): the barriers and the TMEM slot in the
+// first 1024 bytes, then the plane sets, the raw ring, the band and the split taps.
+__host__ __device__ constexpr size_t bfPlaneBytes(int T) { return (size_t) ((bfBlocks(T) * 128 + 1023) & ~1023); }
+// a raw tile and the up to 3 samples before it (copies start on a 16-byte boundary),
+// padded to 128 bytes so that the band behind the ring keeps its 128-byte alignment
+__host__ __device__ constexpr size_t bfRawBytes(int T) { return (size_t) bfBlocks(T) * 256 + 128; }
+__host__ __device__ constexpr size_t bfSmemBytesFor(int T, int stages)
 {
-   return 1024 + 4 * bfPlaneBytes(Tmax) + stages * bfRawBytes(Tmax) + (size_t) bfK(Tmax) * 256 +
-          4 * (size_t) bfTapSlots(Tmax) + 128;
+   return 2048 + 4 * bfPlaneBytes(T) + stages * bfRawBytes(T) + (size_t) bfK(T) * 256 + 4 * (size_t) bfTapSlots(T);
 }
-__host__ __device__ inline int bfStages(int Tmax)
+__host__ __device__ inline int bfStages(int T)
 {
-   return bfSmemBytesFor(Tmax, 2) <= kBfSmemLimit ? 2 : (bfSmemBytesFor(Tmax, 1) <= kBfSmemLimit ? 1 : 0);
+   return bfSmemBytesFor(T, 2) <= kBfSmemLimit ? 2 : (bfSmemBytesFor(T, 1) <= kBfSmemLimit ? 1 : 0);
 }
-__host__ __device__ inline size_t bfSmemBytes(int Tmax) { return bfSmemBytesFor(Tmax, bfStages(Tmax)); }
+__host__ __device__ inline size_t bfSmemBytes(int T) { return bfSmemBytesFor(T, bfStages(T)); }
 static_assert(bfSmemBytesFor(kBfMaxTaps, 0) <= kBfSmemLimit, "two plane sets and the longest band fit");
 
 struct BfSmem {
    unsigned char *sets; // plane set b: hi at sets + 2 b planeBytes, lo planeBytes further (1024-byte aligned)
    size_t planeBytes;
-   float *raw;          // stages x bfBlocks(Tmax) * 64 floats
+   float *raw;          // stages x rawFloats
    int rawFloats, stages;
    unsigned char *Bt;
    uint16_t *gHi, *gLo;
@@ -647,23 +668,23 @@ struct BfSmem {
    __device__ unsigned char *lo(int b) const { return sets + (size_t) (2 * b + 1) * planeBytes; }
 };
 
-__device__ __forceinline__ BfSmem bfSmemLayout(unsigned char *smraw, int Tmax)
+__device__ __forceinline__ BfSmem bfSmemLayout(unsigned char *smraw, int T)
 {
    BfSmem L;
    unsigned char *sm = (unsigned char *) (((uintptr_t) smraw + 1023) & ~(uintptr_t) 1023);
-   const size_t pb = bfPlaneBytes(Tmax);
-   L.stages = bfStages(Tmax);
-   L.planeBytes = pb;
-   L.sets = sm;
-   L.raw = (float *) (sm + 4 * pb);
-   L.rawFloats = bfBlocks(Tmax) * 64;
-   L.Bt = (unsigned char *) L.raw + (size_t) L.stages * bfRawBytes(Tmax);
-   L.gHi = (uint16_t *) (L.Bt + (size_t) bfK(Tmax) * 256); // split taps with zero padding
-   L.gLo = L.gHi + bfTapSlots(Tmax);
-   L.mbar = (uint64_t *) (((uintptr_t) (L.gLo + bfTapSlots(Tmax)) + 15) & ~(uintptr_t) 15);
+   L.mbar = (uint64_t *) sm;
    L.planesFull = L.mbar + 2;
    L.full = L.planesFull + 2;
    L.tslot = (uint32_t *) (L.full + 2);
+   const size_t pb = bfPlaneBytes(T);
+   L.stages = bfStages(T);
+   L.planeBytes = pb;
+   L.sets = sm + 1024;
+   L.raw = (float *) (L.sets + 4 * pb);
+   L.rawFloats = (int) (bfRawBytes(T) / 4);
+   L.Bt = (unsigned char *) L.raw + (size_t) L.stages * bfRawBytes(T);
+   L.gHi = (uint16_t *) (L.Bt + (size_t) bfK(T) * 256); // split taps with zero padding
+   L.gLo = L.gHi + bfTapSlots(T);
    return L;
 }
 
@@ -706,22 +727,26 @@ __device__ __forceinline__ void bfDrain(const BfRun &r, const BfSmem &L, uint32_
       const int quad = warp & 3, qt = warp >> 2, half = qt >> 1;
       const uint32_t acc = tmem + (uint32_t) b * 128 + ((uint32_t) (quad * 32) << 16);
       const int row = quad * 32 + lane;
-      uint32_t a[16], c[16];
-      tc::tmemLoad16(acc + qt * 16, a);
-      tc::tmemLoad16(acc + 64 + qt * 16, c);
-      tc::tmemWaitLoad();
       // 16-byte chunk v4 of row half (row, half) rotated to slot (v4 + row) & 7 so that
-      // eight consecutive rows store to distinct banks.
+      // eight consecutive rows store to distinct banks.  Two passes of 8 columns keep
+      // the register footprint small.
       float *os = (float *) stage + row * kBfPhases + half * 32;
 #pragma unroll
-      for (int v = 0; v < 4; v++) {
-         const int v4 = (qt & 1) * 4 + v;
-         float4 o;
-         o.x = __uint_as_float(a[4 * v + 0]) + __uint_as_float(c[4 * v + 0]);
-         o.y = __uint_as_float(a[4 * v + 1]) + __uint_as_float(c[4 * v + 1]);
-         o.z = __uint_as_float(a[4 * v + 2]) + __uint_as_float(c[4 * v + 2]);
-         o.w = __uint_as_float(a[4 * v + 3]) + __uint_as_float(c[4 * v + 3]);
-         *(float4 *) (os + (((v4 + row) & 7) << 2)) = o;
+      for (int h8 = 0; h8 < 2; h8++) {
+         uint32_t a[8], c[8];
+         tc::tmemLoad8(acc + qt * 16 + h8 * 8, a);
+         tc::tmemLoad8(acc + 64 + qt * 16 + h8 * 8, c);
+         tc::tmemWaitLoad();
+#pragma unroll
+         for (int v = 0; v < 2; v++) {
+            const int v4 = (qt & 1) * 4 + h8 * 2 + v;
+            float4 o;
+            o.x = __uint_as_float(a[4 * v + 0]) + __uint_as_float(c[4 * v + 0]);
+            o.y = __uint_as_float(a[4 * v + 1]) + __uint_as_float(c[4 * v + 1]);
+            o.z = __uint_as_float(a[4 * v + 2]) + __uint_as_float(c[4 * v + 2]);
+            o.w = __uint_as_float(a[4 * v + 3]) + __uint_as_float(c[4 * v + 3]);
+            *(float4 *) (os + (((v4 + row) & 7) << 2)) = o;
+         }
       }
    }
    tc::fenceBeforeSync();
@@ -745,20 +770,30 @@ __device__ __forceinline__ bool bfWork(const BfRun &r, const BfSmem &L, uint32_t
    const int nb = bfBlocks(T_);
    const int slots = bfTapSlots(T_);
    const int S = L.stages;
-   const uint32_t rawBytes = (uint32_t) nb * 256;
    auto q0 = [&](int t) { return r.inShift + (long long) t * kBfTile; };
+   // Blocks of tile t the MMAs read for its valid output rows (a short last tile needs
+   // fewer; the rows beyond are computed from stale planes and never stored).
+   auto blocksOf = [&](int t) {
+      const int outs = (int) min((long long) kBfTile, (long long) r.outLen - (long long) t * kBfTile);
+      return min(nb, (outs + kBfPhases - 1) / kBfPhases + (Kt + 63) / 64);
+   };
+   // samples between the 16-byte boundary at or below the tile's first input and that input
+   auto misOf = [&](int t) { return (int) ((((long long) ((uintptr_t) r.x >> 2)) + q0(t)) & 3); };
+   auto bytesOf = [&](int t) { return (uint32_t) blocksOf(t) * 256u + (misOf(t) ? 16u : 0u); };
+   // a bulk copy needs the whole window [q - mis, q - mis + bytes / 4) inside the input
    auto bulkOk = [&](int t) {
-      const long long q = q0(t);
-      return S > 0 && q >= 0 && q + (long long) nb * 64 <= r.inLen && ((((uintptr_t) (r.x + q)) & 15) == 0);
+      const long long w0 = q0(t) - misOf(t);
+      return S > 0 && w0 >= 0 && w0 + bytesOf(t) / 4 <= r.inLen;
+   };
+   auto fetch = [&](int t, int k) {
+      tc::mbarExpectTx(L.full + k, bytesOf(t));
+      tc::bulkLoad(L.slot(k), r.x + (q0(t) - misOf(t)), bytesOf(t), L.full + k);
    };
    // The first raw tiles are fetched while the taps band is built.  (Every MMA of the
    // previous run completed: its last tile was drained.)
    if (tid == 0)
       for (int k = 0; k < S && r.t0 + k < r.t1; k++)
-         if (bulkOk(r.t0 + k)) {
-            tc::mbarExpectTx(L.full + k, rawBytes);
-            tc::bulkLoad(L.slot(k), r.x + q0(r.t0 + k), rawBytes, L.full + k);
-         }
+         if (bulkOk(r.t0 + k)) fetch(r.t0 + k, k);
    for (int k = 0; k < S && r.t0 + k < r.t1; k++)
       if (bulkOk(r.t0 + k)) pp.pending |= 1u << k;
    // g[c] split into hi/lo, stored at slot c + kBfPadLeft; zero elsewhere.
@@ -816,17 +851,14 @@ __device__ __forceinline__ bool bfWork(const BfRun &r, const BfSmem &L, uint32_t
          }
          if (!ok && tid == 0) raiseError(r.err);
          if (tc::namedSyncOr(kBfBar, kBfWorkers, !ok)) return false; // the raw tile landed (and the band is built)
-         if (viaBulk) bfSplit(L.slot(k), nb, L.hi(cur), L.lo(cur), tid);
-         else bfStage(r.x, q0(t), r.inLen, nb, L.hi(cur), L.lo(cur), tid); // straight from global memory
+         if (viaBulk) bfSplit(L.slot(k), misOf(t), blocksOf(t), L.hi(cur), L.lo(cur), tid);
+         else bfStage(r.x, q0(t), r.inLen, blocksOf(t), L.hi(cur), L.lo(cur), tid); // straight from global memory
          tc::fenceProxyAsync();
          tc::fenceBeforeSync();
          tc::namedSync(kBfBar, kBfWorkers); // planes (and band) written; the raw stage is free again
          if (tid == 0) tc::mbarArrive(L.planesFull + cur);
          if (t + S < r.t1 && bulkOk(t + S)) {
-            if (tid == 0) {
-               tc::mbarExpectTx(L.full + k, rawBytes);
-               tc::bulkLoad(L.slot(k), r.x + q0(t + S), rawBytes, L.full + k);
-            }
+            if (tid == 0) fetch(t + S, k);
             pp.pending |= 1u << k;
          }
          pp.tiles++;
@@ -946,6 +978,7 @@ __global__ void __launch_bounds__(kBfBlock, 1)
                              const float *taps, float *out, int dx, int Tmax, int *err)
 {
    extern __shared__ __align__(16) unsigned char smraw[];
+   // barriers and the TMEM slot sit at fixed offsets; the rest is laid out per run
    const BfSmem L = bfSmemLayout(smraw, Tmax);
    const int tid = threadIdx.x;
    const uint32_t tmem = bfBegin(L, tid);
@@ -955,6 +988,7 @@ __global__ void __launch_bounds__(kBfBlock, 1)
       for (int i = blockIdx.x; i < nRuns; i += gridDim.x) {
          const int4 it = runs[i];
          const RaggedChan c = chans[it.x];
+         const BfSmem Lr = bfSmemLayout(smraw, c.T);
          BfRun r;
          r.x = in + c.xOff;
          r.h = taps + c.hOff;
@@ -967,7 +1001,7 @@ __global__ void __launch_bounds__(kBfBlock, 1)
          r.t0 = it.y;
          r.t1 = it.y + it.z;
          r.err = err;
-         if (!(tid < kBfWorkers ? bfWork(r, L, tmem, pp, tid) : bfIssue(r, L, tmem, mi))) break;
+         if (!(tid < kBfWorkers ? bfWork(r, Lr, tmem, pp, tid) : bfIssue(r, Lr, tmem, mi))) break;
       }
    bfEnd(L, pp, mi, tmem, tid);
 }
@@ -1164,7 +1198,7 @@ cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int
 {
    if (Tmax < 1 || Tmax > kBfMaxTaps) return cudaErrorNotSupported;
    if (nRuns <= 0) return cudaSuccess;
-   const size_t smem = bfSmemBytes(Tmax);
+   const size_t smem = kBfSmemLimit; // every run's layout (for its own taps) fits
    cudaError_t e =
        cudaFuncSetAttribute(fir_bf16x3_ragged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
    if (e != cudaSuccess) return e;

@@ -173,6 +173,14 @@ __device__ __forceinline__ void tmemFree(uint32_t taddr, uint32_t ncols)
    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
+// 32 lanes x 8 consecutive 32-bit columns: thread t of the warp receives lane (base lane + t).
+__device__ __forceinline__ void tmemLoad8(uint32_t taddr, uint32_t (&r)[8])
+{
+   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                : "r"(taddr));
+}
+
 // 32 lanes x 16 consecutive 32-bit columns: thread t of the warp receives lane (base lane + t).
 __device__ __forceinline__ void tmemLoad16(uint32_t taddr, uint32_t (&r)[16])
 {
