@@ -140,6 +140,17 @@ SIGNATURES = {
     "DSPLIB_gpu_firSetPrecision": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_firSetQMode": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_kernelLaunchCount": (ctypes.c_int64, []),
+    "DSPLIB_gpu_autotuneSetMode": (ctypes.c_int, [ctypes.c_int32]),
+    "DSPLIB_gpu_autotuneGetMode": (ctypes.c_int32, []),
+    "DSPLIB_gpu_autotuneSetCachePath": (ctypes.c_int, [ctypes.c_char_p]),
+    "DSPLIB_gpu_autotuneSave": (ctypes.c_int, []),
+    "DSPLIB_gpu_autotuneClear": (ctypes.c_int, []),
+    "DSPLIB_gpu_autotuneLookup": (ctypes.c_int32, [ctypes.c_char_p]),
+    "DSPLIB_gpu_autotuneStore": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32]),
+    "DSPLIB_gpu_autotuneCount": (ctypes.c_int32, []),
+    "DSPLIB_gpu_autotune": (ctypes.c_int, [_VP]),
+    "DSPLIB_gpu_autotuneHandleKey": (ctypes.c_int32, [_VP, ctypes.c_char_p, ctypes.c_int32]),
+    "DSPLIB_gpu_autotuneHandleCandidate": (ctypes.c_int32, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_releaseHandle": (ctypes.c_int, [_VP]),
     "DSPLIB_gpu_firStreamCreate": (ctypes.c_int, [_P(_VP), _P(FirInitArgs), _BP, _BP, _BP]),
     "DSPLIB_gpu_firStreamHandle": (_VP, [_VP]),
@@ -237,6 +248,16 @@ class _Handle:
         """False / 0: exec returns complete; True / 1: returns once queued (device buffers);
         2: returns once queued also with page-locked host buffers used in place."""
         return lib().DSPLIB_gpu_setAsync(self.h, int(level))
+
+    def tune_key(self):
+        """(autotuner key of this handle's configuration, candidate choices)."""
+        buf = ctypes.create_string_buffer(256)
+        n = lib().DSPLIB_gpu_autotuneHandleKey(self.h, buf, 256)
+        return buf.value.decode(), [lib().DSPLIB_gpu_autotuneHandleCandidate(self.h, i) for i in range(n)]
+
+    def autotune(self) -> int:
+        """Measure this configuration's candidates now and store the fastest."""
+        return lib().DSPLIB_gpu_autotune(self.h)
 
     def _check(self, what, st):
         if st != SUCCESS:

@@ -6,6 +6,9 @@
 #include <cstring>
 #include <vector>
 
+#include <string>
+#include <vector>
+
 #include "dsplib_internal.h"
 
 using namespace dsplib;
@@ -54,7 +57,91 @@ bool store(void *dst, const void *src, size_t bytes)
 
 float recipOrZero(float b0) { return b0 == 0.0f ? 0.0f : 1.0f / b0; }
 
+// An OPTIMIZED launch of this handle's problem on compact buffers (no pointers): what the
+// autotuner keys and measures.  Per-channel coefficient rows are padded as exec pads them.
+BiquadLaunch bqShape(const BiquadPriv *p)
+{
+   const DSPLIB_cascadeBiquad_InitArgs &ia = p->initArgs;
+   BiquadLaunch a{};
+   a.form = (int) ia.biquadForm;
+   a.nch = ia.enableNChCoeffs ? 1 : 0;
+   a.optLayout = 1;
+   a.N = (int) ia.dataSize;
+   a.C = (int) ia.numChannels;
+   a.S = (int) ia.numStages;
+   a.inPitch = a.outPitch = a.varPitch = a.C;
+   a.coefPitch = a.nch ? (a.C + kCoefVec - 1) / kCoefVec * kCoefVec : 0;
+   a.prefetch = 1;
+   return a;
+}
+
+// The handle's cached scan choice, resolved again when the table changed.
+int bqChoice(BiquadPriv *p, const BiquadLaunch &a)
+{
+   const unsigned gen = tuneGeneration();
+   if (p->tuneGen != gen) {
+      int c = -1;
+      const std::string key = biquadTuneKey(a);
+      if (key.empty() || !tuneLookup(key, &c)) c = -1;
+      p->tuneGen = gen;
+      p->tuneChoice = c;
+   }
+   return p->tuneChoice;
+}
+
 } // namespace
+
+namespace dsplib {
+
+std::string biquadHandleTuneKey(DSPLIB_kernelHandle h, std::vector<int> *cands)
+{
+   BiquadPriv *p = bqHandle(h);
+   if (!p || p->initArgs.funcStyle == DSPLIB_FUNCTION_NATC || !formValid(p->initArgs.biquadForm)) return std::string();
+   const BiquadLaunch a = bqShape(p);
+   if (cands) *cands = biquadTuneCandidates(a);
+   return biquadTuneKey(a);
+}
+
+// Every candidate shape on zero-filled scratch signals, states and coefficients of the
+// handle's sizes (the scan's time does not depend on the values), on a private stream.
+DSPLIB_STATUS biquadHandleTune(DSPLIB_kernelHandle h)
+{
+   BiquadPriv *p = bqHandle(h);
+   if (!p) return DSPLIB_ERR_NULL_POINTER;
+   std::vector<int> cands;
+   const std::string key = biquadHandleTuneKey(h, &cands);
+   if (key.empty() || cands.empty()) return DSPLIB_ERR_NOT_IMPLEMENTED;
+   BiquadLaunch a = bqShape(p);
+   const int nv = a.form == DSPLIB_BIQUAD_DF1 ? 4 : 2;
+   const size_t rows = a.form == DSPLIB_BIQUAD_TIF ? (size_t) a.S * 4 + tifGroups(a.S) : (size_t) a.S * 5;
+   const size_t xb = (size_t) a.N * a.C * 4, sb = (size_t) a.S * nv * a.C * 4;
+   const size_t cb = (a.nch ? rows * (size_t) a.coefPitch : rows) * 4;
+   void *x = nullptr, *y = nullptr, *st = nullptr, *cf = nullptr;
+   DSPLIB_STATUS status = DSPLIB_ERR_FAILURE;
+   if (cudaMalloc(&x, xb) == cudaSuccess && cudaMalloc(&y, xb) == cudaSuccess && cudaMalloc(&st, sb) == cudaSuccess &&
+       cudaMalloc(&cf, cb) == cudaSuccess && cudaMemset(x, 0, xb) == cudaSuccess &&
+       cudaMemset(st, 0, sb) == cudaSuccess && cudaMemset(cf, 0, cb) == cudaSuccess) {
+      a.x = (const float *) x;
+      a.y = (float *) y;
+      a.state = (float *) st;
+      a.coef = (const float *) cf;
+      const int best = tunePick(key, cands, [&](int c, cudaStream_t s) {
+         BiquadLaunch b = a;
+         b.tuneChoice = c;
+         return launchBiquadScan(b, s);
+      });
+      if (best >= 0) status = DSPLIB_SUCCESS;
+   }
+   (void) cudaGetLastError();
+   cudaFree(x);
+   cudaFree(y);
+   cudaFree(st);
+   cudaFree(cf);
+   p->tuneGen = 0;
+   return status;
+}
+
+} // namespace dsplib
 
 extern "C" {
 
@@ -263,6 +350,12 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_init(DSPLIB_kernelHandle handle,
    if (!formValid(a->biquadForm)) return DSPLIB_ERR_NOT_IMPLEMENTED; // :472-474, :611-614
    if (a->funcStyle != DSPLIB_FUNCTION_NATC) p->initArgs.funcStyle = DSPLIB_FUNCTION_OPTIMIZED;
    p->initialized = 1;
+   p->tuneGen = 0;
+   if (tuneMode() == DSPLIB_GPU_TUNE_MEASURE) {
+      int c = 0;
+      const std::string key = biquadHandleTuneKey(handle, nullptr);
+      if (!key.empty() && !tuneLookup(key, &c)) (void) biquadHandleTune(handle); // a failed measurement keeps the rule
+   }
    return DSPLIB_SUCCESS;
 }
 
@@ -376,6 +469,7 @@ DSPLIB_STATUS DSPLIB_cascadeBiquad_exec(DSPLIB_kernelHandle handle,
    a.varPitch = p->varPitch;
    a.coefPitch = coefPitch;
    a.prefetch = (!rin.onHost || rin.staged) ? 1 : 0; // not for mapped host memory
+   if (!natc) a.tuneChoice = bqChoice(p, bqShape(p));
    auto launch = [&](const BiquadLaunch &l, cudaStream_t st) {
       return natc ? launchBiquadSequential(l, st) : launchBiquadScan(l, st);
    };

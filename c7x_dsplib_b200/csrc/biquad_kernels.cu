@@ -37,6 +37,8 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <cstdio>
+
 #include "dsplib_internal.h"
 
 namespace cg = cooperative_groups;
@@ -886,9 +888,16 @@ template <int FORM> cudaError_t launchChanForm(const BiquadLaunch &a, cudaStream
 //    groups x K <= 128 CTAs resident in one wave; clusters of 16 are only taken while at
 //    most 7 of them are needed (no more are co-resident).  Fewer windows per CTA beat
 //    more CTAs once a second wave would be needed.
+// The autotuner's choice, where it has one for this problem class, replaces the rule:
+// 8 or 16 warps per CTA (windows of 256 or 512 samples) and up to 16 CTAs per cluster.
 template <int FORM> cudaError_t launchScanForm(const BiquadLaunch &a, cudaStream_t s)
 {
    if (a.C <= kChanKernelMaxChannels) return launchChanForm<FORM>(a, s);
+   if (a.tuneChoice > 0) {
+      const int W = a.tuneChoice / 100, K = a.tuneChoice % 100;
+      if (W == 8 && K >= 1) return launchScanShape<FORM, 8>(a, K, s);
+      if (W == 16 && K >= 1) return launchScanShape<FORM, 16>(a, K, s);
+   }
    const int groups = (a.C + 31) / 32;
    const long long chunks = (a.N + kScanL - 1) / kScanL;
    int K = 1;
@@ -922,6 +931,26 @@ cudaError_t launchBiquadSequential(const BiquadLaunch &a, cudaStream_t s)
 // (28 B per stage and channel: 160 stages take 222 KB of the 227 KB); deeper
 // cascades use the sequential kernel.
 int biquadScanMaxStages() { return 160; }
+
+std::string biquadTuneKey(const BiquadLaunch &a)
+{
+   if (!a.optLayout || a.C <= kChanKernelMaxChannels || a.S > biquadScanMaxStages() || a.N <= 0) return std::string();
+   char buf[160];
+   snprintf(buf, sizeof(buf), "bq_scan|form=%d|S=%d|nch=%d|ch=2^%d|N=2^%d|sms=%d", a.form, a.S, a.nch,
+            tuneClass(a.C), tuneClass(a.N), deviceSms());
+   return buf;
+}
+
+std::vector<int> biquadTuneCandidates(const BiquadLaunch &a)
+{
+   std::vector<int> c;
+   if (biquadTuneKey(a).empty()) return c;
+   const long long chunks = (a.N + kScanL - 1) / kScanL;
+   for (int W : {8, 16})
+      for (int K = 1; K <= (W < kMaxCluster ? W : kMaxCluster); K *= 2)
+         if (K == 1 || (long long) K * W <= chunks) c.push_back(100 * W + K);
+   return c;
+}
 
 cudaError_t launchBiquadScan(const BiquadLaunch &a, cudaStream_t s)
 {

@@ -7,6 +7,9 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <functional>
+#include <string>
+#include <vector>
 
 #include "dsplib.h"
 
@@ -44,6 +47,9 @@ struct FirPriv {
    int32_t filterPitch; // elements (DSPLIB_fir.cpp:156)
    int32_t outputSize;  // bufParamsOut->dim_x (DSPLIB_fir.cpp:155)
    int32_t initialized;
+   uint32_t tuneGen;    // autotuner generation the cached choice was resolved at (0: none)
+   int32_t tuneKind;    // kernel kind it was resolved for
+   int32_t tuneChoice;  // the choice (-1: the built-in rule)
 };
 
 struct BiquadPriv {
@@ -56,6 +62,8 @@ struct BiquadPriv {
    int32_t coefRows;  // rows of the coefficient buffer passed to init
    int32_t coefCols;  // elements per coefficient row
    int32_t initialized;
+   uint32_t tuneGen;   // autotuner generation the cached choice was resolved at (0: none)
+   int32_t tuneChoice; // the scan's choice (-1: the built-in rule)
 };
 
 // DSPLIB_fltoq15 / DSPLIB_q15tofl handle (DSPLIB_fltoq15_priv.h / DSPLIB_q15tofl_priv.h
@@ -86,6 +94,33 @@ struct AddNChPriv {
    int32_t dataType;
    int32_t initialized;
 };
+
+// ---------------------------------------------------------------- autotuner (autotune.cpp)
+
+// Current mode (DSPLIB_GPU_TUNE_*), and a counter that changes whenever an entry or
+// the mode does (handles re-resolve their choice when it moved).
+int tuneMode();
+unsigned tuneGeneration();
+// The cached choice for key (false when absent or the tuner is off).
+bool tuneLookup(const std::string &key, int *choice);
+void tuneStore(const std::string &key, int choice, bool save);
+// Power-of-two class of v (smallest c with 2^c >= v), and the current device's SM count.
+int tuneClass(long long v);
+int deviceSms();
+// Median of `reps` event-timed launches after one warm-up (ms; negative on failure).
+float tuneTime(const std::function<cudaError_t(cudaStream_t)> &launch, cudaStream_t s, int reps);
+// Time every candidate on a private stream, store the fastest under key (and rewrite the
+// cache file); returns it, or -1 when nothing could be timed.
+int tunePick(const std::string &key, const std::vector<int> &cands,
+             const std::function<cudaError_t(int, cudaStream_t)> &launch);
+
+// Autotuner entry points of the handle families (fir_api.cpp, biquad_api.cpp): the
+// tuning key of an initialised handle's configuration with its candidates ("" when its
+// kernel has no shapes to choose), and a measurement of them stored in the table.
+std::string firHandleTuneKey(DSPLIB_kernelHandle h, std::vector<int> *cands);
+DSPLIB_STATUS firHandleTune(DSPLIB_kernelHandle h);
+std::string biquadHandleTuneKey(DSPLIB_kernelHandle h, std::vector<int> *cands);
+DSPLIB_STATUS biquadHandleTune(DSPLIB_kernelHandle h);
 
 // ---------------------------------------------------------------- runtime
 
@@ -195,6 +230,8 @@ struct FirLaunch {
    long long filtPitch; // elements between tap rows, 0 = shared
    int shift;
    int *err = nullptr; // tensor-core kernels: error word for an expired bounded wait
+   int tuneTpc = 0;    // tensor-core kernels: output tiles per CTA (0: the built-in rule)
+   int tunePerSm = 0;  // int8/int16 tensor-core kernel: resident CTAs per SM (0: the built-in rule)
 };
 
 enum FirKernelKind {
@@ -244,6 +281,12 @@ cudaError_t launchAddNCh(const AddNChLaunch &a, cudaStream_t s);
 bool firIntTcSupported(const FirLaunch &a);
 bool firBf16x3Supported(const FirLaunch &a);
 cudaError_t launchFirIntTc(const FirLaunch &a, bool qmode, cudaStream_t s);
+// Autotuner entries of the tensor-core FIR kernels (kind FIR_F32_BF16X3, FIR_INT_WRAP_TC,
+// FIR_INT_Q_TC): the key of a launch's problem class ("" for kernels without shapes to
+// choose), its candidate choices, and a choice applied to a launch.
+std::string firTuneKey(const FirLaunch &a, FirKernelKind kind);
+std::vector<int> firTuneCandidates(const FirLaunch &a, FirKernelKind kind);
+void firApplyChoice(FirLaunch &a, FirKernelKind kind, int choice);
 
 // One channel of the batched filter bank: samples at xOff (length L; the FIR
 // output and the biquad signals use the first Lu = L - T + 1), T taps at hOff,
@@ -321,7 +364,14 @@ struct BiquadLaunch {
    int N, C, S;
    long long inPitch, outPitch, varPitch, coefPitch; // elements
    int prefetch = 0; // x is device memory: the scan kernel may fetch the next window early (cp.async)
+   int tuneChoice = -1; // scan shape from the autotuner: 100 * warps per CTA + CTAs per cluster (-1: the rule)
 };
+
+// Autotuner entries of the cascade-biquad scan (OPTIMIZED style): the key of a launch's
+// problem class ("" when the per-channel kernel or the sequential one runs) and its
+// candidate shapes (100 * warps per CTA + CTAs per cluster).
+std::string biquadTuneKey(const BiquadLaunch &a);
+std::vector<int> biquadTuneCandidates(const BiquadLaunch &a);
 
 // DSPLIB_cascadeBiquad_get_coefficients for device buffers (coef_kernels.cu): TIF transform
 // (tif != 0) or the per-channel coefficient-major reorder of the DF forms; pitch in floats

@@ -3,6 +3,8 @@
 // reference line by line where callers can observe it (status codes, computed
 // sizes and pitches); exec launches CUDA kernels instead of C7x code.
 #include <cstring>
+#include <string>
+#include <vector>
 
 #include "dsplib_internal.h"
 
@@ -37,7 +39,113 @@ FirPriv *firHandle(DSPLIB_kernelHandle h)
    return p;
 }
 
+// The kernel an exec of this handle runs for launch a (a's taps and sizes filled).
+FirKernelKind firKindOf(const FirPriv *p, const FirLaunch &a)
+{
+   const DSPLIB_fir_InitArgs &ia = p->initArgs;
+   const HandleCommon *hc = &p->common;
+   const bool natc = ia.funcStyle == DSPLIB_FUNCTION_NATC;
+   const bool floatQ = !natc && p->dtype == DSPLIB_FLOAT32 && ia.enableQ != 0;
+   FirKernelKind kind;
+   if (natc) kind = FIR_NATC;
+   else if (floatQ) kind = FIR_F32_Q;
+   else if (p->dtype == DSPLIB_FLOAT32)
+      kind = hc->firPrecision == DSPLIB_GPU_FIR_BF16X3 ? FIR_F32_BF16X3 : FIR_F32_SIMT;
+   else kind = hc->firQMode ? FIR_QMODE : FIR_NATC;
+   // Optimized 8/16-bit integers run on the tensor cores when the taps fit the band buffer.
+   if (!natc && (p->dtype == DSPLIB_INT8 || p->dtype == DSPLIB_INT16) && firIntTcSupported(a))
+      kind = hc->firQMode ? FIR_INT_Q_TC : FIR_INT_WRAP_TC;
+   // Split-BF16x3 covers up to 512 taps; longer filters run the FP32 CUDA-core kernel.
+   if (kind == FIR_F32_BF16X3 && !firBf16x3Supported(a)) kind = FIR_F32_SIMT;
+   return kind;
+}
+
+// A launch of this handle's problem on compact buffers (no pointers): what the autotuner
+// keys and measures.
+FirLaunch firShape(const FirPriv *p)
+{
+   const DSPLIB_fir_InitArgs &ia = p->initArgs;
+   FirLaunch a{};
+   a.dtype = p->dtype;
+   a.batch = ia.batchSize;
+   a.T = ia.filterSize;
+   a.outSize = p->outputSize;
+   a.inPitch = (long long) p->outputSize + (ia.filterSize > 0 ? ia.filterSize : 1) - 1;
+   a.outPitch = p->outputSize;
+   a.filtPitch = ia.enableNchCoefs ? ia.filterSize : 0;
+   const bool floatQ = ia.funcStyle != DSPLIB_FUNCTION_NATC && p->dtype == DSPLIB_FLOAT32 && ia.enableQ != 0;
+   a.shift = floatQ ? (int) ia.Q : (int) ia.shift;
+   return a;
+}
+
+// The handle's cached autotuner choice for kind, resolved again when the table changed.
+int firChoice(FirPriv *p, const FirLaunch &a, FirKernelKind kind)
+{
+   const unsigned gen = tuneGeneration();
+   if (p->tuneGen != gen || p->tuneKind != (int32_t) kind) {
+      int c = -1;
+      const std::string key = firTuneKey(a, kind);
+      if (key.empty() || !tuneLookup(key, &c)) c = -1;
+      p->tuneGen = gen;
+      p->tuneKind = (int32_t) kind;
+      p->tuneChoice = c;
+   }
+   return p->tuneChoice;
+}
+
 } // namespace
+
+namespace dsplib {
+
+std::string firHandleTuneKey(DSPLIB_kernelHandle h, std::vector<int> *cands)
+{
+   FirPriv *p = firHandle(h);
+   if (!p || p->initArgs.batchSize <= 0 || p->outputSize <= 0) return std::string();
+   const FirLaunch a = firShape(p);
+   const FirKernelKind kind = firKindOf(p, a);
+   if (cands) *cands = firTuneCandidates(a, kind);
+   return firTuneKey(a, kind);
+}
+
+// Every candidate on zero-filled scratch buffers of the handle's shape (the kernels'
+// time does not depend on the values), on a private stream; the fastest is stored.
+DSPLIB_STATUS firHandleTune(DSPLIB_kernelHandle h)
+{
+   FirPriv *p = firHandle(h);
+   if (!p) return DSPLIB_ERR_NULL_POINTER;
+   std::vector<int> cands;
+   const std::string key = firHandleTuneKey(h, &cands);
+   if (key.empty() || cands.empty()) return DSPLIB_ERR_NOT_IMPLEMENTED;
+   FirLaunch a = firShape(p);
+   const FirKernelKind kind = firKindOf(p, a);
+   const size_t xb = (size_t) a.batch * a.inPitch * p->elt;
+   const size_t hb = (size_t) (a.filtPitch ? a.batch : 1) * (a.T > 0 ? a.T : 1) * p->elt;
+   const size_t yb = (size_t) a.batch * a.outPitch * p->elt;
+   void *x = nullptr, *hh = nullptr, *y = nullptr;
+   DSPLIB_STATUS st = DSPLIB_ERR_FAILURE;
+   if (cudaMalloc(&x, xb) == cudaSuccess && cudaMalloc(&hh, hb) == cudaSuccess && cudaMalloc(&y, yb) == cudaSuccess &&
+       cudaMemset(x, 0, xb) == cudaSuccess && cudaMemset(hh, 0, hb) == cudaSuccess) {
+      a.x = x;
+      a.h = hh;
+      a.y = y;
+      a.err = errorWord(&p->common);
+      const int best = tunePick(key, cands, [&](int c, cudaStream_t s) {
+         FirLaunch b = a;
+         firApplyChoice(b, kind, c);
+         return launchFir(b, kind, s);
+      });
+      (void) takeErrorWord(&p->common);
+      if (best >= 0) st = DSPLIB_SUCCESS;
+   }
+   (void) cudaGetLastError();
+   cudaFree(x);
+   cudaFree(hh);
+   cudaFree(y);
+   p->tuneGen = 0;
+   return st;
+}
+
+} // namespace dsplib
 
 extern "C" {
 
@@ -127,6 +235,12 @@ DSPLIB_STATUS DSPLIB_fir_init(DSPLIB_kernelHandle handle,
       p->initArgs.funcStyle = DSPLIB_FUNCTION_OPTIMIZED;
    }
    p->initialized = 1;
+   p->tuneGen = 0;
+   if (status == DSPLIB_SUCCESS && tuneMode() == DSPLIB_GPU_TUNE_MEASURE) {
+      int c = 0;
+      const std::string key = firHandleTuneKey(handle, nullptr);
+      if (!key.empty() && !tuneLookup(key, &c)) (void) firHandleTune(handle); // a failed measurement keeps the rule
+   }
    return status;
 }
 
@@ -182,13 +296,6 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
       return DSPLIB_ERR_INVALID_VALUE;
    }
 
-   FirKernelKind kind;
-   if (natc) kind = FIR_NATC;
-   else if (floatQ) kind = FIR_F32_Q;
-   else if (p->dtype == DSPLIB_FLOAT32)
-      kind = hc->firPrecision == DSPLIB_GPU_FIR_BF16X3 ? FIR_F32_BF16X3 : FIR_F32_SIMT;
-   else kind = hc->firQMode ? FIR_QMODE : FIR_NATC;
-
    cudaStream_t s = hc->stream;
    Region rin{pIn, nullptr, (size_t) (outSize + (T > 0 ? T : 1) - 1) * elt, (size_t) batch,
               (size_t) p->inPitch * elt, false};
@@ -228,11 +335,8 @@ DSPLIB_STATUS DSPLIB_fir_exec(DSPLIB_kernelHandle handle, void *pIn, void *pFilt
    a.filtPitch = nch ? filtPitch : 0; // staging keeps the caller's row pitch
    a.shift = floatQ ? (int) ia.Q : (int) ia.shift;
    a.err = errorWord(hc);
-   // Optimized 8/16-bit integers run on the tensor cores when the taps fit the band buffer.
-   if (!natc && (p->dtype == DSPLIB_INT8 || p->dtype == DSPLIB_INT16) && firIntTcSupported(a))
-      kind = hc->firQMode ? FIR_INT_Q_TC : FIR_INT_WRAP_TC;
-   // Split-BF16x3 covers up to 512 taps; longer filters run the FP32 CUDA-core kernel.
-   if (kind == FIR_F32_BF16X3 && !firBf16x3Supported(a)) kind = FIR_F32_SIMT;
+   const FirKernelKind kind = firKindOf(p, a);
+   firApplyChoice(a, kind, firChoice(p, a, kind));
    if (!pc) {
       if ((e = injectCheck(launchFir(a, kind, s))) != cudaSuccess) return cudaFail(hc, e, "FIR kernel launch");
       if ((e = injectCheck(regionOut(rout, s))) != cudaSuccess) return cudaFail(hc, e, "copy output");

@@ -39,6 +39,9 @@
 // and fetches each item's first segment during the previous item's last tile.
 // All waits on the tensor core are bounded; on expiry the kernel sets the error word it
 // was given (the calling handle's or plan's), frees its TMEM and exits.
+#include <algorithm>
+#include <cstdio>
+
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -447,14 +450,18 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 2 ? 6 : 8) fir_int_tc_k
    if (warp == 0) tc::tmemFree(tmem, kCols);
 }
 
-// Tiles per CTA: a whole channel when there are enough channels to fill the
-// GPU several times over, else split so that at least ~2 waves of CTAs exist.
+// Tiles per CTA (the built-in rule, when the autotuner has no entry): a whole channel
+// when there are enough channels to fill the GPU several times over, else split so that
+// at least ~2 waves of CTAs exist.
 inline int tilesPerCtaFor(int nt, int batch, int ctasPerSm)
 {
+   const long long sms = deviceSms() > 0 ? deviceSms() : 148;
    int tpc = nt;
-   while (tpc > 1 && (long long) ((nt + tpc - 1) / tpc) * batch < 148LL * ctasPerSm * 2) tpc = (tpc + 1) / 2;
+   while (tpc > 1 && (long long) ((nt + tpc - 1) / tpc) * batch < sms * ctasPerSm * 2) tpc = (tpc + 1) / 2;
    return tpc;
 }
+
+template <typename T> constexpr int intLaunchBound() { return sizeof(T) == 2 ? 6 : 8; }
 
 template <typename T, int QMODE> cudaError_t launchIntTc(const FirLaunch &a, cudaStream_t s)
 {
@@ -468,17 +475,14 @@ template <typename T, int QMODE> cudaError_t launchIntTc(const FirLaunch &a, cud
    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
    if (e != cudaSuccess) return e;
    const int nt = (a.outSize + kTile - 1) / kTile;
-   const int tpc = tilesPerCtaFor(nt, a.batch, 8);
+   const int tpc = a.tuneTpc > 0 ? (a.tuneTpc < nt ? a.tuneTpc : nt) : tilesPerCtaFor(nt, a.batch, 8);
    const long long items = (long long) a.batch * ((nt + tpc - 1) / tpc);
    // persistent: one wave of resident CTAs striding over the work items (CTAs per SM: the
-   // launch bound, or fewer when shared memory runs out first)
+   // autotuner's choice or the launch bound, fewer when shared memory runs out first)
    const int bySmem = (int) ((228u * 1024u) / (smem + 1024u));
-   const int perSm = (SPLIT ? 6 : 8) < bySmem ? (SPLIT ? 6 : 8) : bySmem;
-   int sms = 148;
-   {
-      int dev = 0;
-      if (cudaGetDevice(&dev) == cudaSuccess) (void) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-   }
+   const int want = a.tunePerSm > 0 ? a.tunePerSm : intLaunchBound<T>();
+   const int perSm = want < bySmem ? want : bySmem;
+   const int sms = deviceSms() > 0 ? deviceSms() : 148;
    const long long wave = (long long) (perSm > 0 ? perSm : 1) * sms;
    const int grid = (int) (items < wave ? items : wave);
    FirLaunch k = a;
@@ -1186,7 +1190,7 @@ cudaError_t launchFirBf16x3(const FirLaunch &a, cudaStream_t s)
        cudaFuncSetAttribute(fir_bf16x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
    if (e != cudaSuccess) return e;
    const int nt = (a.outSize + kBfTile - 1) / kBfTile;
-   const int tpc = tilesPerCtaFor(nt, a.batch, 1);
+   const int tpc = a.tuneTpc > 0 ? (a.tuneTpc < nt ? a.tuneTpc : nt) : tilesPerCtaFor(nt, a.batch, 1);
    dim3 grid((nt + tpc - 1) / tpc, a.batch < 65535 ? a.batch : 65535);
    fir_bf16x3_tc_kernel<<<grid, kBfBlock, smem, s>>>(a, tpc);
    countLaunch();
@@ -1208,6 +1212,54 @@ cudaError_t launchFirBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int
    fir_bf16x3_ragged_kernel<<<grid, kBfBlock, smem, s>>>(chans, runs, nRuns, in, taps, out, dx ? 1 : 0, Tmax, err);
    countLaunch();
    return cudaGetLastError();
+}
+
+std::string firTuneKey(const FirLaunch &a, FirKernelKind kind)
+{
+   char buf[160];
+   if (kind == FIR_F32_BF16X3 && firBf16x3Supported(a)) {
+      const int nt = (a.outSize + kBfTile - 1) / kBfTile;
+      snprintf(buf, sizeof(buf), "fir_bf16x3|T=%d|tiles=2^%d|batch=2^%d|nch=%d|sms=%d", a.T, tuneClass(nt),
+               tuneClass(a.batch), a.filtPitch ? 1 : 0, deviceSms());
+      return buf;
+   }
+   if ((kind == FIR_INT_WRAP_TC || kind == FIR_INT_Q_TC) && firIntTcSupported(a)) {
+      const int nt = (a.outSize + kTile - 1) / kTile;
+      snprintf(buf, sizeof(buf), "fir_int|dtype=%d|q=%d|T=%d|tiles=2^%d|batch=2^%d|sms=%d", a.dtype,
+               kind == FIR_INT_Q_TC ? 1 : 0, a.T, tuneClass(nt), tuneClass(a.batch), deviceSms());
+      return buf;
+   }
+   return std::string();
+}
+
+// bf16x3: the choice is the tiles per CTA; int: tiles per CTA * 16 + CTAs per SM.
+std::vector<int> firTuneCandidates(const FirLaunch &a, FirKernelKind kind)
+{
+   std::vector<int> c;
+   if (firTuneKey(a, kind).empty()) return c;
+   if (kind == FIR_F32_BF16X3) {
+      const int nt = (a.outSize + kBfTile - 1) / kBfTile;
+      for (int t = 1; t < 2 * nt && t <= 64; t *= 2) c.push_back(t < nt ? t : nt);
+   }
+   else {
+      const int nt = (a.outSize + kTile - 1) / kTile;
+      const int bound = a.dtype == DSPLIB_INT16 ? intLaunchBound<int16_t>() : intLaunchBound<int8_t>();
+      for (int t = 1; t < 2 * nt && t <= 64; t *= 4)
+         for (int per = 2; per <= bound; per += 2) c.push_back((t < nt ? t : nt) * 16 + per);
+   }
+   std::sort(c.begin(), c.end());
+   c.erase(std::unique(c.begin(), c.end()), c.end());
+   return c;
+}
+
+void firApplyChoice(FirLaunch &a, FirKernelKind kind, int choice)
+{
+   if (choice <= 0) return;
+   if (kind == FIR_F32_BF16X3) a.tuneTpc = choice;
+   else if (kind == FIR_INT_WRAP_TC || kind == FIR_INT_Q_TC) {
+      a.tuneTpc = choice / 16;
+      a.tunePerSm = choice % 16;
+   }
 }
 
 cudaError_t launchFirDhBf16x3Ragged(const RaggedChan *chans, const int4 *runs, int nRuns, const float *x,

@@ -35,7 +35,9 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "dsplib_internal.h"
@@ -224,8 +226,11 @@ using namespace dsplib;
 
 extern "C" {
 
-DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t numChannels, const int32_t *length,
-                                          const int32_t *taps, const int32_t *stages)
+// Plan with FIR work lists of runs of up to runTiles tiles (forward and input gradient;
+// the taps gradient keeps kFirBfRunTiles, so its partial sums, and with them its
+// rounding, do not depend on the choice).
+static DSPLIB_STATUS raggedPlanBuild(DSPLIB_gpu_raggedPlan *plan, int32_t numChannels, const int32_t *length,
+                                     const int32_t *taps, const int32_t *stages, int runTiles)
 {
    if (!plan || !length || !taps || !stages || numChannels <= 0) return DSPLIB_ERR_NULL_POINTER;
    *plan = nullptr;
@@ -235,10 +240,10 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    std::vector<int2> fwd, units;
    std::vector<int4> firFwd, firDx, dhRuns;
    std::vector<int> start(numChannels + 1);
-   // runs of up to kFirBfRunTiles consecutive 8192-output tiles of one channel
-   auto addRuns = [](std::vector<int4> &runs, int c, int outLen) {
+   // runs of up to runTiles consecutive 8192-output tiles of one channel
+   auto addRuns = [runTiles](std::vector<int4> &runs, int c, int outLen) {
       const int tiles = (outLen + kFirBfTile - 1) / kFirBfTile;
-      for (int t = 0; t < tiles; t += kFirBfRunTiles) runs.push_back(make_int4(c, t, std::min(kFirBfRunTiles, tiles - t), 0));
+      for (int t = 0; t < tiles; t += runTiles) runs.push_back(make_int4(c, t, std::min(runTiles, tiles - t), 0));
    };
    long long xo = 0, ho = 0, co = 0, po = 0, ck = 0, ph = 0, gr = 0;
    for (int c = 0; c < numChannels; c++) {
@@ -324,6 +329,87 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t n
    }
    *plan = (DSPLIB_gpu_raggedPlan) p;
    return DSPLIB_SUCCESS;
+}
+
+// Autotuner key of a bank's FIR run length, and its candidates.
+static std::string bankRunsKey(int C, const int32_t *length, const int32_t *taps)
+{
+   long long total = 0;
+   int Tmax = 0;
+   for (int c = 0; c < C; c++) {
+      total += length[c];
+      Tmax = std::max(Tmax, (int) taps[c]);
+   }
+   char buf[128];
+   snprintf(buf, sizeof(buf), "bank_runs|ch=2^%d|samples=2^%d|Tmax=%d|sms=%d", tuneClass(C), tuneClass(total),
+            Tmax, deviceSms());
+   return buf;
+}
+
+// Time the forward FIR over zero-filled scratch with work lists of each candidate run
+// length; the fastest is stored under key.
+static void bankRunsMeasure(const RaggedPlan *p, const std::string &key)
+{
+   const int cands[] = {1, 2, 4, 8, 16};
+   float *x = nullptr, *h = nullptr, *u = nullptr;
+   std::vector<int4 *> lists;
+   std::vector<int> counts;
+   bool ok = cudaMalloc(&x, std::max<long long>(1, p->totalLen) * 4) == cudaSuccess &&
+             cudaMalloc(&h, std::max<long long>(1, p->totalTaps) * 4) == cudaSuccess &&
+             cudaMalloc(&u, std::max<long long>(1, p->planeStride) * 4) == cudaSuccess &&
+             cudaMemset(x, 0, std::max<long long>(1, p->totalLen) * 4) == cudaSuccess &&
+             cudaMemset(h, 0, std::max<long long>(1, p->totalTaps) * 4) == cudaSuccess;
+   for (int rt : cands) {
+      if (!ok) break;
+      std::vector<int4> runs;
+      for (int c = 0; c < p->C; c++) {
+         const int tiles = (p->hLen[c] - p->hTaps[c] + 1 + kFirBfTile - 1) / kFirBfTile;
+         for (int t = 0; t < tiles; t += rt) runs.push_back(make_int4(c, t, std::min(rt, tiles - t), 0));
+      }
+      std::stable_sort(runs.begin(), runs.end(), [](const int4 &a, const int4 &b) { return a.z > b.z; });
+      int4 *d = nullptr;
+      ok = upload(&d, runs) == cudaSuccess;
+      lists.push_back(d);
+      counts.push_back((int) runs.size());
+   }
+   if (ok) {
+      std::vector<int> cv(cands, cands + 5);
+      (void) tunePick(key, cv, [&](int rt, cudaStream_t s) {
+         int i = 0;
+         while (cands[i] != rt) i++;
+         return launchFirBf16x3Ragged(p->dChan, lists[i], counts[i], x, h, u, false, p->Tmax, p->err, s);
+      });
+   }
+   (void) cudaGetLastError();
+   for (int4 *d : lists) cudaFree(d);
+   cudaFree(x);
+   cudaFree(h);
+   cudaFree(u);
+   if (p->err) *(volatile int *) p->err = 0;
+}
+
+DSPLIB_STATUS DSPLIB_gpu_raggedPlanCreate(DSPLIB_gpu_raggedPlan *plan, int32_t numChannels, const int32_t *length,
+                                          const int32_t *taps, const int32_t *stages)
+{
+   if (!plan || !length || !taps || !stages || numChannels <= 0) return DSPLIB_ERR_NULL_POINTER;
+   const std::string key = bankRunsKey(numChannels, length, taps);
+   int runTiles = kFirBfRunTiles;
+   int c = 0;
+   const bool cached = tuneLookup(key, &c) && c >= 1 && c <= 64;
+   if (cached) runTiles = c;
+   DSPLIB_STATUS st = raggedPlanBuild(plan, numChannels, length, taps, stages, runTiles);
+   if (st != DSPLIB_SUCCESS || cached || tuneMode() != DSPLIB_GPU_TUNE_MEASURE) return st;
+   for (int i = 0; i < numChannels; i++)
+      if (taps[i] > kFirBfMaxTaps) return st;
+   bankRunsMeasure((RaggedPlan *) *plan, key);
+   if (tuneLookup(key, &c) && c != runTiles && c >= 1 && c <= 64) {
+      DSPLIB_gpu_raggedPlan better = nullptr;
+      if (raggedPlanBuild(&better, numChannels, length, taps, stages, c) == DSPLIB_SUCCESS) {
+         freePlan((RaggedPlan *) *plan);
+         *plan = better;
+      }
+   }
+   return st;
 }
 
 int64_t DSPLIB_gpu_raggedPlanSize(DSPLIB_gpu_raggedPlan plan, int32_t what)

@@ -70,6 +70,59 @@ DSPLIB_STATUS DSPLIB_gpu_injectFault(DSPLIB_kernelHandle handle, int32_t operati
 /** Number of CUDA kernels this library has launched in this process. */
 int64_t DSPLIB_gpu_kernelLaunchCount(void);
 
+/* ---------------------------------------------------------------------------
+ * Autotuner of launch shapes.  The reference picks its kernel variants by fixed
+ * size classes in init (src/DSPLIB_fir/DSPLIB_fir_ci.cpp:350-405,
+ * src/DSPLIB_cascadeBiquad/DSPLIB_cascadeBiquad.cpp:480-615); this library keeps a
+ * measured choice per problem class and GPU instead, where a kernel has shapes to
+ * choose from:
+ *   fir_bf16x3  output tiles per CTA of the split-BF16x3 FIR;
+ *   fir_int     output tiles per CTA and resident CTAs per SM of the int8/int16 FIR;
+ *   bq_scan     warps per CTA (the 32-sample chunks of one window: its length) and
+ *               CTAs per cluster of the cascade-biquad scan;
+ *   bank_runs   output tiles per run of the batched filter bank's FIR work lists.
+ * Keys are text: "<op>|<parameter>=<value>|...|sms=<SM count>"; lengths, batch sizes
+ * and channel counts enter as power-of-two classes ("2^k"), taps, stages, form and
+ * data type exactly.  A choice is one integer (see DSPLIB_gpu_autotuneHandleKey).
+ * Entries are process-wide, read from and written to a JSON cache file:
+ *   {"format": "dsplib_b200 autotune 1", "entries": {"<key>": <choice>, ...}}
+ * The environment variables DSPLIB_GPU_TUNE_CACHE (the file) and DSPLIB_GPU_AUTOTUNE
+ * (the mode) give the initial settings.  Choices never change results beyond the
+ * floating-point summation order of the cascade scan's cluster carry.
+ * ------------------------------------------------------------------------- */
+typedef enum {
+   DSPLIB_GPU_TUNE_OFF = 0,     /* built-in rules only */
+   DSPLIB_GPU_TUNE_CACHED = 1,  /* default: a cached choice where one exists, else the rule */
+   DSPLIB_GPU_TUNE_MEASURE = 2, /* as CACHED; a class without an entry is timed (every
+                                   candidate on scratch buffers of the problem's shape) when a
+                                   handle is initialised or a plan is built, the fastest kept
+                                   and the cache file rewritten */
+} DSPLIB_gpu_tuneMode;
+
+DSPLIB_STATUS DSPLIB_gpu_autotuneSetMode(int32_t mode);
+int32_t DSPLIB_gpu_autotuneGetMode(void);
+/** Cache file (NULL or "": none); entries it holds are merged into the table. */
+DSPLIB_STATUS DSPLIB_gpu_autotuneSetCachePath(const char *path);
+/** Write the table to the cache file (DSPLIB_ERR_INVALID_VALUE when none is set). */
+DSPLIB_STATUS DSPLIB_gpu_autotuneSave(void);
+/** Forget every entry (the file is left as it is). */
+DSPLIB_STATUS DSPLIB_gpu_autotuneClear(void);
+/** The entry for key, or -1. */
+int32_t DSPLIB_gpu_autotuneLookup(const char *key);
+/** Set an entry (pins a choice; not written to the file until DSPLIB_gpu_autotuneSave). */
+DSPLIB_STATUS DSPLIB_gpu_autotuneStore(const char *key, int32_t choice);
+/** Number of entries. */
+int32_t DSPLIB_gpu_autotuneCount(void);
+/** Time the candidates of an initialised FIR or cascade-biquad handle's configuration now
+ *  (as MEASURE mode does in init) and store the fastest; DSPLIB_ERR_NOT_IMPLEMENTED when
+ *  its kernel has no shapes to choose from. */
+DSPLIB_STATUS DSPLIB_gpu_autotune(DSPLIB_kernelHandle handle);
+/** The tuning key of an initialised handle's configuration (copied into buf, at most len
+ *  bytes with the terminator) and the number of candidate choices (0: nothing to tune). */
+int32_t DSPLIB_gpu_autotuneHandleKey(DSPLIB_kernelHandle handle, char *buf, int32_t len);
+/** Candidate i (0 <= i < the count above) of that key, or -1. */
+int32_t DSPLIB_gpu_autotuneHandleCandidate(DSPLIB_kernelHandle handle, int32_t i);
+
 /** End of a handle's life (the reference API has no destructor: callers free
  *  the handle memory themselves).  Waits for work an asynchronous exec queued
  *  on the handle's stream, then marks the handle uninitialised so later calls
