@@ -656,6 +656,7 @@ for _k, _n, _c in (("fltoq15", 64 << 20, 2), ("q15tofl", 64 << 20, 2), ("interle
                    ("deinterleave", 16 << 20, 2), ("addnch", 1 << 20, 16)):
     WORKLOADS[stream_name(_k, _n, _c, 12)] = (lambda k=_k, n=_n, c=_c: StreamWorkload(k, n, channels=c))
 DEFAULT = "fir_biquad_bank_2048ch_ragged"
+TUNE_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "c7x_dsplib_b200", "tune_b200.json")
 
 
 # ----------------------------------------------------------- clocks
@@ -769,6 +770,10 @@ def main():
     ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune-cache", default=None,
+                    help="autotuner cache file (default: $DSPLIB_GPU_TUNE_CACHE, else the package's tune_b200.json)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="measure launch shapes missing from the cache at set-up and save them to it")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
@@ -786,6 +791,16 @@ def main():
     import c7x_dsplib_b200 as D
 
     torch.cuda.set_device(local)
+    # launch shapes measured on this GPU model by the library's autotuner (CACHED mode:
+    # problem classes without an entry keep the built-in rules)
+    tune = a.tune_cache or os.environ.get("DSPLIB_GPU_TUNE_CACHE") or TUNE_CACHE
+    shapes = "built-in rules"
+    if tune and (os.path.exists(tune) or a.autotune):
+        D.lib().DSPLIB_gpu_autotuneSetCachePath(tune.encode())
+        shapes = f"autotuner cache {os.path.basename(tune)}" + (" (measured in this run where missing)" if a.autotune
+                                                                 else "")
+    if a.autotune:
+        D.lib().DSPLIB_gpu_autotuneSetMode(2)
     dist = None
     if world > 1:
         import datetime
@@ -909,7 +924,7 @@ def main():
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic (seeded)",
                 "config": dict(wl.config(), l2="flushed between steps (256 MiB write outside the timed events)",
-                               parallelism=f"channel blocks x{world}, no collective"),
+                               parallelism=f"channel blocks x{world}, no collective", launch_shapes=shapes),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
         print(json.dumps(line))
     if dist:

@@ -206,7 +206,11 @@ int deviceSms()
    return sms;
 }
 
-float tuneTime(const std::function<cudaError_t(cudaStream_t)> &launch, cudaStream_t s, int reps)
+// L2 flush between timed launches: a write larger than the L2 cache, outside the events,
+// so that every candidate reads its inputs from HBM as a call in a pipeline does.
+constexpr size_t kFlushBytes = 256u << 20;
+
+float tuneTime(const std::function<cudaError_t(cudaStream_t)> &launch, cudaStream_t s, int reps, void *flush)
 {
    cudaEvent_t e0 = nullptr, e1 = nullptr;
    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
@@ -218,7 +222,8 @@ float tuneTime(const std::function<cudaError_t(cudaStream_t)> &launch, cudaStrea
    bool ok = launch(s) == cudaSuccess && cudaStreamSynchronize(s) == cudaSuccess; // warm-up
    std::vector<float> times;
    for (int r = 0; ok && r < reps; r++) {
-      ok = cudaEventRecord(e0, s) == cudaSuccess && launch(s) == cudaSuccess && cudaEventRecord(e1, s) == cudaSuccess &&
+      ok = (!flush || cudaMemsetAsync(flush, r & 0xff, kFlushBytes, s) == cudaSuccess) &&
+           cudaEventRecord(e0, s) == cudaSuccess && launch(s) == cudaSuccess && cudaEventRecord(e1, s) == cudaSuccess &&
            cudaEventSynchronize(e1) == cudaSuccess;
       float ms = 0.0f;
       if (ok && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) times.push_back(ms);
@@ -242,16 +247,22 @@ int tunePick(const std::string &key, const std::vector<int> &cands,
       (void) cudaGetLastError();
       return -1;
    }
+   void *flush = nullptr;
+   if (cudaMalloc(&flush, kFlushBytes) != cudaSuccess) {
+      (void) cudaGetLastError();
+      flush = nullptr;
+   }
    int best = -1;
    float bestMs = 0.0f;
    for (int c : cands) {
-      const float ms = tuneTime([&](cudaStream_t st) { return launch(c, st); }, s, 3);
+      const float ms = tuneTime([&](cudaStream_t st) { return launch(c, st); }, s, 5, flush);
       if (ms >= 0.0f && (best < 0 || ms < bestMs)) {
          best = c;
          bestMs = ms;
       }
    }
    (void) cudaStreamSynchronize(s);
+   if (flush) cudaFree(flush);
    cudaStreamDestroy(s);
    (void) cudaGetLastError();
    if (best >= 0) tuneStore(key, best, true);

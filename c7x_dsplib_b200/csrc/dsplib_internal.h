@@ -107,8 +107,9 @@ void tuneStore(const std::string &key, int choice, bool save);
 // Power-of-two class of v (smallest c with 2^c >= v), and the current device's SM count.
 int tuneClass(long long v);
 int deviceSms();
-// Median of `reps` event-timed launches after one warm-up (ms; negative on failure).
-float tuneTime(const std::function<cudaError_t(cudaStream_t)> &launch, cudaStream_t s, int reps);
+// Median of `reps` event-timed launches after one warm-up (ms; negative on failure), the
+// L2 cache flushed through `flush` (256 MiB, or null) before each.
+float tuneTime(const std::function<cudaError_t(cudaStream_t)> &launch, cudaStream_t s, int reps, void *flush);
 // Time every candidate on a private stream, store the fastest under key (and rewrite the
 // cache file); returns it, or -1 when nothing could be timed.
 int tunePick(const std::string &key, const std::vector<int> &cands,

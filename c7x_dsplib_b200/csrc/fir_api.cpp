@@ -78,13 +78,32 @@ FirLaunch firShape(const FirPriv *p)
    return a;
 }
 
+// Whether the handle's stream is being captured into a graph (no measurement then).
+bool capturing(cudaStream_t s)
+{
+   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
+      (void) cudaGetLastError();
+      return true;
+   }
+   return cs != cudaStreamCaptureStatusNone;
+}
+
 // The handle's cached autotuner choice for kind, resolved again when the table changed.
+// In MEASURE mode a class still without an entry (settings changed after init: precision,
+// Q mode) is measured here, on scratch buffers, before the call's own launch.
+int firChoice(FirPriv *p, const FirLaunch &a, FirKernelKind kind);
+DSPLIB_STATUS firMeasureFor(FirPriv *p);
+
 int firChoice(FirPriv *p, const FirLaunch &a, FirKernelKind kind)
 {
    const unsigned gen = tuneGeneration();
    if (p->tuneGen != gen || p->tuneKind != (int32_t) kind) {
       int c = -1;
       const std::string key = firTuneKey(a, kind);
+      if (!key.empty() && !tuneLookup(key, &c) && tuneMode() == DSPLIB_GPU_TUNE_MEASURE &&
+          !capturing(p->common.stream))
+         (void) firMeasureFor(p);
       if (key.empty() || !tuneLookup(key, &c)) c = -1;
       p->tuneGen = gen;
       p->tuneKind = (int32_t) kind;
@@ -92,6 +111,8 @@ int firChoice(FirPriv *p, const FirLaunch &a, FirKernelKind kind)
    }
    return p->tuneChoice;
 }
+
+DSPLIB_STATUS firMeasureFor(FirPriv *p) { return firHandleTune((DSPLIB_kernelHandle) p); }
 
 } // namespace
 
