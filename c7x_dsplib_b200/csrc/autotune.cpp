@@ -238,6 +238,19 @@ float tuneTime(const std::function<cudaError_t(cudaStream_t)> &launch, cudaStrea
    return best;
 }
 
+bool tuneFill(void *p, size_t bytes, bool asFloat)
+{
+   cudaStream_t s = nullptr;
+   if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      (void) cudaGetLastError();
+      return false;
+   }
+   const bool ok = launchTuneFill(p, bytes, asFloat, s) == cudaSuccess && cudaStreamSynchronize(s) == cudaSuccess;
+   cudaStreamDestroy(s);
+   (void) cudaGetLastError();
+   return ok;
+}
+
 int tunePick(const std::string &key, const std::vector<int> &cands,
              const std::function<cudaError_t(int, cudaStream_t)> &launch)
 {

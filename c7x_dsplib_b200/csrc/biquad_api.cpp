@@ -102,8 +102,9 @@ std::string biquadHandleTuneKey(DSPLIB_kernelHandle h, std::vector<int> *cands)
    return biquadTuneKey(a);
 }
 
-// Every candidate shape on zero-filled scratch signals, states and coefficients of the
-// handle's sizes (the scan's time does not depend on the values), on a private stream.
+// Every candidate shape on a scratch signal of the handle's sizes filled with a hashed
+// pattern, zero states and coefficients (the scan's work does not depend on them), on a
+// private stream.
 DSPLIB_STATUS biquadHandleTune(DSPLIB_kernelHandle h)
 {
    BiquadPriv *p = bqHandle(h);
@@ -119,8 +120,8 @@ DSPLIB_STATUS biquadHandleTune(DSPLIB_kernelHandle h)
    void *x = nullptr, *y = nullptr, *st = nullptr, *cf = nullptr;
    DSPLIB_STATUS status = DSPLIB_ERR_FAILURE;
    if (cudaMalloc(&x, xb) == cudaSuccess && cudaMalloc(&y, xb) == cudaSuccess && cudaMalloc(&st, sb) == cudaSuccess &&
-       cudaMalloc(&cf, cb) == cudaSuccess && cudaMemset(x, 0, xb) == cudaSuccess &&
-       cudaMemset(st, 0, sb) == cudaSuccess && cudaMemset(cf, 0, cb) == cudaSuccess) {
+       cudaMalloc(&cf, cb) == cudaSuccess && tuneFill(x, xb, true) && cudaMemset(st, 0, sb) == cudaSuccess &&
+       cudaMemset(cf, 0, cb) == cudaSuccess) {
       a.x = (const float *) x;
       a.y = (float *) y;
       a.state = (float *) st;

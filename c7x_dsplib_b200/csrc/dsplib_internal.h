@@ -110,6 +110,10 @@ int deviceSms();
 // Median of `reps` event-timed launches after one warm-up (ms; negative on failure), the
 // L2 cache flushed through `flush` (256 MiB, or null) before each.
 float tuneTime(const std::function<cudaError_t(cudaStream_t)> &launch, cudaStream_t s, int reps, void *flush);
+// Fill scratch with a hashed pattern (tune_fill.cu): floats in [-0.5, 0.5) or raw bits.
+cudaError_t launchTuneFill(void *p, size_t bytes, bool asFloat, cudaStream_t s);
+// The same on a private stream, waited for.
+bool tuneFill(void *p, size_t bytes, bool asFloat);
 // Time every candidate on a private stream, store the fastest under key (and rewrite the
 // cache file); returns it, or -1 when nothing could be timed.
 int tunePick(const std::string &key, const std::vector<int> &cands,

@@ -128,8 +128,8 @@ std::string firHandleTuneKey(DSPLIB_kernelHandle h, std::vector<int> *cands)
    return firTuneKey(a, kind);
 }
 
-// Every candidate on zero-filled scratch buffers of the handle's shape (the kernels'
-// time does not depend on the values), on a private stream; the fastest is stored.
+// Every candidate on scratch buffers of the handle's shape filled with a hashed
+// pattern, on a private stream; the fastest is stored.
 DSPLIB_STATUS firHandleTune(DSPLIB_kernelHandle h)
 {
    FirPriv *p = firHandle(h);
@@ -145,7 +145,7 @@ DSPLIB_STATUS firHandleTune(DSPLIB_kernelHandle h)
    void *x = nullptr, *hh = nullptr, *y = nullptr;
    DSPLIB_STATUS st = DSPLIB_ERR_FAILURE;
    if (cudaMalloc(&x, xb) == cudaSuccess && cudaMalloc(&hh, hb) == cudaSuccess && cudaMalloc(&y, yb) == cudaSuccess &&
-       cudaMemset(x, 0, xb) == cudaSuccess && cudaMemset(hh, 0, hb) == cudaSuccess) {
+       tuneFill(x, xb, p->dtype == DSPLIB_FLOAT32) && tuneFill(hh, hb, p->dtype == DSPLIB_FLOAT32)) {
       a.x = x;
       a.h = hh;
       a.y = y;

@@ -1237,15 +1237,23 @@ std::vector<int> firTuneCandidates(const FirLaunch &a, FirKernelKind kind)
 {
    std::vector<int> c;
    if (firTuneKey(a, kind).empty()) return c;
+   // tiles per CTA: powers of two up to a whole channel, and the built-in rule's value
+   auto tileCounts = [](int nt, int rule) {
+      std::vector<int> t;
+      for (int v = 1; v < nt && v <= 64; v *= 2) t.push_back(v);
+      t.push_back(nt < 64 ? nt : 64);
+      t.push_back(rule);
+      return t;
+   };
    if (kind == FIR_F32_BF16X3) {
       const int nt = (a.outSize + kBfTile - 1) / kBfTile;
-      for (int t = 1; t < 2 * nt && t <= 64; t *= 2) c.push_back(t < nt ? t : nt);
+      c = tileCounts(nt, tilesPerCtaFor(nt, a.batch, 1));
    }
    else {
       const int nt = (a.outSize + kTile - 1) / kTile;
       const int bound = a.dtype == DSPLIB_INT16 ? intLaunchBound<int16_t>() : intLaunchBound<int8_t>();
-      for (int t = 1; t < 2 * nt && t <= 64; t *= 4)
-         for (int per = 2; per <= bound; per += 2) c.push_back((t < nt ? t : nt) * 16 + per);
+      for (int t : tileCounts(nt, tilesPerCtaFor(nt, a.batch, 8)))
+         for (int per = 4; per <= bound; per += 2) c.push_back(t * 16 + per);
    }
    std::sort(c.begin(), c.end());
    c.erase(std::unique(c.begin(), c.end()), c.end());

@@ -346,7 +346,7 @@ static std::string bankRunsKey(int C, const int32_t *length, const int32_t *taps
    return buf;
 }
 
-// Time the forward FIR over zero-filled scratch with work lists of each candidate run
+// Time the forward FIR over scratch filled with a hashed pattern, with work lists of each candidate run
 // length; the fastest is stored under key.
 static void bankRunsMeasure(const RaggedPlan *p, const std::string &key)
 {
@@ -357,8 +357,8 @@ static void bankRunsMeasure(const RaggedPlan *p, const std::string &key)
    bool ok = cudaMalloc(&x, std::max<long long>(1, p->totalLen) * 4) == cudaSuccess &&
              cudaMalloc(&h, std::max<long long>(1, p->totalTaps) * 4) == cudaSuccess &&
              cudaMalloc(&u, std::max<long long>(1, p->planeStride) * 4) == cudaSuccess &&
-             cudaMemset(x, 0, std::max<long long>(1, p->totalLen) * 4) == cudaSuccess &&
-             cudaMemset(h, 0, std::max<long long>(1, p->totalTaps) * 4) == cudaSuccess;
+             tuneFill(x, std::max<long long>(1, p->totalLen) * 4, true) &&
+             tuneFill(h, std::max<long long>(1, p->totalTaps) * 4, true);
    for (int rt : cands) {
       if (!ok) break;
       std::vector<int4> runs;
