@@ -148,3 +148,32 @@ def test_filter_bank_full_size():
         assert rel(gx[xo[k]:xo[k + 1]], gx64) <= 1e-4, what
         assert rel(gh[ho[k]:ho[k + 1]], gh64) <= 1e-4, what
         assert rel(gc[co[k]:co[k + 1]], gc64.reshape(-1)) <= 1e-4, what
+
+
+@pytest.mark.parametrize("form", [D.DF1, D.DF2, D.TDF2, D.TIF])
+@pytest.mark.parametrize("nch", [0, 1])
+def test_biquad_second_configuration_flat_bound(form, nch):
+    """The second benchmark configuration exactly (32 ch x 8192 x 4 stages, poles of radius
+    U[0.5, 0.95], zero pairs on the unit circle, sections normalised to unit gain at the
+    pole angle, input N(0, 1), zero state), every form and both coefficient layouts: every
+    channel's output within a flat 1e-4 of its peak against FP64 (no allowance for the
+    sequential FP32 recursion's own error), final states too (TIF: outputs only, its state
+    is in the transformed coordinates)."""
+    from test_biquad_gpu import stable_sections
+
+    rng = np.random.default_rng(200 + 2 * form + nch)
+    N, C, S = 8192, 32, 4
+    x = rng.standard_normal((N, C)).astype(np.float32)
+    nat = stable_sections(rng, C if nch else 1, S, rmax=0.95)
+    opt, _ = D.opt_coefficients(nat, form, nch, C)
+    nv = 4 if form == D.DF1 else 2
+    sd = dev(np.zeros((S * nv, C), np.float32))
+    y = host(D.cascade_biquad(dev(x), dev(opt), sd, form=form, nch=nch)).astype(np.float64)
+    f64 = D.DF2 if form == D.TIF else form
+    s64 = np.zeros((S * (4 if f64 == D.DF1 else 2), C), np.float64)
+    y64 = oracle.biquad_f64(f64, x, nat, s64, nch=nch)
+    err = np.max(np.abs(y - y64), axis=0) / np.max(np.abs(y64), axis=0)
+    assert np.max(err) <= 1e-4, float(np.max(err))
+    if form != D.TIF:
+        st = host(sd).astype(np.float64)
+        assert np.max(np.abs(st - s64)) <= 1e-4 * max(1.0, float(np.max(np.abs(s64))))
