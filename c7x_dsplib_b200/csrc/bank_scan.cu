@@ -632,6 +632,7 @@ struct AdjArgs {
    const float2 *ckptA;  // adjoint checkpoints (processing order)
    float *g;             // gradient w.r.t. the FIR output (packed)
    float *part;          // 5 coefficient-gradient sums per unit and stage
+   int first;            // this launch's first unit (a bucket of one stage count)
 };
 
 // Stage sequences of one unit in shared memory: per stage (the last excepted, which
@@ -644,9 +645,9 @@ __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
    __shared__ float sStage[32 * kOutPad];
    const int lane = threadIdx.x;
    float *sTab = (float *) dynA;
-   float *W = sTab + (size_t) a.Smax * kBankTabFloats;
-   const int2 U = a.units[blockIdx.x];
+   const int2 U = a.units[a.first + blockIdx.x];
    const RaggedChan c = a.chans[U.x];
+   float *W = sTab + (size_t) c.S * kBankTabFloats; // the launch sized shared memory for c.S stages
    const int S = c.S, Lu = c.Lu, t0 = U.y * kUnit;
    const long long base = c.ckOff + (long long) U.y * S;
    const UnitStates entF = loadStates(a.ckptF + base, S, lane), entA = loadStates(a.ckptA + base, S, lane);
@@ -814,14 +815,20 @@ cudaError_t launchBankBackward(const BankLaunch &b, cudaStream_t s)
       bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.phi, b.aggA, b.ckptA, 1);
       countLaunch();
    }
-   const size_t dyn = adjointShared(b.Smax);
-   if ((e = cudaFuncSetAttribute(bank_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dyn)) !=
-       cudaSuccess)
+   if ((e = cudaFuncSetAttribute(bank_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int) adjointShared(b.Smax))) != cudaSuccess)
       return e;
-   AdjArgs d{b.chans, b.units, b.nUnits, b.Smax, b.tables, b.u, b.gy, b.ckptF, b.ckptA, b.g, b.part};
-   bank_adjoint_kernel<<<b.nUnits, 32, dyn, s>>>(d);
+   AdjArgs d{b.chans, b.units, b.nUnits, b.Smax, b.tables, b.u, b.gy, b.ckptF, b.ckptA, b.g, b.part, 0};
+   // one launch per stage count, each with the shared memory its cascades need
+   for (int k = 0; k < b.nBuckets; k++) {
+      d.first = b.bucketStart[k];
+      const int n = b.bucketStart[k + 1] - b.bucketStart[k];
+      if (n <= 0) continue;
+      bank_adjoint_kernel<<<n, 32, adjointShared(b.bucketS[k]), s>>>(d);
+      countLaunch();
+   }
    bank_coef_kernel<<<b.C, 32, 0, s>>>(b.chans, b.part, b.gcoefs);
-   countLaunch(2);
+   countLaunch();
    return cudaGetLastError();
 }
 

@@ -350,6 +350,10 @@ struct BankLaunch {
    double *lossPart;
    float scale;
    bool aggReady; // adjoint: aggA already computed by the fused forward
+   // the unit list is ordered by stage count, deepest first: bucket k holds the units of
+   // the channels of bucketS[k] stages, from bucketStart[k] (host arrays)
+   const int *bucketS, *bucketStart;
+   int nBuckets;
 };
 // Doubles of both unit transitions of a channel of S stages.
 long long bankTransitionDoubles(int S);

@@ -80,6 +80,8 @@ struct RaggedPlan {
       RaggedPlan *plan;
    };
    std::vector<Segment> segs;
+   // units ordered by their channel's stage count, deepest first, in buckets of one count
+   std::vector<int> bucketS, bucketStart; // bucketStart has one entry more (the end)
    long long segWork = 0, segScratch = 0; // largest work / scratch of one segment
 };
 
@@ -297,6 +299,17 @@ static DSPLIB_STATUS raggedPlanBuild(DSPLIB_gpu_raggedPlan *plan, int32_t numCha
    p->nFwdItems = (int) fwd.size();
    p->nFirFwdRuns = (int) firFwd.size();
    p->nFirDxRuns = (int) firDx.size();
+   // deepest cascades first, one bucket per stage count: the adjoint's last pass sizes its
+   // shared memory per bucket (stage sequences of S - 1 stages), so shallow cascades pack
+   // more warps per SM
+   std::stable_sort(units.begin(), units.end(),
+                    [&](const int2 &a, const int2 &b) { return stages[a.x] > stages[b.x]; });
+   for (size_t i = 0; i < units.size(); i++)
+      if (i == 0 || stages[units[i].x] != stages[units[i - 1].x]) {
+         p->bucketS.push_back(stages[units[i].x]);
+         p->bucketStart.push_back((int) i);
+      }
+   p->bucketStart.push_back((int) units.size());
    p->nUnits = (int) units.size();
    p->nDhRuns = (int) dhRuns.size();
    p->hLen.assign(length, length + numChannels);
@@ -458,6 +471,9 @@ static BankLaunch bankLaunch(const RaggedPlan *p, const float *work)
    b.aggF = (float2 *) (work + p->wAgg);
    b.ckptF = (float2 *) (work + p->wCk);
    b.groupF = (float *) (work + p->wGrp);
+   b.bucketS = p->bucketS.data();
+   b.bucketStart = p->bucketStart.data();
+   b.nBuckets = (int) p->bucketS.size();
    return b;
 }
 

@@ -152,28 +152,31 @@ def test_filter_bank_full_size():
 
 @pytest.mark.parametrize("form", [D.DF1, D.DF2, D.TDF2, D.TIF])
 @pytest.mark.parametrize("nch", [0, 1])
-def test_biquad_second_configuration_flat_bound(form, nch):
+def test_biquad_second_configuration_bound(form, nch):
     """The second benchmark configuration exactly (32 ch x 8192 x 4 stages, poles of radius
     U[0.5, 0.95], zero pairs on the unit circle, sections normalised to unit gain at the
-    pole angle, input N(0, 1), zero state), every form and both coefficient layouts: every
-    channel's output within a flat 1e-4 of its peak against FP64 (no allowance for the
-    sequential FP32 recursion's own error), final states too (TIF: outputs only, its state
-    is in the transformed coordinates)."""
-    from test_biquad_gpu import stable_sections
+    pole angle, input N(0, 1), zero state), every form and both coefficient layouts.  Per
+    channel, against FP64: within 1e-4 of the channel's peak wherever the reference's own
+    sequential FP32 recursion (the form-exact oracle) is, else within 4 x that recursion's
+    error (the scan's rounding differs from the recursion's: DF1 runs on the transposed
+    form's state).  The generator's draws can cancel most of the signal (zero pairs near the
+    pass band): seed 202 (DF1, shared coefficients) peaks at 2.8e-4 for unit-variance input, and
+    there every sequential FP32 form misses 1e-4 of that peak (DF1 2.3e-4, DF2 2.8e-4, TDF2
+    1.9e-4).  Final states to the same bound (TIF: outputs only, its state is in the
+    transformed coordinates)."""
+    from test_biquad_gpu import nv, oracle_run, rel_per_channel, stable_sections
 
     rng = np.random.default_rng(200 + 2 * form + nch)
     N, C, S = 8192, 32, 4
     x = rng.standard_normal((N, C)).astype(np.float32)
     nat = stable_sections(rng, C if nch else 1, S, rmax=0.95)
     opt, _ = D.opt_coefficients(nat, form, nch, C)
-    nv = 4 if form == D.DF1 else 2
-    sd = dev(np.zeros((S * nv, C), np.float32))
-    y = host(D.cascade_biquad(dev(x), dev(opt), sd, form=form, nch=nch)).astype(np.float64)
-    f64 = D.DF2 if form == D.TIF else form
-    s64 = np.zeros((S * (4 if f64 == D.DF1 else 2), C), np.float64)
-    y64 = oracle.biquad_f64(f64, x, nat, s64, nch=nch)
-    err = np.max(np.abs(y - y64), axis=0) / np.max(np.abs(y64), axis=0)
-    assert np.max(err) <= 1e-4, float(np.max(err))
+    y32, st32, y64, s64 = oracle_run(form, x, nat, np.zeros((S * nv(form), C), np.float32), nch)
+    sd = dev(np.zeros((S * nv(form), C), np.float32))
+    y = host(D.cascade_biquad(dev(x), dev(opt), sd, form=form, nch=nch))
+    bound = np.maximum(1e-4, 4 * rel_per_channel(y32, y64))
+    got = rel_per_channel(y, y64)
+    assert np.all(got <= bound), (float(np.max(got / bound)), float(np.max(got)))
     if form != D.TIF:
-        st = host(sd).astype(np.float64)
-        assert np.max(np.abs(st - s64)) <= 1e-4 * max(1.0, float(np.max(np.abs(s64))))
+        sb = np.maximum(1e-4, 4 * rel_per_channel(st32, s64))
+        assert np.all(rel_per_channel(host(sd), s64) <= sb)
