@@ -1050,14 +1050,18 @@ __device__ __forceinline__ uint64_t descSw128Mn(uint32_t saddr, uint32_t lbo, ui
    return d;
 }
 
-__global__ void __launch_bounds__(kBfThreads, 1)
+// Warp roles as in the split-BF16x3 FIR: warps 0-15 stage tiles into the two buffers
+// (planesFull[b] when buffer b holds tile k) and form the diagonal sums at the end; warp 16
+// issues the MMAs (mmaDone[b] when tile k's MMAs, reading buffer b, completed).
+__global__ void __launch_bounds__(kBfBlock, 1)
     fir_dh_bf16x3_kernel(const RaggedChan *chans, const int4 *runs, const float *x, const float *gu, float *part,
                          int *err)
 {
    extern __shared__ __align__(16) unsigned char smraw[];
    unsigned char *sm = (unsigned char *) (((uintptr_t) smraw + 1023) & ~(uintptr_t) 1023);
-   uint64_t *mbar = (uint64_t *) (sm + 2 * kDhBuf); // one per buffer
-   uint32_t *tslot = (uint32_t *) (mbar + 2);
+   uint64_t *mbar = (uint64_t *) (sm + 2 * kDhBuf); // mmaDone, one per buffer
+   uint64_t *full = mbar + 2;                        // planesFull, one per buffer
+   uint32_t *tslot = (uint32_t *) (full + 2);
    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
    const int4 run = runs[blockIdx.x]; // {channel, first tile, tiles, partial slot}
    const RaggedChan c = chans[run.x];
@@ -1074,22 +1078,58 @@ __global__ void __launch_bounds__(kBfThreads, 1)
    };
    if (warp == 0) tc::tmemAlloc(tslot, 512);
    if (tid == 0) {
-      tc::mbarInit(mbar, 1);
-      tc::mbarInit(mbar + 1, 1);
+      for (int k = 0; k < 2; k++) {
+         tc::mbarInit(mbar + k, 1);
+         tc::mbarInit(full + k, 1);
+      }
       tc::fenceMbarInit();
    }
-   stage(run.y, 0);
-   tc::fenceProxyAsync();
    tc::fenceBeforeSync();
    __syncthreads();
    tc::fenceAfterSync();
    const uint32_t tmem = *tslot;
-   const uint32_t id = tc::idesc(1, 1, 1, kRows, 64) | (1u << 15) | (1u << 16); // both operands MN-major
-   uint32_t par = 0; // MMA barrier phase, one bit per buffer
-   bool ok = true;
-   for (int k = 0; k < run.z && ok; k++) {
-      const int b = k & 1;
-      if (tid == 0) {
+   bool fail = false;
+   if (tid < kBfWorkers) {
+      uint32_t par = 0; // mmaDone phase, one bit per buffer
+      for (int k = 0; k < run.z; k++) {
+         const int b = k & 1;
+         if (k >= 2) { // buffer b is free once tile k - 2's MMAs completed
+            const bool done = tid == 0 ? tc::mbarWait(mbar + b, (par >> b) & 1) : true;
+            par ^= 1u << b;
+            if (!done && tid == 0) raiseError(err);
+            if (tc::namedSyncOr(kBfBar, kBfWorkers, !done)) {
+               fail = true;
+               break;
+            }
+         }
+         stage(run.y + k, b);
+         tc::fenceProxyAsync();
+         tc::namedSync(kBfBar, kBfWorkers);
+         if (tid == 0) tc::mbarArrive(full + b);
+      }
+      // the last two tiles (bounded: after a failure, waits for tiles never issued give up)
+      for (int k = run.z >= 2 ? run.z - 2 : 0; !fail && k < run.z; k++) {
+         const int b = k & 1;
+         const bool done = tid == 0 ? tc::mbarWait(mbar + b, (par >> b) & 1) : true;
+         par ^= 1u << b;
+         if (!done && tid == 0) {
+            raiseError(err);
+            fail = true;
+         }
+      }
+   }
+   else if (tid == kBfWorkers) {
+      const uint32_t id = tc::idesc(1, 1, 1, kRows, 64) | (1u << 15) | (1u << 16); // both operands MN-major
+      uint32_t pf = 0;                                                               // planesFull phase per buffer
+      int commits = 0;
+      for (int k = 0; k < run.z; k++) {
+         const int b = k & 1;
+         if (!tc::mbarWait(full + b, (pf >> b) & 1)) {
+            raiseError(err);
+            fail = true;
+            break;
+         }
+         pf ^= 1u << b;
          tc::fenceAfterSync();
          unsigned char *B = buf(b);
          const uint32_t xh = tc::smemAddr(B), xl = tc::smemAddr(B + kDhXPlane);
@@ -1108,35 +1148,15 @@ __global__ void __launch_bounds__(kBfThreads, 1)
             }
          }
          tc::commit(mbar + b);
+         commits++;
       }
-      if (k + 1 < run.z) {
-         // the other buffer is free once the MMAs of the tile before this one completed
-         if (k >= 1) {
-            const bool done = tid == 0 ? tc::mbarWait(mbar + (1 - b), (par >> (1 - b)) & 1) : true;
-            par ^= 1u << (1 - b);
-            if (!done && tid == 0) raiseError(err);
-            ok = !__syncthreads_or(!done);
-            if (!ok) break;
-         }
-         stage(run.y + k + 1, 1 - b);
-         tc::fenceProxyAsync();
-         tc::fenceBeforeSync();
-         __syncthreads();
-      }
-   }
-   // The loop waited for tiles 0 .. n-3; wait for the last two (bounded: after a failure
-   // above, waits for tiles never issued give up, and the kernel returns).
-   bool fail = !ok;
-   for (int k = run.z >= 2 ? run.z - 2 : 0; k < run.z; k++) {
-      const int b = k & 1;
-      const bool done = tid == 0 ? tc::mbarWait(mbar + b, (par >> b) & 1) : true;
-      par ^= 1u << b;
-      if (!done && tid == 0) {
-         raiseError(err);
-         fail = true;
-      }
+      // after a failure: let the MMAs already committed finish before TMEM is released
+      // (tile n commits phase n / 2 of barrier n % 2)
+      if (fail)
+         for (int n = commits >= 2 ? commits - 2 : 0; n < commits; n++) (void) tc::mbarWait(mbar + (n & 1), (n >> 1) & 1);
    }
    if (__syncthreads_or(fail)) {
+      tc::fenceAfterSync();
       if (warp == 0) tc::tmemFree(tmem, 512);
       return;
    }
@@ -1145,7 +1165,7 @@ __global__ void __launch_bounds__(kBfThreads, 1)
    float acc = 0.0f;
    float *Ds = (float *) buf(0);
    for (int m = 0; m < Mt; m++) {
-      {
+      if (warp < 16) {
          const int quad = warp & 3, cg = warp >> 2; // TMEM lanes 32 quad.., columns 16 cg..
          uint32_t r[16];
          tc::tmemLoad16(tmem + ((uint32_t) (quad * 32) << 16) + 64 * m + 16 * cg, r);
@@ -1277,7 +1297,7 @@ cudaError_t launchFirDhBf16x3Ragged(const RaggedChan *chans, const int4 *runs, i
    cudaError_t e =
        cudaFuncSetAttribute(fir_dh_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kDhSmem);
    if (e != cudaSuccess) return e;
-   fir_dh_bf16x3_kernel<<<nRuns, kBfThreads, kDhSmem, s>>>(chans, runs, x, gu, part, err);
+   fir_dh_bf16x3_kernel<<<nRuns, kBfBlock, kDhSmem, s>>>(chans, runs, x, gu, part, err);
    countLaunch();
    return cudaGetLastError();
 }
