@@ -575,14 +575,19 @@ static DSPLIB_STATUS stepMseCore(RaggedPlan *p, const float *x, const float *tap
 
 // Input bytes (x and target) per segment of a host-buffer step.
 constexpr long long kStepSegmentBytes = 16LL << 20;
+// Segments of one host-buffer step.  The step moves its bytes over PCIe in both directions
+// at once; on B200 the 2048-channel bank took 15.7 ms with 8 segments and 16.3 ms with 16
+// (the link, about 75 GB/s both directions together, not the pipeline's ends, bounds it).
+// The pipeline's events are reused cyclically (a wait takes the event's state when queued).
+constexpr int kStepMaxSegments = 8;
 
-// Split the channels into up to kPipeMaxBlocks contiguous segments of about equal
+// Split the channels into up to kStepMaxSegments contiguous segments of about equal
 // samples, each with a plan of its own (on the plan's device, which is current).
 static bool buildSegments(RaggedPlan *p)
 {
    if (!p->segs.empty()) return true;
    const long long bytes = 8LL * p->totalLen;
-   int G = (int) std::min<long long>(kPipeMaxBlocks, std::max<long long>(1, (bytes + kStepSegmentBytes - 1) /
+   int G = (int) std::min<long long>(kStepMaxSegments, std::max<long long>(1, (bytes + kStepSegmentBytes - 1) /
                                                                               kStepSegmentBytes));
    G = std::min(G, p->C);
    std::vector<RaggedPlan::Segment> segs;
@@ -679,7 +684,7 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMseHost(DSPLIB_gpu_raggedPlan plan
                        {gy, nullptr, false},     {gx, nullptr, false},     {taps, nullptr, false},
                        {gtaps, nullptr, false},  {coefs, nullptr, false},  {gcoefs, nullptr, false}};
    const long long len[9] = {nx, nx, nx, nx, nx, nh, nh, nk, nk};
-   const long long stagedFloats = 5 * nx + 2 * nh + 2 * nk + 2 * kPipeMaxBlocks + 4;
+   const long long stagedFloats = 5 * nx + 2 * nh + 2 * nk + 2 * kStepMaxSegments + 4;
    float *blk = (float *) stagingBuffer(0, (size_t) stagedFloats * sizeof(float), s);
    float *work = (float *) stagingBuffer(1, (size_t) p->segWork * sizeof(float), s);
    float *scratch = (float *) stagingBuffer(2, (size_t) p->segScratch * sizeof(float), s);
@@ -691,7 +696,7 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMseHost(DSPLIB_gpu_raggedPlan plan
       off += len[i];
    }
    double *sums = (double *) (blk + off);
-   float *lossDev = blk + off + 2 * kPipeMaxBlocks;
+   float *lossDev = blk + off + 2 * kStepMaxSegments;
    const bool lossStaged = !isDevicePtr(loss);
    if (!lossStaged) lossDev = loss;
    auto h2d = [&](const StepArray &a, long long o, long long n) {
@@ -713,16 +718,16 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMseHost(DSPLIB_gpu_raggedPlan plan
       const long long xo = sg.x0, xn = sg.x1 - sg.x0, ho = sg.h0, hn = sg.h1 - sg.h0, ko = sg.k0, kn = sg.k1 - sg.k0;
       if ((e = h2d(arr[0], xo, xn)) != cudaSuccess || (e = h2d(arr[1], xo, xn)) != cudaSuccess ||
           (e = h2d(arr[5], ho, hn)) != cudaSuccess || (e = h2d(arr[7], ko, kn)) != cudaSuccess ||
-          (e = cudaEventRecord(pc->copied[g], pc->in)) != cudaSuccess ||
-          (e = cudaStreamWaitEvent(pc->comp, pc->copied[g], 0)) != cudaSuccess)
+          (e = cudaEventRecord(pc->copied[g % kPipeMaxBlocks], pc->in)) != cudaSuccess ||
+          (e = cudaStreamWaitEvent(pc->comp, pc->copied[g % kPipeMaxBlocks], 0)) != cudaSuccess)
          return pipeFail(nullptr, pc, e, "copy segment in");
       float *gyDev = arr[3].dev + xo;
       if (stepMseCore(sg.plan, arr[0].dev + xo, arr[5].dev + ho, arr[7].dev + ko, arr[1].dev + xo, arr[2].dev + xo,
                       gyDev, nullptr, sums + g, arr[4].dev + xo, arr[6].dev + ho, arr[8].dev + ko, work, scratch,
                       scale, 0.0, pc->comp) != DSPLIB_SUCCESS)
          return pipeFail(nullptr, pc, cudaErrorLaunchFailure, "segment step");
-      if ((e = cudaEventRecord(pc->computed[g], pc->comp)) != cudaSuccess ||
-          (e = cudaStreamWaitEvent(pc->out, pc->computed[g], 0)) != cudaSuccess ||
+      if ((e = cudaEventRecord(pc->computed[g % kPipeMaxBlocks], pc->comp)) != cudaSuccess ||
+          (e = cudaStreamWaitEvent(pc->out, pc->computed[g % kPipeMaxBlocks], 0)) != cudaSuccess ||
           (e = d2h(arr[2], xo, xn)) != cudaSuccess || (e = d2h(arr[3], xo, xn)) != cudaSuccess ||
           (e = d2h(arr[4], xo, xn)) != cudaSuccess || (e = d2h(arr[6], ho, hn)) != cudaSuccess ||
           (e = d2h(arr[8], ko, kn)) != cudaSuccess)
