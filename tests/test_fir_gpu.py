@@ -107,6 +107,20 @@ _NP_CODE = {np.int8: D.INT8, np.int16: D.INT16, np.int32: D.INT32}
 
 
 @pytest.mark.parametrize("dt", [np.int8, np.int16])
+@pytest.mark.parametrize("shift", [30, 31, 32, 33, 47, 62])
+def test_qmode_boundary_shifts(dt, shift):
+    """Q-mode shifts around and beyond the 32-bit accumulator of the int8 output stage and up
+    to the 62 accepted: bit-exact to the restatement (large shifts round every output to 0
+    or -1 exactly as the exact accumulator does), on the tensor-core kernel."""
+    rng = np.random.default_rng(shift)
+    info = np.iinfo(dt)
+    x = rng.integers(info.min, info.max, size=(3, 5000), endpoint=True).astype(dt)
+    h = rng.integers(info.min, info.max, size=(1, 128), endpoint=True).astype(dt)
+    got = host(D.fir(dev(x), dev(h), 128, nch=0, func_style=D.OPTIMIZED, qmode=True, shift=shift))
+    assert np.array_equal(got, oracle.fir_q(x, h, 128, shift, nch=0))
+
+
+@pytest.mark.parametrize("dt", [np.int8, np.int16])
 @pytest.mark.parametrize("qmode", [False, True])
 def test_int_tensor_core_edges(dt, qmode):
     """Tensor-core integer path: partial tiles, odd pitches, extreme values, long filters
