@@ -819,13 +819,26 @@ cudaError_t launchBankBackward(const BankLaunch &b, cudaStream_t s)
                                  (int) adjointShared(b.Smax))) != cudaSuccess)
       return e;
    AdjArgs d{b.chans, b.units, b.nUnits, b.Smax, b.tables, b.u, b.gy, b.ckptF, b.ckptA, b.g, b.part, 0};
-   // one launch per stage count, each with the shared memory its cascades need
+   // One launch per stage count, each with the shared memory its cascades need, spread over
+   // the caller's stream and the auxiliary ones so that CTAs of different buckets share the
+   // SMs (and no launch waits for another's tail).
+   const int lanes = 1 + b.nAux;
+   if (b.nAux > 0) {
+      if ((e = cudaEventRecord(b.fork, s)) != cudaSuccess) return e;
+      for (int i = 0; i < b.nAux; i++)
+         if ((e = cudaStreamWaitEvent(b.aux[i], b.fork, 0)) != cudaSuccess) return e;
+   }
    for (int k = 0; k < b.nBuckets; k++) {
       d.first = b.bucketStart[k];
       const int n = b.bucketStart[k + 1] - b.bucketStart[k];
       if (n <= 0) continue;
-      bank_adjoint_kernel<<<n, 32, adjointShared(b.bucketS[k]), s>>>(d);
+      const cudaStream_t st = (k % lanes) == 0 ? s : b.aux[(k % lanes) - 1];
+      bank_adjoint_kernel<<<n, 32, adjointShared(b.bucketS[k]), st>>>(d);
       countLaunch();
+   }
+   for (int i = 0; i < b.nAux; i++) {
+      if ((e = cudaEventRecord(b.join[i], b.aux[i])) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(s, b.join[i], 0)) != cudaSuccess) return e;
    }
    bank_coef_kernel<<<b.C, 32, 0, s>>>(b.chans, b.part, b.gcoefs);
    countLaunch();

@@ -354,6 +354,12 @@ struct BankLaunch {
    // the channels of bucketS[k] stages, from bucketStart[k] (host arrays)
    const int *bucketS, *bucketStart;
    int nBuckets;
+   // streams the adjoint's buckets fan out to (forked from and joined back into the
+   // caller's stream with events; capturable), or nAux = 0
+   const cudaStream_t *aux;
+   int nAux;
+   cudaEvent_t fork;
+   const cudaEvent_t *join;
 };
 // Doubles of both unit transitions of a channel of S stages.
 long long bankTransitionDoubles(int S);

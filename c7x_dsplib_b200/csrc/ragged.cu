@@ -35,6 +35,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -82,6 +83,14 @@ struct RaggedPlan {
    std::vector<Segment> segs;
    // units ordered by their channel's stage count, deepest first, in buckets of one count
    std::vector<int> bucketS, bucketStart; // bucketStart has one entry more (the end)
+   // auxiliary streams and events of the adjoint's bucket launches (created with the plan)
+   static constexpr int kAux = 3;
+   cudaStream_t aux[kAux] = {};
+   cudaEvent_t fork = nullptr, join[kAux] = {};
+   int nAux = 0;
+   // the fork / join events are per plan: calls on one plan from several host threads
+   // queue their adjoints one at a time
+   std::mutex forkMu;
    long long segWork = 0, segScratch = 0; // largest work / scratch of one segment
 };
 
@@ -188,6 +197,11 @@ static void freePlan(RaggedPlan *p)
    cudaFree(p->dUnits);
    freeErrorWord(p->err);
    for (RaggedPlan::Segment &g : p->segs) freePlan(g.plan);
+   for (int i = 0; i < p->nAux; i++) {
+      cudaStreamDestroy(p->aux[i]);
+      cudaEventDestroy(p->join[i]);
+   }
+   if (p->fork) cudaEventDestroy(p->fork);
    delete p;
 }
 
@@ -317,6 +331,18 @@ static DSPLIB_STATUS raggedPlanBuild(DSPLIB_gpu_raggedPlan *plan, int32_t numCha
    p->hStages.assign(stages, stages + numChannels);
    cudaGetDevice(&p->device);
    p->err = allocErrorWord();
+   if (p->bucketS.size() > 1) {
+      bool ok = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) == cudaSuccess;
+      for (int i = 0; ok && i < RaggedPlan::kAux; i++) {
+         ok = cudaStreamCreateWithFlags(&p->aux[i], cudaStreamNonBlocking) == cudaSuccess;
+         if (ok && cudaEventCreateWithFlags(&p->join[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaStreamDestroy(p->aux[i]);
+            ok = false;
+         }
+         if (ok) p->nAux = i + 1;
+      }
+      (void) cudaGetLastError(); // without auxiliary streams the buckets run in sequence
+   }
    // work buffer: u | forward checkpoints | forward aggregates | stage tables | unit transitions
    p->wCk = align4(p->planeStride);
    p->wAgg = p->wCk + align4(2 * p->nCk);
@@ -474,6 +500,10 @@ static BankLaunch bankLaunch(const RaggedPlan *p, const float *work)
    b.bucketS = p->bucketS.data();
    b.bucketStart = p->bucketStart.data();
    b.nBuckets = (int) p->bucketS.size();
+   b.aux = p->aux;
+   b.nAux = p->nAux;
+   b.fork = p->fork;
+   b.join = p->join;
    return b;
 }
 
@@ -517,7 +547,10 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_bwd(DSPLIB_gpu_raggedPlan plan, const 
    b.groupA = scratch + p->sGrp;
    b.part = scratch + p->sPart;
    b.gcoefs = gcoefs;
-   if (launchBankBackward(b, s) != cudaSuccess) return DSPLIB_ERR_FAILURE;
+   {
+      std::lock_guard<std::mutex> lock(p->forkMu);
+      if (launchBankBackward(b, s) != cudaSuccess) return DSPLIB_ERR_FAILURE;
+   }
    if (launchFirBf16x3Ragged(p->dChan, p->dFirDxRuns, p->nFirDxRuns, g, taps, gx, true, p->Tmax, p->err, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
    if (launchFirDhBf16x3Ragged(p->dChan, p->dDhRuns, p->nDhRuns, x, g, part, p->err, s) != cudaSuccess)
@@ -564,7 +597,12 @@ static DSPLIB_STATUS stepMseCore(RaggedPlan *p, const float *x, const float *tap
    b.part = scratch + p->sPart;
    b.gcoefs = gcoefs;
    b.aggReady = true;
-   if (launchBankBackward(b, s) != cudaSuccess ||
+   cudaError_t be;
+   {
+      std::lock_guard<std::mutex> lock(p->forkMu);
+      be = launchBankBackward(b, s);
+   }
+   if (be != cudaSuccess ||
        launchFirBf16x3Ragged(p->dChan, p->dFirDxRuns, p->nFirDxRuns, g, taps, gx, true, p->Tmax, p->err, s) != cudaSuccess ||
        launchFirDhBf16x3Ragged(p->dChan, p->dDhRuns, p->nDhRuns, x, g, scratch + p->sDh, p->err, s) != cudaSuccess)
       return DSPLIB_ERR_FAILURE;
