@@ -642,18 +642,22 @@ struct AdjArgs {
 __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
 {
    extern __shared__ float4 dynA[];
-   __shared__ float sStage[32 * kOutPad];
    const int lane = threadIdx.x;
    float *sTab = (float *) dynA;
    const int2 U = a.units[a.first + blockIdx.x];
    const RaggedChan c = a.chans[U.x];
    float *W = sTab + (size_t) c.S * kBankTabFloats; // the launch sized shared memory for c.S stages
+   // The staging rows of the packed gradient loads and stores share the stage sequences'
+   // space: the output gradient is read before the sequences are written, the input
+   // gradient stored after the last of them was read (at least 32 x 17 floats: adjointShared).
+   float *sStage = W;
    const int S = c.S, Lu = c.Lu, t0 = U.y * kUnit;
    const long long base = c.ckOff + (long long) U.y * S;
    const UnitStates entF = loadStates(a.ckptF + base, S, lane), entA = loadStates(a.ckptA + base, S, lane);
    loadTables(sTab, a.tables, c, lane);
-   float v[kL], w[kL];
+   float v[kL], w[kL], g[kL];
    loadChunk(v, a.u + c.pOff, t0 + lane * kL, Lu);
+   loadPacked(g, a.gy + c.xOff, t0, Lu, sStage, lane);
    // 1. the forward of this unit from its checkpoints; every stage's sequence kept
    for (int s = 0; s < S; s++) {
       const float *tb = sTab + s * kBankTabFloats;
@@ -667,8 +671,6 @@ __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
       }
    }
    // 2. the stages' adjoints, last stage first, in reverse time
-   float g[kL];
-   loadPacked(g, a.gy + c.xOff, t0, Lu, sStage, lane);
    for (int p = 0; p < S; p++) {
       const int s = S - 1 - p;
       const float *tb = sTab + s * kBankTabFloats;
@@ -720,6 +722,7 @@ __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
          a.part[(base + s) * 5 + lane] = val;
       }
    }
+   __syncwarp(); // every lane's last read of the stage sequences precedes the staging writes
    storePacked(g, a.g + c.xOff, t0, Lu, sStage, lane);
 }
 
@@ -755,7 +758,8 @@ cudaError_t launchBankTables(const RaggedChan *chans, int C, const float *coefs,
 static size_t unitShared(int Smax) { return (size_t) kWarps * Smax * kBankTabFloats * sizeof(float); }
 static size_t adjointShared(int Smax)
 {
-   return ((size_t) Smax * kBankTabFloats + (size_t) (Smax > 0 ? Smax - 1 : 0) * kL * 32) * sizeof(float);
+   const size_t seq = (size_t) (Smax > 0 ? Smax - 1 : 0) * kL * 32, stage = (size_t) 32 * kOutPad;
+   return ((size_t) Smax * kBankTabFloats + (seq > stage ? seq : stage)) * sizeof(float);
 }
 
 template <int MODE> static cudaError_t launchUnits(const UnitArgs &a, cudaStream_t s)
