@@ -104,6 +104,10 @@ constexpr int kRaggedMaxStages = 64;
 // 512-float slot per run, slots of a channel consecutive and in time order, summed in
 // that order in FP64 (deterministic):  gtaps[T - 1 - c] = sum_slots part[slot][c].
 constexpr int kDhMaxT = 512;
+// Tiles per run of the taps gradient: each run (one CTA) pays a set-up, a first tile
+// staged before any MMA and a diagonal-sum epilogue, so runs span up to 16 tiles
+// (131072 samples summed in FP32 in TMEM; runs added in FP64).
+constexpr int kDhRunTiles = 16;
 
 __global__ void __launch_bounds__(256) fir_dh_reduce_kernel(const RaggedChan *chans, const int *start,
                                                              const float *part, float *gtaps)
@@ -243,7 +247,7 @@ using namespace dsplib;
 extern "C" {
 
 // Plan with FIR work lists of runs of up to runTiles tiles (forward and input gradient;
-// the taps gradient keeps kFirBfRunTiles, so its partial sums, and with them its
+// the taps gradient keeps kDhRunTiles, so its partial sums, and with them its
 // rounding, do not depend on the choice).
 static DSPLIB_STATUS raggedPlanBuild(DSPLIB_gpu_raggedPlan *plan, int32_t numChannels, const int32_t *length,
                                      const int32_t *taps, const int32_t *stages, int runTiles)
@@ -285,8 +289,8 @@ static DSPLIB_STATUS raggedPlanBuild(DSPLIB_gpu_raggedPlan *plan, int32_t numCha
       for (int t = 0; t * kRTile < Lu; t++) fwd.push_back(make_int2(c, t));
       {
          const int tiles = (Lu + kFirBfTile - 1) / kFirBfTile;
-         for (int t = 0; t < tiles; t += kFirBfRunTiles)
-            dhRuns.push_back(make_int4(c, t, std::min(kFirBfRunTiles, tiles - t), (int) dhRuns.size()));
+         for (int t = 0; t < tiles; t += kDhRunTiles)
+            dhRuns.push_back(make_int4(c, t, std::min(kDhRunTiles, tiles - t), (int) dhRuns.size()));
       }
       for (int j = 0; j < nu; j++) units.push_back(make_int2(c, j));
       addRuns(firFwd, c, Lu);
