@@ -162,6 +162,7 @@ SIGNATURES = {
     "DSPLIB_gpu_raggedPlanSize": (ctypes.c_int64, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_raggedPlanDestroy": (ctypes.c_int, [_VP]),
     "DSPLIB_gpu_raggedPlanStatus": (ctypes.c_int, [_VP]),
+    "DSPLIB_gpu_raggedPlanSetAsync": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_status": (ctypes.c_int, [_VP]),
     "DSPLIB_gpu_injectFault": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "DSPLIB_gpu_firBiquadBatched_fwd": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),

@@ -92,6 +92,10 @@ struct RaggedPlan {
    // queue their adjoints one at a time
    std::mutex forkMu;
    long long segWork = 0, segScratch = 0; // largest work / scratch of one segment
+   // device buffers of the host-buffer step (allocated by its first call, kept with the
+   // plan), and whether it returns once queued (DSPLIB_gpu_raggedPlanSetAsync)
+   float *hBlk = nullptr, *hWork = nullptr, *hScratch = nullptr;
+   int async = 0;
 };
 
 namespace {
@@ -206,6 +210,9 @@ static void freePlan(RaggedPlan *p)
       cudaEventDestroy(p->join[i]);
    }
    if (p->fork) cudaEventDestroy(p->fork);
+   cudaFree(p->hBlk);
+   cudaFree(p->hWork);
+   cudaFree(p->hScratch);
    delete p;
 }
 
@@ -474,10 +481,24 @@ DSPLIB_STATUS DSPLIB_gpu_raggedPlanStatus(DSPLIB_gpu_raggedPlan plan)
 {
    RaggedPlan *p = (RaggedPlan *) plan;
    if (!p) return DSPLIB_ERR_NULL_POINTER;
+   bool expired = false;
    if (p->err && *(volatile int *) p->err != 0) {
       *(volatile int *) p->err = 0;
-      return DSPLIB_ERR_FAILURE;
+      expired = true;
    }
+   for (const RaggedPlan::Segment &sg : p->segs) // the host-buffer step's segment plans
+      if (sg.plan->err && *(volatile int *) sg.plan->err != 0) {
+         *(volatile int *) sg.plan->err = 0;
+         expired = true;
+      }
+   return expired ? DSPLIB_ERR_FAILURE : DSPLIB_SUCCESS;
+}
+
+DSPLIB_STATUS DSPLIB_gpu_raggedPlanSetAsync(DSPLIB_gpu_raggedPlan plan, int32_t async)
+{
+   RaggedPlan *p = (RaggedPlan *) plan;
+   if (!p) return DSPLIB_ERR_NULL_POINTER;
+   p->async = async ? 1 : 0;
    return DSPLIB_SUCCESS;
 }
 
@@ -727,10 +748,20 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMseHost(DSPLIB_gpu_raggedPlan plan
                        {gtaps, nullptr, false},  {coefs, nullptr, false},  {gcoefs, nullptr, false}};
    const long long len[9] = {nx, nx, nx, nx, nx, nh, nh, nk, nk};
    const long long stagedFloats = 5 * nx + 2 * nh + 2 * nk + 2 * kStepMaxSegments + 4;
-   float *blk = (float *) stagingBuffer(0, (size_t) stagedFloats * sizeof(float), s);
-   float *work = (float *) stagingBuffer(1, (size_t) p->segWork * sizeof(float), s);
-   float *scratch = (float *) stagingBuffer(2, (size_t) p->segScratch * sizeof(float), s);
-   if (!blk || !work || !scratch) return DSPLIB_ERR_FAILURE;
+   if (!p->hBlk) {
+      // the plan's own staging (not the thread's): calls on different plans may be in
+      // flight together
+      if (cudaMalloc(&p->hBlk, (size_t) stagedFloats * sizeof(float)) != cudaSuccess ||
+          cudaMalloc(&p->hWork, (size_t) std::max(1LL, p->segWork) * sizeof(float)) != cudaSuccess ||
+          cudaMalloc(&p->hScratch, (size_t) std::max(1LL, p->segScratch) * sizeof(float)) != cudaSuccess) {
+         (void) cudaGetLastError();
+         cudaFree(p->hBlk);
+         cudaFree(p->hWork);
+         p->hBlk = p->hWork = nullptr;
+         return DSPLIB_ERR_FAILURE;
+      }
+   }
+   float *blk = p->hBlk, *work = p->hWork, *scratch = p->hScratch;
    long long off = 0;
    for (int i = 0; i < 9; i++) {
       arr[i].staged = arr[i].host == nullptr || !isDevicePtr(arr[i].host);
@@ -782,9 +813,10 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMseHost(DSPLIB_gpu_raggedPlan plan
       return pipeFail(nullptr, pc, e, "loss");
    if (lossStaged && (e = cudaMemcpyAsync(loss, lossDev, sizeof(float), cudaMemcpyDeviceToHost, pc->out)) != cudaSuccess)
       return pipeFail(nullptr, pc, e, "copy loss");
-   if ((e = cudaEventRecord(pc->done, pc->out)) != cudaSuccess || (e = cudaStreamWaitEvent(s, pc->done, 0)) != cudaSuccess ||
-       (e = cudaStreamSynchronize(s)) != cudaSuccess)
+   if ((e = cudaEventRecord(pc->done, pc->out)) != cudaSuccess || (e = cudaStreamWaitEvent(s, pc->done, 0)) != cudaSuccess)
       return pipeFail(nullptr, pc, e, "pipeline join");
+   if (p->async) return DSPLIB_SUCCESS; // the caller synchronises `stream`, then DSPLIB_gpu_raggedPlanStatus
+   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return pipeFail(nullptr, pc, e, "pipeline join");
    bool expired = false;
    for (const RaggedPlan::Segment &sg : p->segs)
       if (sg.plan->err && *(volatile int *) sg.plan->err != 0) {

@@ -151,6 +151,15 @@ class RaggedFilterBank:
         if st != SUCCESS:
             raise DsplibError("DSPLIB_gpu_firBiquadBatched_stepMse", st)
 
+    def set_async(self, on: bool):
+        """True: step_mse_host returns once queued on the current stream (page-locked
+        tensors; synchronise the stream, then check status()); False: it returns complete."""
+        return lib().DSPLIB_gpu_raggedPlanSetAsync(self._plan, int(bool(on)))
+
+    def status(self) -> int:
+        """DSPLIB_gpu_raggedPlanStatus: nonzero if a bounded tensor-core wait expired."""
+        return lib().DSPLIB_gpu_raggedPlanStatus(self._plan)
+
     def step_mse_host(self, x, taps, coefs, target, y, gy, loss, gx, gtaps, gcoefs):
         """The training step on host tensors (DSPLIB_gpu_firBiquadBatched_stepMseHost):
         inputs copied in and results copied out by the library, channel segments

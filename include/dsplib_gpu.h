@@ -237,15 +237,20 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMse(DSPLIB_gpu_raggedPlan plan, co
 /** The training step of DSPLIB_gpu_firBiquadBatched_stepMse on buffers in host memory
  *  (device pointers are accepted too, per array, and used in place): x, taps, coefs and
  *  target are read, y, gy, loss, gx, gtaps and gcoefs written (gy may be NULL when the
- *  caller does not want it).  No work or scratch argument: the library stages through
- *  device buffers of its own (per host thread and device, kept until the thread exits).
+ *  caller does not want it).  No work or scratch argument: the plan stages through
+ *  device buffers of its own (allocated by the first call, about 20 bytes per sample,
+ *  released by DSPLIB_gpu_raggedPlanDestroy).
  *  The channels are split into up to 8 contiguous segments of about equal samples, each
  *  with a plan of its own (built by the first call on the plan); segment k is copied in
  *  while segment k - 1 is filtered and segment k - 2's results are copied out, on three
  *  streams, so that both transfer directions and the kernels overlap.  With page-locked
  *  buffers the copies run at the link's rate; pageable ones are copied by the driver
- *  through its own bounce buffers and overlap less.  Synchronous: returns once every
- *  result is in the caller's memory (after the work queued on `stream` before it).
+ *  through its own bounce buffers and overlap less.  Synchronous by default: returns once
+ *  every result is in the caller's memory (after the work queued on `stream` before it);
+ *  after DSPLIB_gpu_raggedPlanSetAsync(plan, 1) it returns once the work is queued, so
+ *  calls on different plans overlap one call's copies out with the next call's copies in;
+ *  the caller synchronises `stream` before touching the buffers, then checks
+ *  DSPLIB_gpu_raggedPlanStatus.
  *  y, gy, gx, gtaps and gcoefs equal the device call's bit for bit; loss is the same sum
  *  of squares added per segment, then over the segments in order.  DSPLIB_ERR_FAILURE if
  *  a copy or launch fails or a bounded tensor-core wait expired.  No counterpart in the
@@ -254,6 +259,10 @@ DSPLIB_STATUS DSPLIB_gpu_firBiquadBatched_stepMseHost(DSPLIB_gpu_raggedPlan plan
                                                       const float *coefs, const float *target, float *y, float *gy,
                                                       float *loss, float *gx, float *gtaps, float *gcoefs,
                                                       void *stream);
+
+/** 1: DSPLIB_gpu_firBiquadBatched_stepMseHost on this plan returns once queued (page-locked
+ *  buffers; the caller synchronises the stream); 0 (default): it returns complete. */
+DSPLIB_STATUS DSPLIB_gpu_raggedPlanSetAsync(DSPLIB_gpu_raggedPlan plan, int32_t async);
 
 /** After the calls queued on this plan were synchronised: DSPLIB_ERR_FAILURE if a bounded
  *  wait of one of its tensor-core kernels expired since the last check (the outputs of

@@ -413,3 +413,45 @@ def test_host_step_equals_device_step(pinned):
                 continue
             assert torch.equal(out[k].cpu(), ref[k]), (rep, k)
         assert float(out["loss"]) == pytest.approx(float(ref["loss"]), rel=1e-6)
+
+
+@pytest.mark.gpu
+def test_host_step_async_two_plans_in_flight():
+    """Two plans of the same bank, each DSPLIB_gpu_raggedPlanSetAsync(plan, 1), calls queued
+    on two streams before either finishes (one call's copies out overlap the next's copies
+    in), three rounds: every result bitwise equal to the device step's."""
+    import torch
+
+    from c7x_dsplib_b200.filterbank import RaggedFilterBank
+
+    lengths, taps, stages, x, h, c = _bank_case(22, 40, Lrange=(1000, 240000), Tmax=300, Smax=6)
+    dev = "cuda"
+    xt, ht, ct = (torch.tensor(a, dtype=torch.float32, device=dev) for a in (x, h, c))
+    ref_bank = RaggedFilterBank(lengths, taps, stages)
+    target = torch.randn(ref_bank.sizes[0], device=dev, generator=torch.Generator(dev).manual_seed(9))
+    n = ref_bank.sizes[0]
+    ref = {k: torch.empty(n, device=dev) for k in ("y", "gy", "gx")}
+    ref["gtaps"], ref["gcoefs"], ref["loss"] = torch.empty_like(ht), torch.empty_like(ct), torch.empty(1, device=dev)
+    ref_bank.step_mse_raw(xt, ht, ct, target, ref["y"], ref["gy"], ref["loss"], ref["gx"], ref["gtaps"],
+                          ref["gcoefs"], torch.empty(ref_bank.sizes[3], device=dev),
+                          torch.empty(ref_bank.sizes[4], device=dev))
+    torch.cuda.synchronize()
+    ref = {k: v.cpu() for k, v in ref.items()}
+    hx, hh, hc, htg = (t.cpu().pin_memory() for t in (xt, ht, ct, target))
+    banks = [RaggedFilterBank(lengths, taps, stages) for _ in range(2)]
+    streams = [torch.cuda.Stream() for _ in range(2)]
+    outs = []
+    for b in banks:
+        assert b.set_async(True) == 0
+        outs.append({k: torch.full(v.shape, 7.0).pin_memory() for k, v in ref.items() if k != "gy"})
+    for rnd in range(3):
+        for b, st, o in zip(banks, streams, outs):
+            st.synchronize()  # this slot's previous call finished: its buffers may be reused
+            with torch.cuda.stream(st):
+                b.step_mse_host(hx, hh, hc, htg, o["y"], None, o["loss"], o["gx"], o["gtaps"], o["gcoefs"])
+        for b, st, o in zip(banks, streams, outs):
+            st.synchronize()
+            assert b.status() == 0
+            for k in ("y", "gx", "gtaps", "gcoefs"):
+                assert torch.equal(o[k], ref[k]), (rnd, k)
+            assert float(o["loss"]) == pytest.approx(float(ref["loss"]), rel=1e-6)
