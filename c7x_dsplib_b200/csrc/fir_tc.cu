@@ -784,14 +784,37 @@ __device__ __forceinline__ bool bfWork(const BfRun &r, const BfSmem &L, uint32_t
    // samples between the 16-byte boundary at or below the tile's first input and that input
    auto misOf = [&](int t) { return (int) ((((long long) ((uintptr_t) r.x >> 2)) + q0(t)) & 3); };
    auto bytesOf = [&](int t) { return (uint32_t) blocksOf(t) * 256u + (misOf(t) ? 16u : 0u); };
-   // a bulk copy needs the whole window [q - mis, q - mis + bytes / 4) inside the input
-   auto bulkOk = [&](int t) {
+   // The raw window of tile t is [w0, w0 + bytes / 4), w0 = q - mis on a 16-byte boundary.
+   // The bulk copy takes its part inside the input, [lo, hi), both ends on 16-byte
+   // boundaries (window offsets multiples of 4 samples); the threads write the rest:
+   // the up to 3 samples beside each end and the zeros outside the input.
+   auto bulkLo = [&](int t) {
       const long long w0 = q0(t) - misOf(t);
-      return S > 0 && w0 >= 0 && w0 + bytesOf(t) / 4 <= r.inLen;
+      return w0 >= 0 ? w0 : w0 + ((-w0 + 3) & ~3LL);
    };
+   auto bulkHi = [&](int t) {
+      const long long w0 = q0(t) - misOf(t), end = min(w0 + (long long) (bytesOf(t) / 4), r.inLen);
+      return w0 + ((end - w0) & ~3LL);
+   };
+   auto bulkOk = [&](int t) { return S > 0 && bulkHi(t) > bulkLo(t); };
    auto fetch = [&](int t, int k) {
-      tc::mbarExpectTx(L.full + k, bytesOf(t));
-      tc::bulkLoad(L.slot(k), r.x + (q0(t) - misOf(t)), bytesOf(t), L.full + k);
+      const long long w0 = q0(t) - misOf(t), lo = bulkLo(t), hi = bulkHi(t);
+      tc::mbarExpectTx(L.full + k, (uint32_t) (hi - lo) * 4u);
+      tc::bulkLoad(L.slot(k) + (lo - w0), r.x + lo, (uint32_t) (hi - lo) * 4u, L.full + k);
+   };
+   // the window's samples outside the bulk range: input values or zeros beyond it
+   auto fixEdges = [&](int t, int k) {
+      const long long w0 = q0(t) - misOf(t), lo = bulkLo(t), hi = bulkHi(t);
+      const int W = (int) (bytesOf(t) / 4);
+      float *raw = L.slot(k);
+      for (int i = tid; i < (int) (lo - w0); i += kBfWorkers) {
+         const long long q = w0 + i;
+         raw[i] = (q >= 0 && q < r.inLen) ? r.x[q] : 0.0f;
+      }
+      for (int i = (int) (hi - w0) + tid; i < W; i += kBfWorkers) {
+         const long long q = w0 + i;
+         raw[i] = (q >= 0 && q < r.inLen) ? r.x[q] : 0.0f;
+      }
    };
    // The first raw tiles are fetched while the taps band is built.  (Every MMA of the
    // previous run completed: its last tile was drained.)
@@ -854,6 +877,7 @@ __device__ __forceinline__ bool bfWork(const BfRun &r, const BfSmem &L, uint32_t
             pp.pending &= ~(1u << k);
          }
          if (!ok && tid == 0) raiseError(r.err);
+         if (viaBulk) fixEdges(t, k);
          if (tc::namedSyncOr(kBfBar, kBfWorkers, !ok)) return false; // the raw tile landed (and the band is built)
          if (viaBulk) bfSplit(L.slot(k), misOf(t), blocksOf(t), L.hi(cur), L.lo(cur), tid);
          else bfStage(r.x, q0(t), r.inLen, blocksOf(t), L.hi(cur), L.lo(cur), tid); // straight from global memory
