@@ -634,6 +634,8 @@ constexpr int kChThreads = kChWarps * 32;
 constexpr int kChWindow = kChThreads * kChL;
 constexpr int kChPowers = 10; // M^(2^k), k = 0..9: M^512 spans a window
 constexpr int kChanKernelMaxChannels = 16;
+constexpr int kChanTuneMaxChannels = 128; // the autotuner may pick the per-channel kernel up to here
+constexpr int kTuneChanKernel = 1;        // the autotuner's choice value for the per-channel kernel
 
 size_t chanSmemBytes(int S) { return (size_t) S * (kChPowers * sizeof(M2) + sizeof(double2) + 5 * sizeof(float)); }
 
@@ -892,7 +894,7 @@ template <int FORM> cudaError_t launchChanForm(const BiquadLaunch &a, cudaStream
 // 8 or 16 warps per CTA (windows of 256 or 512 samples) and up to 16 CTAs per cluster.
 template <int FORM> cudaError_t launchScanForm(const BiquadLaunch &a, cudaStream_t s)
 {
-   if (a.C <= kChanKernelMaxChannels) return launchChanForm<FORM>(a, s);
+   if (a.C <= kChanKernelMaxChannels || a.tuneChoice == kTuneChanKernel) return launchChanForm<FORM>(a, s);
    if (a.tuneChoice > 0) {
       const int W = a.tuneChoice / 100, K = a.tuneChoice % 100;
       if (W == 8 && K >= 1) return launchScanShape<FORM, 8>(a, K, s);
@@ -945,6 +947,8 @@ std::vector<int> biquadTuneCandidates(const BiquadLaunch &a)
 {
    std::vector<int> c;
    if (biquadTuneKey(a).empty()) return c;
+   // a few dozen channels: one CTA per channel along time (more SMs than one cluster) is a candidate
+   if (a.C <= kChanTuneMaxChannels) c.push_back(kTuneChanKernel);
    const long long chunks = (a.N + kScanL - 1) / kScanL;
    for (int W : {8, 16})
       for (int K = 1; K <= (W < kMaxCluster ? W : kMaxCluster); K *= 2)

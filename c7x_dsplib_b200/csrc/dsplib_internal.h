@@ -379,12 +379,13 @@ struct BiquadLaunch {
    int N, C, S;
    long long inPitch, outPitch, varPitch, coefPitch; // elements
    int prefetch = 0; // x is device memory: the scan kernel may fetch the next window early (cp.async)
-   int tuneChoice = -1; // scan shape from the autotuner: 100 * warps per CTA + CTAs per cluster (-1: the rule)
+   int tuneChoice = -1; // scan shape from the autotuner: 100 * warps per CTA + CTAs per cluster, or 1 for
+                        // the per-channel kernel (-1: the rule)
 };
 
 // Autotuner entries of the cascade-biquad scan (OPTIMIZED style): the key of a launch's
 // problem class ("" when the per-channel kernel or the sequential one runs) and its
-// candidate shapes (100 * warps per CTA + CTAs per cluster).
+// candidate shapes (100 * warps per CTA + CTAs per cluster; 1: one CTA per channel).
 std::string biquadTuneKey(const BiquadLaunch &a);
 std::vector<int> biquadTuneCandidates(const BiquadLaunch &a);
 
