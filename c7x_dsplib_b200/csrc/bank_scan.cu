@@ -263,27 +263,27 @@ __global__ void __launch_bounds__(32) bank_chain_kernel(const RaggedChan *chans,
 // with Phi^32, then every group runs again from its true start and writes the
 // checkpoints.  In a step, lane r holds state component r and row r of the
 // transition in registers; z is broadcast by shuffles.  Group states sit in shared
-// memory for channels of up to 64 groups, in the caller's buffer beyond.
+// memory for channels of up to 48 groups, in the caller's buffer beyond.
 constexpr int kChainWarps = 8;
 constexpr int kChainGroup = 32;
-constexpr int kChainSharedGroups = 64;
+constexpr int kChainSharedGroups = 48;
 
-__device__ __forceinline__ void loadRow(float (&row)[2 * kChainFastStages], const double *P, int n2, int lane)
+// Row r of a transition (lane r's) at rows[r * kRowPad + k], zero beyond n2 and above the
+// block diagonal: in shared memory rather than registers, which keeps the kernel's register
+// count low enough for four CTAs per SM (the rows are read conflict-free: lane r, column q
+// sits in bank (r + q) mod 32).
+constexpr int kRowPad = 2 * kChainFastStages + 1;
+__device__ __forceinline__ void loadRows(float *rows, const double *P, int n2, int tid, int nthreads)
 {
-#pragma unroll
-   for (int k = 0; k < 2 * kChainFastStages; k++) row[k] = 0.0f;
-   if (lane < n2) {
-      const int p = lane >> 1, i = lane & 1;
-#pragma unroll
-      for (int k = 0; k < 2 * kChainFastStages; k++) {
-         const int q = k >> 1;
-         if (k < n2 && q <= p) row[k] = (float) P[4 * blk(p, q) + 2 * i + (k & 1)];
-      }
+   for (int i = tid; i < 2 * kChainFastStages * kRowPad; i += nthreads) {
+      const int r = i / kRowPad, k = i % kRowPad;
+      const int p = r >> 1, q = k >> 1;
+      rows[i] = (r < n2 && k < n2 && q <= p) ? (float) P[4 * blk(p, q) + 2 * (r & 1) + (k & 1)] : 0.0f;
    }
 }
 
 // z' = row . z + e (lane r: component r), z broadcast from lanes 0 .. n2 - 1.
-__device__ __forceinline__ float chainStep(const float (&row)[2 * kChainFastStages], float z, float e, int n2)
+__device__ __forceinline__ float chainStep(const float *row, float z, float e, int n2)
 {
    float a0 = e, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
 #pragma unroll
@@ -303,6 +303,7 @@ __global__ void __launch_bounds__(kChainWarps * 32) bank_chain_fast_kernel(const
 {
    __shared__ float sE[kChainWarps][kChainGroup * 2 * kChainFastStages]; // a group's aggregates, per warp
    __shared__ float sG[kChainSharedGroups * 2 * kChainFastStages];       // group states
+   __shared__ float sRow[2][2 * kChainFastStages * kRowPad];             // Phi and Phi^32
    const RaggedChan c = chans[blockIdx.x];
    const int S = c.S, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    if (S == 0 || S > kChainFastStages) return;
@@ -311,7 +312,6 @@ __global__ void __launch_bounds__(kChainWarps * 32) bank_chain_fast_kernel(const
    float *G = groups <= kChainSharedGroups ? sG : groupBuf + c.grpOff;
    const float *ag = (const float *) (agg + c.ckOff);
    float *ck = (float *) (ckpt + c.ckOff);
-   float row[2 * kChainFastStages];
    // unit of step k of group g (processing order), and that group's units in memory order
    auto unitOf = [&](int g, int k) { return adj ? units - 1 - (g * kChainGroup + k) : g * kChainGroup + k; };
    auto stageGroup = [&](int g, int gn) {
@@ -321,8 +321,11 @@ __global__ void __launch_bounds__(kChainWarps * 32) bank_chain_fast_kernel(const
       __syncwarp();
       return j0;
    };
+   loadRows(sRow[0], phi + c.phiOff + (adj ? 4LL * nb : 0), n2, threadIdx.x, blockDim.x);
+   loadRows(sRow[1], phi + c.phiOff + 8LL * nb + (adj ? 4LL * nb : 0), n2, threadIdx.x, blockDim.x);
+   __syncthreads();
+   const float *row = sRow[0] + lane * kRowPad;
    // 1. group aggregates from a zero state (the last group's is not needed)
-   loadRow(row, phi + c.phiOff + (adj ? 4LL * nb : 0), n2, lane);
    for (int g = warp; g + 1 < groups; g += kChainWarps) {
       const int j0 = stageGroup(g, kChainGroup);
       float z = 0.0f;
@@ -333,8 +336,7 @@ __global__ void __launch_bounds__(kChainWarps * 32) bank_chain_fast_kernel(const
    __syncthreads();
    // 2. true group starts: Z_0 = 0, Z_{g+1} = Phi^32 Z_g + E_g
    if (warp == 0) {
-      float rowQ[2 * kChainFastStages];
-      loadRow(rowQ, phi + c.phiOff + 8LL * nb + (adj ? 4LL * nb : 0), n2, lane);
+      const float *rowQ = sRow[1] + lane * kRowPad;
       float Z = 0.0f;
       for (int g = 0; g < groups; g++) {
          const float E = (lane < n2 && g + 1 < groups) ? G[g * n2 + lane] : 0.0f;
@@ -726,15 +728,19 @@ __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
    storePacked(g, a.g + c.xOff, t0, Lu, sStage, lane);
 }
 
-// Coefficient gradients of one channel (one warp): the units' partial sums in unit order, FP64.
+// Coefficient gradients of one channel (one warp): per coefficient, lane l adds the partial
+// sums of units l, l + 32, ... in FP64, then a fixed butterfly adds the lanes' sums (bitwise
+// repeatable; the channel's units are read 32 at a time instead of one after another).
 __global__ void __launch_bounds__(32) bank_coef_kernel(const RaggedChan *chans, const float *part, float *gcoefs)
 {
    const RaggedChan c = chans[blockIdx.x];
-   const int S = c.S, units = (c.Lu + kUnit - 1) / kUnit;
-   for (int q = threadIdx.x; q < 5 * S; q += 32) {
+   const int S = c.S, units = (c.Lu + kUnit - 1) / kUnit, lane = threadIdx.x;
+   for (int q = 0; q < 5 * S; q++) {
       double acc = 0.0;
-      for (int j = 0; j < units; j++) acc += (double) part[(c.ckOff + (long long) j * S) * 5 + q];
-      gcoefs[c.cOff + q] = (float) acc;
+      for (int j = lane; j < units; j += 32) acc += (double) part[(c.ckOff + (long long) j * S) * 5 + q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) gcoefs[c.cOff + q] = (float) acc;
    }
 }
 

@@ -159,9 +159,17 @@ __global__ void __launch_bounds__(1024) mse_reduce_kernel(const double *part, in
                                                           double *sum)
 {
    __shared__ double red[1024];
-   double s = 0.0;
-   for (int i = threadIdx.x; i < n; i += 1024) s += part[i];
-   red[threadIdx.x] = s;
+   // four independent sums per thread keep four loads in flight
+   double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+   int i = threadIdx.x;
+   for (; i + 3 * 1024 < n; i += 4 * 1024) {
+      s0 += part[i];
+      s1 += part[i + 1024];
+      s2 += part[i + 2048];
+      s3 += part[i + 3072];
+   }
+   for (; i < n; i += 1024) s0 += part[i];
+   red[threadIdx.x] = (s0 + s1) + (s2 + s3);
    __syncthreads();
    for (int w = 512; w > 0; w >>= 1) {
       if ((int) threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
