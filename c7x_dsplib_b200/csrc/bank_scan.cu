@@ -756,7 +756,9 @@ cudaError_t launchBankTables(const RaggedChan *chans, int C, const float *coefs,
    const size_t dyn = (size_t) 8 * Smax * (Smax + 1) / 2 * sizeof(double);
    cudaError_t e = cudaFuncSetAttribute(bank_transition_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dyn);
    if (e != cudaSuccess) return e;
-   bank_transition_kernel<<<dim3(C, 2), 128, dyn, s>>>(chans, coefs, phi);
+   // one warp per (channel, direction) while the block count is small (up to 36 blocks of
+   // 2 x 2 for 8 stages): the squarings' barriers then cost a warp, not four
+   bank_transition_kernel<<<dim3(C, 2), Smax <= 8 ? 32 : 128, dyn, s>>>(chans, coefs, phi);
    countLaunch(2);
    return cudaGetLastError();
 }
