@@ -429,6 +429,7 @@ __device__ __forceinline__ float2 zeroStatePassRev(const float (&g)[kL], float (
 
 // Initial state of this lane's chunk from the unit's entry state, forward time:
 // M^lane entry + the scan of the lanes before.  Returns the inclusive scan in *incl.
+template <bool ZERO_ENTRY = false>
 __device__ __forceinline__ float2 chunkStateUp(float2 end, float2 entry, const float *tb, int lane, float2 *incl)
 {
    float2 val = end;
@@ -439,14 +440,16 @@ __device__ __forceinline__ float2 chunkStateUp(float2 end, float2 entry, const f
    }
    float2 ex = scan::shflUp(val, 1, 32);
    if (lane == 0) ex = make_float2(0.0f, 0.0f);
+   *incl = val;
+   if (ZERO_ENTRY) return ex; // the unit starts from a zero state: nothing to carry in
 #pragma unroll
    for (int k = 0; k < 5; k++)
       if ((lane >> k) & 1) entry = scan::affine(tabP(tb, k), entry, make_float2(0.0f, 0.0f));
-   *incl = val;
    return f2add(entry, ex);
 }
 
 // Reverse time: M^(31 - lane) entry + the scan of the lanes after.
+template <bool ZERO_ENTRY = false>
 __device__ __forceinline__ float2 chunkStateDown(float2 end, float2 entry, const float *tb, int lane, float2 *incl)
 {
    float2 val = end;
@@ -457,11 +460,12 @@ __device__ __forceinline__ float2 chunkStateDown(float2 end, float2 entry, const
    }
    float2 ex = shflDown(val, 1);
    if (lane == 31) ex = make_float2(0.0f, 0.0f);
+   *incl = val;
+   if (ZERO_ENTRY) return ex;
    const int m = 31 - lane;
 #pragma unroll
    for (int k = 0; k < 5; k++)
       if ((m >> k) & 1) entry = scan::affine(tabP(tb, k), entry, make_float2(0.0f, 0.0f));
-   *incl = val;
    return f2add(entry, ex);
 }
 
@@ -557,7 +561,7 @@ __device__ __forceinline__ void adjointAggregates(float (&g)[kL], const float *s
       float w[kL];
       float2 incl;
       const float2 st =
-          chunkStateDown(zeroStatePassRev(g, w, tb[3], tb[4]), make_float2(0.0f, 0.0f), tb, lane, &incl);
+          chunkStateDown<true>(zeroStatePassRev(g, w, tb[3], tb[4]), make_float2(0.0f, 0.0f), tb, lane, &incl);
       correctAndOutputRev(w, g, tb, st.x, st.y);
       if (lane == 0) agg[p] = incl;
    }
@@ -592,7 +596,8 @@ __global__ void __launch_bounds__(kThreads) bank_unit_kernel(UnitArgs a)
       float w[kL];
       const float2 entry = OUT ? entryAt(ent, p) : make_float2(0.0f, 0.0f);
       float2 incl;
-      const float2 st = chunkStateUp(zeroStatePass(v, w, tb[3], tb[4]), entry, tb, lane, &incl);
+      const float2 st = OUT ? chunkStateUp(zeroStatePass(v, w, tb[3], tb[4]), entry, tb, lane, &incl)
+                            : chunkStateUp<true>(zeroStatePass(v, w, tb[3], tb[4]), entry, tb, lane, &incl);
       correctAndOutput(w, v, tb, st.x, st.y);
       if (MODE == UNIT_AGG && lane == 31) a.agg[base + p] = incl;
    }
