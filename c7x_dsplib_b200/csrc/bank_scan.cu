@@ -382,10 +382,24 @@ __device__ __forceinline__ void loadChunk(float (&v)[kL], const float *row, int 
 }
 
 // The chunk of an unaligned packed row (x, y, gradients), through the warp's staging
-// area so that every access of the warp covers 32 consecutive samples.
-__device__ __forceinline__ void loadPacked(float (&v)[kL], const float *row, int t0, int n, float *stage, int lane)
+// area so that every access of the warp covers 32 consecutive samples.  fetchPacked
+// issues the unit's coalesced loads (sample t0 + lane + 32 j in r[j]); stagePacked turns
+// them into the lane's chunk, so that a kernel can put other work between the two.
+__device__ __forceinline__ void fetchPacked(float (&r)[kL], const float *row, int t0, int n, int lane)
 {
-   for (int k = lane; k < kUnit; k += 32) stage[(k >> 4) * kOutPad + (k & 15)] = t0 + k < n ? row[t0 + k] : 0.0f;
+#pragma unroll
+   for (int j = 0; j < kL; j++) {
+      const int k = lane + 32 * j;
+      r[j] = t0 + k < n ? row[t0 + k] : 0.0f;
+   }
+}
+__device__ __forceinline__ void stagePacked(float (&v)[kL], const float (&r)[kL], float *stage, int lane)
+{
+#pragma unroll
+   for (int j = 0; j < kL; j++) {
+      const int k = lane + 32 * j;
+      stage[(k >> 4) * kOutPad + (k & 15)] = r[j];
+   }
    __syncwarp();
 #pragma unroll
    for (int i = 0; i < kL; i++) v[i] = stage[lane * kOutPad + i];
@@ -441,11 +455,15 @@ __device__ __forceinline__ float2 chunkStateUp(float2 end, float2 entry, const f
    float2 ex = scan::shflUp(val, 1, 32);
    if (lane == 0) ex = make_float2(0.0f, 0.0f);
    *incl = val;
-   if (ZERO_ENTRY) return ex; // the unit starts from a zero state: nothing to carry in
+   if constexpr (ZERO_ENTRY) {
+      return ex; // the unit starts from a zero state: nothing to carry in
+   }
+   else {
 #pragma unroll
-   for (int k = 0; k < 5; k++)
-      if ((lane >> k) & 1) entry = scan::affine(tabP(tb, k), entry, make_float2(0.0f, 0.0f));
-   return f2add(entry, ex);
+      for (int k = 0; k < 5; k++)
+         if ((lane >> k) & 1) entry = scan::affine(tabP(tb, k), entry, make_float2(0.0f, 0.0f));
+      return f2add(entry, ex);
+   }
 }
 
 // Reverse time: M^(31 - lane) entry + the scan of the lanes after.
@@ -461,12 +479,16 @@ __device__ __forceinline__ float2 chunkStateDown(float2 end, float2 entry, const
    float2 ex = shflDown(val, 1);
    if (lane == 31) ex = make_float2(0.0f, 0.0f);
    *incl = val;
-   if (ZERO_ENTRY) return ex;
-   const int m = 31 - lane;
+   if constexpr (ZERO_ENTRY) {
+      return ex;
+   }
+   else {
+      const int m = 31 - lane;
 #pragma unroll
-   for (int k = 0; k < 5; k++)
-      if ((m >> k) & 1) entry = scan::affine(tabP(tb, k), entry, make_float2(0.0f, 0.0f));
-   return f2add(entry, ex);
+      for (int k = 0; k < 5; k++)
+         if ((m >> k) & 1) entry = scan::affine(tabP(tb, k), entry, make_float2(0.0f, 0.0f));
+      return f2add(entry, ex);
+   }
 }
 
 // True internal sequence (in place of the zero-state one) and stage output, from the
@@ -539,11 +561,21 @@ struct UnitArgs {
    float scale;
 };
 
-// Copy the channel's stage tables into the warp's slice of shared memory.
+// Copy the channel's stage tables into the warp's slice of shared memory, four loads
+// per lane in flight before their stores (up to 6 stages in one round).
 __device__ __forceinline__ void loadTables(float *dst, const float *tables, const RaggedChan &c, int lane)
 {
    const float4 *src = (const float4 *) (tables + (c.cOff / 5) * kBankTabFloats);
-   for (int i = lane; i < c.S * (kBankTabFloats / 4); i += 32) ((float4 *) dst)[i] = src[i];
+   const int n4 = c.S * (kBankTabFloats / 4);
+   for (int i0 = lane; i0 < n4; i0 += 4 * 32) {
+      float4 r[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+         if (i0 + 32 * j < n4) r[j] = src[i0 + 32 * j];
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+         if (i0 + 32 * j < n4) ((float4 *) dst)[i0 + 32 * j] = r[j];
+   }
    __syncwarp();
 }
 
@@ -580,17 +612,21 @@ __global__ void __launch_bounds__(kThreads) bank_unit_kernel(UnitArgs a)
    const RaggedChan c = a.chans[U.x];
    const int S = c.S, Lu = c.Lu, t0 = U.y * kUnit;
    const long long base = c.ckOff + (long long) U.y * S;
-   loadTables(sTab, a.tables, c, lane);
    constexpr bool OUT = MODE == UNIT_OUT || MODE == UNIT_OUT_MSE;
+   // every global load of the unit is issued before the tables' copy waits on its own
    UnitStates ent = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
    if (OUT) ent = loadStates(a.ckpt + base, S, lane);
-   float v[kL];
+   float v[kL], tg[kL];
    if (MODE == UNIT_ADJ_AGG) {
-      loadPacked(v, a.in + c.xOff, t0, Lu, sStage[warp], lane);
+      fetchPacked(tg, a.in + c.xOff, t0, Lu, lane);
+      loadTables(sTab, a.tables, c, lane);
+      stagePacked(v, tg, sStage[warp], lane);
       adjointAggregates(v, sTab, S, a.agg + base, lane);
       return;
    }
    loadChunk(v, a.in + c.pOff, t0 + lane * kL, Lu);
+   if (MODE == UNIT_OUT_MSE) fetchPacked(tg, a.target + c.xOff, t0, Lu, lane);
+   loadTables(sTab, a.tables, c, lane);
    for (int p = 0; p < S; p++) {
       const float *tb = sTab + p * kBankTabFloats;
       float w[kL];
@@ -607,8 +643,7 @@ __global__ void __launch_bounds__(kThreads) bank_unit_kernel(UnitArgs a)
          for (int t = Lu + lane; t < c.L; t += 32) a.out[c.xOff + t] = 0.0f;
    }
    if (MODE == UNIT_OUT_MSE) {
-      float tg[kL];
-      loadPacked(tg, a.target + c.xOff, t0, Lu, sStage[warp], lane);
+      stagePacked(tg, tg, sStage[warp], lane);
       double sq = 0.0;
 #pragma unroll
       for (int i = 0; i < kL; i++) {
@@ -661,10 +696,11 @@ __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
    const int S = c.S, Lu = c.Lu, t0 = U.y * kUnit;
    const long long base = c.ckOff + (long long) U.y * S;
    const UnitStates entF = loadStates(a.ckptF + base, S, lane), entA = loadStates(a.ckptA + base, S, lane);
-   loadTables(sTab, a.tables, c, lane);
    float v[kL], w[kL], g[kL];
    loadChunk(v, a.u + c.pOff, t0 + lane * kL, Lu);
-   loadPacked(g, a.gy + c.xOff, t0, Lu, sStage, lane);
+   fetchPacked(w, a.gy + c.xOff, t0, Lu, lane);
+   loadTables(sTab, a.tables, c, lane);
+   stagePacked(g, w, sStage, lane);
    // 1. the forward of this unit from its checkpoints; every stage's sequence kept
    for (int s = 0; s < S; s++) {
       const float *tb = sTab + s * kBankTabFloats;
@@ -716,18 +752,22 @@ __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
          pr[4] = fmaf(-lam[i], wr[i], pr[4]);
          g[i] = lam[i];
       }
+      // the five sums over the warp by halving: at each step a lane keeps half of its
+      // values and adds the partner's copy of them; lane 4 k ends with sum k (9 shuffles)
+      const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+      float q[4], q2[2];
 #pragma unroll
-      for (int k = 0; k < 5; k++) {
-#pragma unroll
-         for (int o = 16; o > 0; o >>= 1) pr[k] += __shfl_xor_sync(0xffffffffu, pr[k], o);
+      for (int j = 0; j < 4; j++) {
+         const float lo = pr[j], hi = j == 0 ? pr[4] : 0.0f;
+         q[j] = (b4 ? hi : lo) + __shfl_xor_sync(0xffffffffu, b4 ? lo : hi, 16);
       }
-      if (lane < 5) {
-         float val = pr[0];
 #pragma unroll
-         for (int k = 1; k < 5; k++)
-            if (lane == k) val = pr[k];
-         a.part[(base + s) * 5 + lane] = val;
-      }
+      for (int j = 0; j < 2; j++) q2[j] = (b3 ? q[j + 2] : q[j]) + __shfl_xor_sync(0xffffffffu, b3 ? q[j] : q[j + 2], 8);
+      float r = (b2 ? q2[1] : q2[0]) + __shfl_xor_sync(0xffffffffu, b2 ? q2[0] : q2[1], 4);
+      r += __shfl_xor_sync(0xffffffffu, r, 2);
+      r += __shfl_xor_sync(0xffffffffu, r, 1);
+      const int k = lane >> 2;
+      if ((lane & 3) == 0 && k < 5) a.part[(base + s) * 5 + k] = r;
    }
    __syncwarp(); // every lane's last read of the stage sequences precedes the staging writes
    storePacked(g, a.g + c.xOff, t0, Lu, sStage, lane);
