@@ -613,7 +613,7 @@ __global__ void __launch_bounds__(kThreads) bank_unit_kernel(UnitArgs a)
    const int S = c.S, Lu = c.Lu, t0 = U.y * kUnit;
    const long long base = c.ckOff + (long long) U.y * S;
    constexpr bool OUT = MODE == UNIT_OUT || MODE == UNIT_OUT_MSE;
-   // every global load of the unit is issued before the tables' copy waits on its own
+   // the unit's entry states and input are requested before the tables' copy waits on its own loads
    UnitStates ent = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
    if (OUT) ent = loadStates(a.ckpt + base, S, lane);
    float v[kL], tg[kL];
@@ -625,7 +625,6 @@ __global__ void __launch_bounds__(kThreads) bank_unit_kernel(UnitArgs a)
       return;
    }
    loadChunk(v, a.in + c.pOff, t0 + lane * kL, Lu);
-   if (MODE == UNIT_OUT_MSE) fetchPacked(tg, a.target + c.xOff, t0, Lu, lane);
    loadTables(sTab, a.tables, c, lane);
    for (int p = 0; p < S; p++) {
       const float *tb = sTab + p * kBankTabFloats;
@@ -643,6 +642,9 @@ __global__ void __launch_bounds__(kThreads) bank_unit_kernel(UnitArgs a)
          for (int t = Lu + lane; t < c.L; t += 32) a.out[c.xOff + t] = 0.0f;
    }
    if (MODE == UNIT_OUT_MSE) {
+      // the target is read here, not with the unit's other loads: held across the stages
+      // it costs 16 registers a thread and the occupancy they buy (measured 1 % slower)
+      fetchPacked(tg, a.target + c.xOff, t0, Lu, lane);
       stagePacked(tg, tg, sStage[warp], lane);
       double sq = 0.0;
 #pragma unroll
