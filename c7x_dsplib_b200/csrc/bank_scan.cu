@@ -65,8 +65,6 @@ __device__ __forceinline__ M2f tabP(const float *tb, int k)
    return {q.x, q.y, q.z, q.w};
 }
 
-__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-
 __device__ __forceinline__ float2 shflDown(float2 v, int d)
 {
    v.x = __shfl_down_sync(0xffffffffu, v.x, d);
@@ -441,54 +439,42 @@ __device__ __forceinline__ float2 zeroStatePassRev(const float (&g)[kL], float (
    return make_float2(v[0], v[1]);
 }
 
-// Initial state of this lane's chunk from the unit's entry state, forward time:
-// M^lane entry + the scan of the lanes before.  Returns the inclusive scan in *incl.
+// Initial state of this lane's chunk, forward time: M^lane entry + the scan of the lanes
+// before.  The first chunk's end state takes the unit's entry (M entry + its zero-state end)
+// before the scan, which then carries it to every lane with the chunks' own contributions.
+// Returns the inclusive scan in *incl (the unit's aggregate in the last lane when ZERO_ENTRY).
 template <bool ZERO_ENTRY = false>
 __device__ __forceinline__ float2 chunkStateUp(float2 end, float2 entry, const float *tb, int lane, float2 *incl)
 {
    float2 val = end;
+   if (!ZERO_ENTRY && lane == 0) val = scan::affine(tabP(tb, 0), entry, val);
 #pragma unroll
    for (int k = 0; k < 5; k++) {
       const float2 o = scan::shflUp(val, 1 << k, 32);
       if (lane >= (1 << k)) val = scan::affine(tabP(tb, k), o, val);
    }
    float2 ex = scan::shflUp(val, 1, 32);
-   if (lane == 0) ex = make_float2(0.0f, 0.0f);
+   if (lane == 0) ex = ZERO_ENTRY ? make_float2(0.0f, 0.0f) : entry;
    *incl = val;
-   if constexpr (ZERO_ENTRY) {
-      return ex; // the unit starts from a zero state: nothing to carry in
-   }
-   else {
-#pragma unroll
-      for (int k = 0; k < 5; k++)
-         if ((lane >> k) & 1) entry = scan::affine(tabP(tb, k), entry, make_float2(0.0f, 0.0f));
-      return f2add(entry, ex);
-   }
+   return ex;
 }
 
-// Reverse time: M^(31 - lane) entry + the scan of the lanes after.
+// Reverse time: M^(31 - lane) entry + the scan of the lanes after (lane 31 holds the chunk
+// processed first).
 template <bool ZERO_ENTRY = false>
 __device__ __forceinline__ float2 chunkStateDown(float2 end, float2 entry, const float *tb, int lane, float2 *incl)
 {
    float2 val = end;
+   if (!ZERO_ENTRY && lane == 31) val = scan::affine(tabP(tb, 0), entry, val);
 #pragma unroll
    for (int k = 0; k < 5; k++) {
       const float2 o = shflDown(val, 1 << k);
       if (lane + (1 << k) < 32) val = scan::affine(tabP(tb, k), o, val);
    }
    float2 ex = shflDown(val, 1);
-   if (lane == 31) ex = make_float2(0.0f, 0.0f);
+   if (lane == 31) ex = ZERO_ENTRY ? make_float2(0.0f, 0.0f) : entry;
    *incl = val;
-   if constexpr (ZERO_ENTRY) {
-      return ex;
-   }
-   else {
-      const int m = 31 - lane;
-#pragma unroll
-      for (int k = 0; k < 5; k++)
-         if ((m >> k) & 1) entry = scan::affine(tabP(tb, k), entry, make_float2(0.0f, 0.0f));
-      return f2add(entry, ex);
-   }
+   return ex;
 }
 
 // True internal sequence (in place of the zero-state one) and stage output, from the
