@@ -273,10 +273,18 @@ constexpr int kChainSharedGroups = 48;
 constexpr int kRowPad = 2 * kChainFastStages + 1;
 __device__ __forceinline__ void loadRows(float *rows, const double *P, int n2, int tid, int nthreads)
 {
-   for (int i = tid; i < 2 * kChainFastStages * kRowPad; i += nthreads) {
-      const int r = i / kRowPad, k = i % kRowPad;
-      const int p = r >> 1, q = k >> 1;
-      rows[i] = (r < n2 && k < n2 && q <= p) ? (float) P[4 * blk(p, q) + 2 * (r & 1) + (k & 1)] : 0.0f;
+   constexpr int n = 2 * kChainFastStages * kRowPad;
+   for (int i0 = tid; i0 < n; i0 += 4 * nthreads) { // four loads in flight per thread
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+         const int i = i0 + u * nthreads, r = i / kRowPad, k = i % kRowPad;
+         const int p = r >> 1, q = k >> 1;
+         v[u] = (i < n && r < n2 && k < n2 && q <= p) ? (float) P[4 * blk(p, q) + 2 * (r & 1) + (k & 1)] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+         if (i0 + u * nthreads < n) rows[i0 + u * nthreads] = v[u];
    }
 }
 
@@ -314,8 +322,18 @@ __global__ void __launch_bounds__(kChainWarps * 32) bank_chain_fast_kernel(const
    auto unitOf = [&](int g, int k) { return adj ? units - 1 - (g * kChainGroup + k) : g * kChainGroup + k; };
    auto stageGroup = [&](int g, int gn) {
       const int j0 = adj ? units - g * kChainGroup - gn : g * kChainGroup;
+      const float *src = ag + (long long) j0 * n2;
+      const int n = gn * n2;
       __syncwarp();
-      for (int q = lane; q < gn * n2; q += 32) sE[warp][q] = ag[(long long) j0 * n2 + q];
+      for (int q0 = lane; q0 < n; q0 += 4 * 32) { // four loads in flight per lane
+         float r[4];
+#pragma unroll
+         for (int u = 0; u < 4; u++)
+            if (q0 + 32 * u < n) r[u] = src[q0 + 32 * u];
+#pragma unroll
+         for (int u = 0; u < 4; u++)
+            if (q0 + 32 * u < n) sE[warp][q0 + 32 * u] = r[u];
+      }
       __syncwarp();
       return j0;
    };
@@ -761,16 +779,28 @@ __global__ void __launch_bounds__(32) bank_adjoint_kernel(AdjArgs a)
    storePacked(g, a.g + c.xOff, t0, Lu, sStage, lane);
 }
 
-// Coefficient gradients of one channel (one warp): per coefficient, lane l adds the partial
-// sums of units l, l + 32, ... in FP64, then a fixed butterfly adds the lanes' sums (bitwise
-// repeatable; the channel's units are read 32 at a time instead of one after another).
-__global__ void __launch_bounds__(32) bank_coef_kernel(const RaggedChan *chans, const float *part, float *gcoefs)
+// Coefficient gradients of one channel (one CTA, coefficients spread over its warps): per
+// coefficient, lane l adds the partial sums of units l, l + 32, ... in FP64, in that order,
+// four loads in flight, then a fixed butterfly adds the lanes' sums (bitwise repeatable).
+constexpr int kCoefWarps = 8;
+__global__ void __launch_bounds__(32 * kCoefWarps) bank_coef_kernel(const RaggedChan *chans, const float *part,
+                                                                    float *gcoefs)
 {
    const RaggedChan c = chans[blockIdx.x];
-   const int S = c.S, units = (c.Lu + kUnit - 1) / kUnit, lane = threadIdx.x;
-   for (int q = 0; q < 5 * S; q++) {
+   const int S = c.S, units = (c.Lu + kUnit - 1) / kUnit, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   for (int q = warp; q < 5 * S; q += kCoefWarps) {
+      const float *pq = part + c.ckOff * 5 + q;
+      const long long st = 5LL * S; // one unit's partial sums
       double acc = 0.0;
-      for (int j = lane; j < units; j += 32) acc += (double) part[(c.ckOff + (long long) j * S) * 5 + q];
+      int j = lane;
+      for (; j + 96 < units; j += 128) {
+         const float v0 = pq[j * st], v1 = pq[(j + 32) * st], v2 = pq[(j + 64) * st], v3 = pq[(j + 96) * st];
+         acc += (double) v0;
+         acc += (double) v1;
+         acc += (double) v2;
+         acc += (double) v3;
+      }
+      for (; j < units; j += 32) acc += (double) pq[j * st];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
       if (lane == 0) gcoefs[c.cOff + q] = (float) acc;
@@ -885,7 +915,7 @@ cudaError_t launchBankBackward(const BankLaunch &b, cudaStream_t s)
       if ((e = cudaEventRecord(b.join[i], b.aux[i])) != cudaSuccess) return e;
       if ((e = cudaStreamWaitEvent(s, b.join[i], 0)) != cudaSuccess) return e;
    }
-   bank_coef_kernel<<<b.C, 32, 0, s>>>(b.chans, b.part, b.gcoefs);
+   bank_coef_kernel<<<b.C, 32 * kCoefWarps, 0, s>>>(b.chans, b.part, b.gcoefs);
    countLaunch();
    return cudaGetLastError();
 }
