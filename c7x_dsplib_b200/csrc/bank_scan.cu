@@ -6,7 +6,8 @@
 // stage the chunk is filtered from a zero state (the only serial pass), the
 // chunk end states are combined by a warp scan of the affine maps
 // s -> M s + e (M = A^16 and its powers, A the stage's 2x2 companion matrix,
-// formed in FP64 and rounded once), and the true output follows without a
+// formed in FP64 and rounded once; the unit's entry state joins the first
+// chunk's end state before the scan), and the true output follows without a
 // serial chain: w[i] = w_zs[i] + alpha_i w1 + beta_i w2 with (alpha_i, beta_i)
 // the first row of A^(i+1) and (w1, w2) the chunk's initial state, then
 // y[i] = b0 w[i] + b1 w[i-1] + b2 w[i-2].
@@ -18,9 +19,11 @@
 // lower-triangular: stage p's output drives stage p + 1).  So:
 //   pass 1 (bank_unit_kernel<AGG>): every unit, all stages from a zero state:
 //           e, 2 floats per stage;
-//   pass 2 (bank_chain_kernel): per channel, z_0 = 0, z_{j+1} = Phi z_j + e_j
-//           in FP64, j over the channel's units; z_j is stored (2 floats per
-//           unit and stage): the checkpoints;
+//   pass 2 (bank_chain_fast_kernel up to 16 stages, bank_chain_kernel beyond):
+//           per channel, z_0 = 0, z_{j+1} = Phi z_j + e_j, j over the
+//           channel's units (in two levels through Phi^32 over groups of 32
+//           units in FP32, or one unit after another in FP64); z_j is stored
+//           (2 floats per unit and stage): the checkpoints;
 //   pass 3 (bank_unit_kernel<OUT>): every unit again from its checkpoint: y.
 // The adjoint is the same cascade run backwards in time with the stages in
 // reverse order (v[t] = g[t] - a1 v[t+1] - a2 v[t+2], lambda[t] = b0 v[t] +
@@ -30,7 +33,7 @@
 // checkpoints, keeping every stage's internal sequence w_s in shared memory,
 // and accumulates the coefficient gradients
 //     dL/db_i = sum_t g[t] w[t-i],   dL/da_i = -sum_t lambda[t] w[t-i]
-// in FP32 per unit, then in FP64 per channel in unit order (bank_coef_kernel):
+// in FP32 per unit, then in FP64 per channel in a fixed order (bank_coef_kernel):
 // bitwise repeatable.
 #include <cuda_runtime.h>
 
