@@ -215,11 +215,11 @@ __global__ void __launch_bounds__(128) bank_transition_kernel(const RaggedChan *
 // Per channel (one warp): z_0 = 0, checkpoint z_j, z_{j+1} = Phi z_j + e_j over the
 // channel's units (adjoint: from the last unit back).  z in FP64; cascades of more than
 // 16 stages (those of up to 16 take bank_chain_fast_kernel).
-__global__ void __launch_bounds__(32) bank_chain_kernel(const RaggedChan *chans, const double *phi,
+__global__ void __launch_bounds__(32) bank_chain_kernel(const RaggedChan *chans, const int *order, const double *phi,
                                                         const float2 *agg, float2 *ckpt, int adj)
 {
    extern __shared__ double dynC[];
-   const RaggedChan c = chans[blockIdx.x];
+   const RaggedChan c = chans[order[blockIdx.x]];
    const int S = c.S, lane = threadIdx.x;
    if (S <= kChainFastStages) return; // bank_chain_fast_kernel
    const int nb = S * (S + 1) / 2, n2 = 2 * S;
@@ -306,14 +306,14 @@ __device__ __forceinline__ float chainStep(const float *row, float z, float e, i
    return (a0 + a1) + (a2 + a3);
 }
 
-__global__ void __launch_bounds__(kChainWarps * 32) bank_chain_fast_kernel(const RaggedChan *chans,
+__global__ void __launch_bounds__(kChainWarps * 32) bank_chain_fast_kernel(const RaggedChan *chans, const int *order,
                                                                            const double *phi, const float2 *agg,
                                                                            float2 *ckpt, float *groupBuf, int adj)
 {
    __shared__ float sE[kChainWarps][kChainGroup * 2 * kChainFastStages]; // a group's aggregates, per warp
    __shared__ float sG[kChainSharedGroups * 2 * kChainFastStages];       // group states
    __shared__ float sRow[2][2 * kChainFastStages * kRowPad];             // Phi and Phi^32
-   const RaggedChan c = chans[blockIdx.x];
+   const RaggedChan c = chans[order[blockIdx.x]];
    const int S = c.S, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    if (S == 0 || S > kChainFastStages) return;
    const int n2 = 2 * S, nb = S * (S + 1) / 2;
@@ -856,10 +856,10 @@ cudaError_t launchBankForward(const BankLaunch &b, cudaStream_t s)
    if ((e = cudaFuncSetAttribute(bank_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dynC)) !=
        cudaSuccess)
       return e;
-   bank_chain_fast_kernel<<<b.C, kChainWarps * 32, 0, s>>>(b.chans, b.phi, b.aggF, b.ckptF, b.groupF, 0);
+   bank_chain_fast_kernel<<<b.C, kChainWarps * 32, 0, s>>>(b.chans, b.chainOrder, b.phi, b.aggF, b.ckptF, b.groupF, 0);
    countLaunch();
    if (b.Smax > kChainFastStages) {
-      bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.phi, b.aggF, b.ckptF, 0);
+      bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.chainOrder, b.phi, b.aggF, b.ckptF, 0);
       countLaunch();
    }
    a.out = b.y;
@@ -887,10 +887,10 @@ cudaError_t launchBankBackward(const BankLaunch &b, cudaStream_t s)
    if ((e = cudaFuncSetAttribute(bank_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dynC)) !=
        cudaSuccess)
       return e;
-   bank_chain_fast_kernel<<<b.C, kChainWarps * 32, 0, s>>>(b.chans, b.phi, b.aggA, b.ckptA, b.groupA, 1);
+   bank_chain_fast_kernel<<<b.C, kChainWarps * 32, 0, s>>>(b.chans, b.chainOrder, b.phi, b.aggA, b.ckptA, b.groupA, 1);
    countLaunch();
    if (b.Smax > kChainFastStages) {
-      bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.phi, b.aggA, b.ckptA, 1);
+      bank_chain_kernel<<<b.C, 32, dynC, s>>>(b.chans, b.chainOrder, b.phi, b.aggA, b.ckptA, 1);
       countLaunch();
    }
    if ((e = cudaFuncSetAttribute(bank_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

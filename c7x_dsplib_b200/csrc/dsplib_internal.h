@@ -341,6 +341,7 @@ struct BankLaunch {
    float *g;          // adjoint: gradient w.r.t. the FIR output
    float2 *aggF, *ckptF, *aggA, *ckptA;
    float *groupF, *groupA; // chain group states of channels beyond 64 groups of 32 units
+   const int *chainOrder;  // channel of each chain CTA (most units first)
    float *part;       // adjoint: 5 coefficient-gradient sums per unit and stage
    float *gcoefs;
    // forward with the loss fused (target != nullptr): gyOut = scale (y - target), unit

@@ -64,6 +64,7 @@ struct RaggedPlan {
    int4 *dDhRuns = nullptr;     // (channel, first tile, tiles, slot): taps gradient, longest first
    int nDhRuns = 0;
    int2 *dUnits = nullptr;      // cascade units (channel, unit index)
+   int *dChainOrder = nullptr;  // channels by unit count, most first: the chains' CTA order
    int *err = nullptr;          // error word of the tensor-core kernels (mapped page-locked)
    int device = 0;
    // work buffer layout (float offsets)
@@ -211,6 +212,7 @@ static void freePlan(RaggedPlan *p)
    cudaFree(p->dDhStart);
    cudaFree(p->dDhRuns);
    cudaFree(p->dUnits);
+   cudaFree(p->dChainOrder);
    freeErrorWord(p->err);
    for (RaggedPlan::Segment &g : p->segs) freePlan(g.plan);
    for (int i = 0; i < p->nAux; i++) {
@@ -317,6 +319,11 @@ static DSPLIB_STATUS raggedPlanBuild(DSPLIB_gpu_raggedPlan *plan, int32_t numCha
    std::stable_sort(firFwd.begin(), firFwd.end(), longer);
    std::stable_sort(firDx.begin(), firDx.end(), longer);
    std::stable_sort(dhRuns.begin(), dhRuns.end(), longer);
+   // the chains run one CTA per channel, their time in proportion to its units: the longest
+   // channels start first, so that no long chain is left for the last wave
+   std::vector<int> chainOrder(numChannels);
+   for (int c = 0; c < numChannels; c++) chainOrder[c] = c;
+   std::stable_sort(chainOrder.begin(), chainOrder.end(), [&](int a, int b) { return ch[a].Lu > ch[b].Lu; });
    if (co / 5 > INT_MAX || units.size() > (size_t) INT_MAX) {
       delete p;
       return DSPLIB_ERR_INVALID_DIMENSION;
@@ -380,7 +387,7 @@ static DSPLIB_STATUS raggedPlanBuild(DSPLIB_gpu_raggedPlan *plan, int32_t numCha
    const bool ok = upload(&p->dChan, ch) == cudaSuccess && upload(&p->dFwdItems, fwd) == cudaSuccess &&
                    upload(&p->dFirFwdRuns, firFwd) == cudaSuccess && upload(&p->dFirDxRuns, firDx) == cudaSuccess &&
                    upload(&p->dDhStart, start) == cudaSuccess && upload(&p->dDhRuns, dhRuns) == cudaSuccess &&
-                   upload(&p->dUnits, units) == cudaSuccess;
+                   upload(&p->dUnits, units) == cudaSuccess && upload(&p->dChainOrder, chainOrder) == cudaSuccess;
    if (!ok) {
       freePlan(p);
       return DSPLIB_ERR_FAILURE;
@@ -522,6 +529,7 @@ static BankLaunch bankLaunch(const RaggedPlan *p, const float *work)
    b.chans = p->dChan;
    b.C = p->C;
    b.units = p->dUnits;
+   b.chainOrder = p->dChainOrder;
    b.nUnits = p->nUnits;
    b.Smax = p->Smax;
    b.tables = work + p->wTab;
